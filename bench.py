@@ -1,0 +1,301 @@
+"""Benchmark of the Biot LBM hot path on B200.
+
+Default workload (one line of JSON on rank 0): D2Q9 Darcy flow on a 1024 x 1024
+grid with log-normal permeability (GRF, correlation length 16 cells, sigma 1,
+seed 0), per-cell omega, Dirichlet pressure left/right, no flux top/bottom,
+FP32 populations with an FP64 residual norm.  One step = 200 fused sweeps
+(one CUDA-graph replay) plus the FP64 residual reduction.  ``value`` is GLUPS
+(10^9 lattice-cell updates per second) with the populations resident in HBM;
+``e2e`` adds, per step, the host->device copy of the populations from pinned
+host memory and the device->host read of the residual.  L2 is flushed (a
+256 MiB write) between timed steps.
+
+``--impl reference`` times the CPU restatement of the reference's JAX solver
+(the oracle, NumPy) on the host on a bounded sample of the same workload.
+
+Multi-GPU (``torchrun --nproc-per-node N``): the Darcy path of the reference
+runs one domain per device, and a second GPU holds an independent replica
+(replicas only, weak scaling); timing is the max over ranks.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SWEEPS_PER_STEP = 200
+N = 1024
+BYTES_PER_LU_F32 = (9 + 9 + 1) * 4     # read f, write f, read per-cell omega
+METRIC = "GLUPS"
+WORKLOAD = "darcy_d2q9_1024x1024_lognormal_k"
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 8:
+                continue
+            try:
+                sm.append(float(p[0]))
+                mx.append(float(p[1]))
+            except ValueError:
+                continue
+            for name, v in zip(names, p[4:8]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(np.max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak_hbm():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def ncu_traffic_per_launch():
+    """DRAM bytes per launch of the Darcy sweep from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "darcy_sweep_1024x1024_lognormal.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+def cpu_oracle_glups(seconds=12.0, n=N):
+    """The oracle (NumPy, one host thread) on the same workload: full-size
+    sweeps until ``seconds`` of CPU work are done."""
+    import oracle.api as O
+    from xlb_biot_b200.workloads import darcy_lognormal
+    solver, _ = darcy_lognormal(O, n=n)
+    f = solver.assign_fields_sharded()
+    f, _ = solver.step(f, 0)             # warm-up
+    t0 = time.perf_counter()
+    sweeps = 0
+    while time.perf_counter() - t0 < seconds:
+        f, _ = solver.step(f, sweeps)
+        sweeps += 1
+    dt = time.perf_counter() - t0
+    return n * n * sweeps / dt / 1e9, sweeps
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    import oracle.api as O
+    from xlb_biot_b200.workloads import darcy_lognormal
+    solver, _ = darcy_lognormal(O, n=N)
+    f = solver.assign_fields_sharded()
+    sweeps_per_step = 3                      # bounded sample of the 200-sweep step
+    for w in range(args.warmup):
+        f, _ = solver.step(f, w)
+    times = []
+    for s in range(args.steps):
+        t0 = time.perf_counter()
+        for k in range(sweeps_per_step):
+            f, _ = solver.step(f, k)
+        np.sum((f - f) ** 2)
+        times.append(time.perf_counter() - t0)
+    total = float(np.sum(times))
+    glups = N * N * sweeps_per_step * args.steps / total / 1e9
+    line = {"impl": "reference", "metric": METRIC, "value": glups, "unit": "GLUPS", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "nx": N, "ny": N, "sweeps_per_step": sweeps_per_step},
+            "cpu_baseline": {"value": glups, "unit": "GLUPS", "cores": 1, "kind": "port",
+                             "sample": f"{sweeps_per_step} full 1024x1024 sweeps per step of the NumPy restatement "
+                                       "of the reference's JAX Darcy solver (JAX is not installable offline)"},
+            "e2e": {"value": glups, "unit": "GLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    import xlb_biot_b200.api as G
+    from xlb_biot_b200.workloads import darcy_lognormal
+
+    solver, _ = darcy_lognormal(G, n=N)
+    f0 = solver.assign_fields_sharded()
+    loop = solver.sweep_graph(SWEEPS_PER_STEP)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")     # 256 MiB > L2
+    stream = torch.cuda.current_stream()
+
+    # host buffers of the end-to-end variant (pinned)
+    host_f = torch.empty(loop.state.shape[2] * loop.state.stride(2), dtype=loop.state.dtype).pin_memory()
+    state_flat = loop.state.as_strided((host_f.numel(),), (1,))
+    state_flat.copy_(f0.as_strided((host_f.numel(),), (1,)))
+    host_f.copy_(state_flat)
+    host_res = torch.empty(1, dtype=torch.float64).pin_memory()
+
+    def device_step():
+        loop.replay()
+
+    for _ in range(max(3, args.warmup)):
+        device_step()
+    torch.cuda.synchronize()
+
+    # -- device-resident timing (value) --------------------------------------
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for s in range(args.steps):
+        flush.fill_(float(s))
+        ev[s][0].record(stream)
+        device_step()
+        ev[s][1].record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    dev_ms = sum(a.elapsed_time(b) for a, b in ev)
+
+    # -- end-to-end through the public loop with host buffers ------------------
+    ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for s in range(args.steps):
+        flush.fill_(float(s))
+        ev2[s][0].record(stream)
+        state_flat.copy_(host_f, non_blocking=True)
+        device_step()
+        host_res.copy_(loop.sumsq, non_blocking=True)
+        ev2[s][1].record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = sum(a.elapsed_time(b) for a, b in ev2)
+
+    # -- per-launch kernel time for the roofline (same stream, no flush) --------
+    kev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+    reps = 5
+    kev[0].record(stream)
+    for _ in range(reps):
+        device_step()
+    kev[1].record(stream)
+    torch.cuda.synchronize()
+    per_sweep_ms = kev[0].elapsed_time(kev[1]) / (reps * SWEEPS_PER_STEP)
+
+    t = torch.tensor([dev_ms, e2e_ms], dtype=torch.float64, device="cuda")
+    if ws > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    dev_ms, e2e_ms = float(t[0]), float(t[1])
+    lu_total = ws * N * N * SWEEPS_PER_STEP * args.steps
+    value = lu_total / (dev_ms * 1e-3) / 1e9
+    e2e = lu_total / (e2e_ms * 1e-3) / 1e9
+    peak, peak_kind = measured_peak_hbm()
+    achieved = N * N * BYTES_PER_LU_F32 / (per_sweep_ms * 1e-3) / 1e9
+    traffic = ncu_traffic_per_launch()
+    res = float(host_res[0])
+    if rank == 0:
+        cpu = None
+        if ws == 1 and not args.no_cpu_baseline:
+            g, sweeps = cpu_oracle_glups()
+            cpu = {"value": g, "unit": "GLUPS", "cores": 1, "kind": "port",
+                   "sample": f"{sweeps} full 1024x1024 sweeps of the NumPy restatement of the reference's Darcy "
+                             "solver on one host thread"}
+        line = {
+            "metric": METRIC, "value": value, "unit": "GLUPS", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "nx": N, "ny": N, "sweeps_per_step": SWEEPS_PER_STEP,
+                       "permeability": "exp(GRF), SE covariance, ell=16 cells, sigma=1, seed 0",
+                       "bcs": "ADR anti-bounce-back p=1 left, p=0 right; ADR bounce-back top/bottom",
+                       "residual": "FP64 sum (f_new - f_old)^2 fused into the last sweep",
+                       "l2": "flushed between timed steps (256 MiB write)", "parallelism": f"replicas{ws}"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "traffic": traffic, "algorithmic_bytes_per_launch": N * N * BYTES_PER_LU_F32,
+                         "kernel": "xlbb::sweep_kernel<DarcyPhys<float>>", "kernel_ms": per_sweep_ms},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e, "unit": "GLUPS", "h2d_bytes_per_step": host_f.numel() * host_f.element_size(),
+                    "d2h_bytes_per_step": 8},
+            "gpu_launches": args.steps * loop.launches_per_replay,
+            "clocks": clk,
+            "residual_sumsq_last_sweep": res,
+        }
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

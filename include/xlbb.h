@@ -1,0 +1,181 @@
+/*
+ * xlbb.h -- C ABI of the B200 (sm_100a) lattice-Boltzmann Biot hot path.
+ *
+ * The reference (s-lunowa/xlb-biot) is pure Python/JAX; its "interface" for
+ * this path is the set of solver methods listed beside each entry point below
+ * (file:line inside the reference project).  Every entry point:
+ *   - takes device pointers owned by the caller plus a cudaStream_t (as void*),
+ *   - is stream-ordered and asynchronous, allocates nothing,
+ *   - returns XLBB_OK (0) or a negative XLBB_E* code; a thread-local message is
+ *     kept for xlbb_last_error().
+ *
+ * Memory layout of every field ("SoA"): component planes of a (ny x pitch)
+ * row-major grid, x fastest:  value(x, y, i) = base[i*plane + y*pitch + x],
+ * with pitch >= nx and plane >= ny*pitch.  The Python layer exposes such a
+ * buffer to users as a tensor of the reference's shape (nx, ny, q).
+ */
+#ifndef XLBB_H
+#define XLBB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define XLBB_OK 0
+#define XLBB_EBADARG (-1)
+#define XLBB_ELAUNCH (-2)
+#define XLBB_ETIMEOUT (-3)
+#define XLBB_ENONFINITE (-4)
+#define XLBB_EUNSUPPORTED (-5)
+
+#define XLBB_F32 0
+#define XLBB_F64 1
+
+typedef struct {
+    int nx, ny;        /* logical grid size (cells)                        */
+    int pitch;         /* row stride in elements                           */
+    long long plane;   /* component-plane stride in elements               */
+} XlbbGrid;
+
+/*
+ * Boundary rules compiled on the host from the reference's BC objects.
+ * Rule cells are stored CSR-by-row: the cells of row y are
+ * cell_x[row_ptr[y] .. row_ptr[y+1]) sorted by x.  For each rule cell and
+ * direction d, code[r*q+d] selects the base value and cst[r*q+d] is added:
+ *   0..q-1      : +src[code]        (src = pre-collision input for a
+ *   q..2q-1     : -src[code-q]       post-collision rule, own post-collision
+ *   2q          : 0                  populations for a post-streaming rule)
+ *   2q+1        : +current value    (collision output / streamed value)
+ *   2q+2        : -current value
+ */
+typedef struct {
+    int count;
+    const int* row_ptr;      /* ny+1 entries */
+    const int* cell_x;       /* count entries */
+    const uint8_t* code;     /* count*q entries */
+    const void* cst;         /* count*q entries, compute dtype */
+} XlbbRules;
+
+typedef struct {
+    double lam, mu;          /* uniform Lame parameters (lattice units)       */
+    const void* lam_field;   /* optional per-cell lambda (1 plane) or NULL    */
+    const void* mu_field;    /* optional per-cell mu (1 plane) or NULL        */
+} XlbbElastMaterial;
+
+/*
+ * One D2Q8 elasticity sweep, fused collide + post-collision BCs + stream +
+ * post-streaming BCs, with the multigrid smoother algebra folded in:
+ *     g   = f_in - resid                      (resid may be NULL)
+ *     out = a * f_in + b * STEP(g)
+ * a=0,b=1 is LBMElasticity._step (src/elasticity.py:1169-1219);
+ * a=1-gamma,b=gamma the damped smoothing sweep of _mg_step (:1258-1267);
+ * a=1,b=-1 the residual f - STEP(f - r) (:1285-1286).
+ * STEP applies force (if use_force) + fext as in collision() (:959-1000).
+ * If sumsq != NULL, each CTA writes sum(out^2) over the box [bx0,bx1)x[by0,by1)
+ * into sumsq[cta] (FP64; reduce with xlbb_reduce_sum); count via
+ * xlbb_elast_sweep_ctas().  If div_out != NULL the divergence moment of out
+ * (update_divergence, :1040-1058) is written as a side output.
+ */
+typedef struct {
+    const void* f_in;
+    void* f_out;
+    const void* force;       /* static force (2 planes) or NULL */
+    int use_force;
+    const void* fext;        /* external force (2 planes) or NULL */
+    const void* resid;       /* residual (8 planes, zero outside the interior) or NULL */
+    double a, b;
+    XlbbRules pc, ps;
+    double* sumsq;
+    int bx0, bx1, by0, by1;
+    void* div_out;
+} XlbbElastSweep;
+
+int xlbb_elast_sweep(int dtype, const XlbbGrid* g, const XlbbElastMaterial* mat,
+                     const XlbbElastSweep* s, void* stream);
+int xlbb_elast_sweep_ctas(const XlbbGrid* g);
+
+/*
+ * One D2Q9 advection-diffusion-reaction BGK sweep (AdvectionDiffusionReactionBGK.step,
+ * src/darcy.py:131-171 with collision :106-129): omega uniform or per cell.
+ * If sumsq != NULL each CTA writes sum((out - f_in)^2) (FP64 convergence residual).
+ */
+typedef struct {
+    const void* f_in;
+    void* f_out;
+    double omega;
+    const void* omega_field; /* per-cell omega (1 plane) or NULL */
+    const void* source;      /* static source (1 plane) or NULL */
+    const void* ext_source;  /* external source (1 plane) or NULL */
+    XlbbRules pc, ps;
+    double* sumsq;
+} XlbbDarcySweep;
+
+int xlbb_darcy_sweep(int dtype, const XlbbGrid* g, const XlbbDarcySweep* s, void* stream);
+int xlbb_darcy_sweep_ctas(const XlbbGrid* g);
+
+/*
+ * Isotropic 9-point gradient of a scalar field with the ADR (anti-)bounce-back
+ * rules applied to the shifted copies (AdvectionDiffusionReactionBGK.gradient,
+ * src/darcy.py:75-104):  out = base + gradient(q, scale)  (2 planes; base may
+ * be NULL, out may alias base).
+ */
+int xlbb_darcy_gradient(int dtype, const XlbbGrid* g, const void* q, double scale,
+                        const XlbbRules* rules, const void* base, void* out, void* stream);
+
+/*
+ * Elasticity macroscopic fields (LBMElasticity.update_macroscopic :1002-1038,
+ * update_divergence :1040-1058).  eta = m10,m01 + 0.5*(force + fext);
+ * any output may be NULL.  div is computed from f (not f + force).
+ */
+int xlbb_elast_moments(int dtype, const XlbbGrid* g, const XlbbElastMaterial* mat,
+                       const void* f, const void* force, const void* fext,
+                       void* eta, void* sigma, void* div, double div_scale, void* stream);
+
+/* Elasticity equilibrium (LBMElasticity.equilibrium :909-957). */
+int xlbb_elast_equilibrium(int dtype, const XlbbGrid* g, const XlbbElastMaterial* mat,
+                           const void* eta, const void* sigma, const void* force,
+                           const void* fext, void* f_out, void* stream);
+
+/*
+ * Darcy macroscopic fields (update_macroscopic, src/darcy.py:36-73):
+ * rho = sum f + 0.5*(source + ext_source); grad = -3*omega*sum c_i f_i.
+ */
+int xlbb_darcy_moments(int dtype, const XlbbGrid* g, const void* f, double omega,
+                       const void* omega_field, const void* source, const void* ext_source,
+                       void* rho, void* grad, void* stream);
+
+/*
+ * Multigrid transfers (LBMElasticity._restrict :850-865, _prolong :878-894).
+ * Interior box of the fine grid: [x0, nx_f - x1bc) x [y0, ny_f - y1bc) with the
+ * same BC offsets on the coarse grid.  restrict writes the 2x2 block SUMS into
+ * the coarse grid's interior and zeros outside it; prolong_add adds the coarse
+ * interior, injected, into the fine interior.
+ */
+int xlbb_restrict(int dtype, const XlbbGrid* fine, const XlbbGrid* coarse, int q,
+                  int x0, int x1bc, int y0, int y1bc, const void* res, void* r_coarse, void* stream);
+int xlbb_prolong_add(int dtype, const XlbbGrid* fine, const XlbbGrid* coarse, int q,
+                     int x0, int x1bc, int y0, int y1bc, const void* f_coarse, void* f_fine, void* stream);
+
+/* Deterministic FP64 sum of n partials (fixed order) into *out. */
+int xlbb_reduce_sum(const double* partials, int n, double* out, void* stream);
+
+/* Sum of squares of nplanes planes over a box, into partials[] (one per CTA; see
+ * xlbb_sumsq_ctas) -- the norm of substract/residual fields at any level. */
+int xlbb_sumsq(int dtype, const XlbbGrid* g, int nplanes, const void* data,
+               int bx0, int bx1, int by0, int by1, double* partials, void* stream);
+int xlbb_sumsq_ctas(const XlbbGrid* g);
+
+/* out = a*x + b*y elementwise over n elements (n contiguous elements). */
+int xlbb_axpby(int dtype, long long n, double a, const void* x, double b, const void* y,
+               void* out, void* stream);
+
+const char* xlbb_last_error(void);
+int xlbb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* XLBB_H */

@@ -1,0 +1,119 @@
+"""ctypes binding of ``libxlbb.so`` (the C ABI declared in ``include/xlbb.h``).
+
+There is no CPU fallback: if the library or a CUDA device is missing, every
+solver call raises.  All calls are asynchronous on torch's current CUDA stream.
+"""
+import ctypes
+import os
+
+import torch
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libxlbb.so")
+
+XLBB_F32, XLBB_F64 = 0, 1
+ERRORS = {-1: "XLBB_EBADARG", -2: "XLBB_ELAUNCH", -3: "XLBB_ETIMEOUT", -4: "XLBB_ENONFINITE",
+          -5: "XLBB_EUNSUPPORTED"}
+
+
+class XlbbError(RuntimeError):
+    """A negative status returned by the C ABI."""
+
+
+class Grid(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("pitch", ctypes.c_int), ("plane", ctypes.c_longlong)]
+
+
+class Rules(ctypes.Structure):
+    _fields_ = [("count", ctypes.c_int), ("row_ptr", ctypes.c_void_p), ("cell_x", ctypes.c_void_p),
+                ("code", ctypes.c_void_p), ("cst", ctypes.c_void_p)]
+
+
+class ElastMaterial(ctypes.Structure):
+    _fields_ = [("lam", ctypes.c_double), ("mu", ctypes.c_double), ("lam_field", ctypes.c_void_p),
+                ("mu_field", ctypes.c_void_p)]
+
+
+class ElastSweep(ctypes.Structure):
+    _fields_ = [("f_in", ctypes.c_void_p), ("f_out", ctypes.c_void_p), ("force", ctypes.c_void_p),
+                ("use_force", ctypes.c_int), ("fext", ctypes.c_void_p), ("resid", ctypes.c_void_p),
+                ("a", ctypes.c_double), ("b", ctypes.c_double), ("pc", Rules), ("ps", Rules),
+                ("sumsq", ctypes.c_void_p), ("bx0", ctypes.c_int), ("bx1", ctypes.c_int),
+                ("by0", ctypes.c_int), ("by1", ctypes.c_int), ("div_out", ctypes.c_void_p)]
+
+
+class DarcySweep(ctypes.Structure):
+    _fields_ = [("f_in", ctypes.c_void_p), ("f_out", ctypes.c_void_p), ("omega", ctypes.c_double),
+                ("omega_field", ctypes.c_void_p), ("source", ctypes.c_void_p), ("ext_source", ctypes.c_void_p),
+                ("pc", Rules), ("ps", Rules), ("sumsq", ctypes.c_void_p)]
+
+
+P = ctypes.c_void_p
+I = ctypes.c_int
+D = ctypes.c_double
+PG = ctypes.POINTER(Grid)
+SIGNATURES = {
+    "xlbb_elast_sweep": (I, [I, PG, ctypes.POINTER(ElastMaterial), ctypes.POINTER(ElastSweep), P]),
+    "xlbb_elast_sweep_ctas": (I, [PG]),
+    "xlbb_darcy_sweep": (I, [I, PG, ctypes.POINTER(DarcySweep), P]),
+    "xlbb_darcy_sweep_ctas": (I, [PG]),
+    "xlbb_darcy_gradient": (I, [I, PG, P, D, ctypes.POINTER(Rules), P, P, P]),
+    "xlbb_elast_moments": (I, [I, PG, ctypes.POINTER(ElastMaterial), P, P, P, P, P, P, D, P]),
+    "xlbb_elast_equilibrium": (I, [I, PG, ctypes.POINTER(ElastMaterial), P, P, P, P, P, P]),
+    "xlbb_darcy_moments": (I, [I, PG, P, D, P, P, P, P, P, P]),
+    "xlbb_restrict": (I, [I, PG, PG, I, I, I, I, I, P, P, P]),
+    "xlbb_prolong_add": (I, [I, PG, PG, I, I, I, I, I, P, P, P]),
+    "xlbb_reduce_sum": (I, [P, I, P, P]),
+    "xlbb_sumsq": (I, [I, PG, I, P, I, I, I, I, P, P]),
+    "xlbb_sumsq_ctas": (I, [PG]),
+    "xlbb_axpby": (I, [I, ctypes.c_longlong, D, P, D, P, P, P]),
+    "xlbb_last_error": (ctypes.c_char_p, []),
+    "xlbb_version": (I, []),
+}
+
+_lib = None
+
+
+def lib():
+    """Load ``libxlbb.so`` once.  Raises if it is missing (build it with
+    ``python -m xlb_biot_b200.build``)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise XlbbError(f"CUDA library not built: {LIB_PATH} is missing "
+                            "(run `python -m xlb_biot_b200.build`)")
+        handle = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(handle, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = handle
+    return _lib
+
+
+def require_cuda():
+    if not torch.cuda.is_available():
+        raise XlbbError("xlb_biot_b200 needs a CUDA device: there is no CPU fallback")
+
+
+def check(status, what):
+    if status < 0:
+        msg = lib().xlbb_last_error().decode()
+        raise XlbbError(f"{what} failed with {ERRORS.get(status, status)}: {msg}")
+    return status
+
+
+def stream_ptr():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def dtype_code(dtype):
+    if dtype == torch.float32:
+        return XLBB_F32
+    if dtype == torch.float64:
+        return XLBB_F64
+    raise XlbbError(f"unsupported dtype {dtype}")
+
+
+def ptr(t):
+    return None if t is None else ctypes.c_void_p(t.data_ptr())

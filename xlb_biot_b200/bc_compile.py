@@ -1,0 +1,182 @@
+"""Compile an ordered list of boundary-condition objects into per-cell rules.
+
+Every boundary condition of the Biot path is, cell by cell, an affine map of
+the populations it reads (``fout`` = collision output or streamed values, and
+``fin`` = the step input or post-collision values).  Applying a list of them in
+order (``apply_bc``, ``src/elasticity.py:1061-1091``) is again affine per cell.
+This module finds that map by probing the objects' own ``apply`` methods with
+basis vectors once, then checks that every output direction is
+``+-base + constant`` with ``base`` one of {same direction of fout, one
+direction of fin, zero}.  The result is uploaded as a CSR-by-row rule table
+(``XlbbRules`` in ``include/xlbb.h``) and applied inside the sweep kernels.
+
+A random self-check at compile time compares the compiled rules with the
+direct application of the BC list, so non-local or non-affine user BCs are
+rejected instead of silently mis-compiled.
+"""
+import numpy as np
+import torch
+
+from . import _lib
+from .boundary_conditions import apply_in_order
+
+
+class CompiledRules:
+    """Device-resident rule table of one grid and one phase."""
+
+    def __init__(self, q, ny, cells, code, cst, dtype, device):
+        self.q = q
+        self.count = len(cells)
+        order = np.lexsort((cells[:, 0], cells[:, 1])) if self.count else np.zeros(0, dtype=np.int64)
+        cells = cells[order]
+        self.cells = cells
+        self.code_np = code[order]
+        self.cst_np = cst[order]
+        row_ptr = np.zeros(ny + 1, dtype=np.int32)
+        if self.count:
+            np.add.at(row_ptr, cells[:, 1] + 1, 1)
+        row_ptr = np.cumsum(row_ptr).astype(np.int32)
+        if self.count:
+            self.row_ptr = torch.as_tensor(row_ptr, device=device)
+            self.cell_x = torch.as_tensor(cells[:, 0].astype(np.int32), device=device)
+            self.code = torch.as_tensor(self.code_np.astype(np.uint8).reshape(-1), device=device)
+            self.cst = torch.as_tensor(self.cst_np.reshape(-1), device=device).to(dtype)
+        else:
+            self.row_ptr = self.cell_x = self.code = self.cst = None
+
+    def struct(self):
+        if self.count == 0:
+            return _lib.Rules(0, None, None, None, None)
+        return _lib.Rules(self.count, self.row_ptr.data_ptr(), self.cell_x.data_ptr(), self.code.data_ptr(),
+                          self.cst.data_ptr())
+
+    def restricted(self, nx, ny, dtype, device):
+        """The same rules on a smaller grid: cells outside it are dropped (the
+        reference's coarse-level gradient gathers clamp and scatters drop)."""
+        keep = (self.cells[:, 0] < nx) & (self.cells[:, 1] < ny) if self.count else np.zeros(0, bool)
+        return CompiledRules(self.q, ny, self.cells[keep], self.code_np[keep], self.cst_np[keep], dtype, device)
+
+
+def _run(bcs, fout, fin, step, names):
+    return apply_in_order(bcs, fout, fin, implementation_step=step, names=names)
+
+
+def compile_rules(bcs, nx, ny, q, dtype, device, step=None, names=None, check=True):
+    """Rules of ``bcs`` for one phase: ``step`` in {"PostCollision",
+    "PostStreaming"} (apply_bc semantics) or ``names`` (the gradient's filter)."""
+    if step is not None:
+        active = [bc for bc in bcs if bc.implementationStep == step]
+    else:
+        active = [bc for bc in bcs if bc.name in names]
+    cells = []
+    for bc in active:
+        idx = np.array(bc.indices, dtype=np.int64).reshape(2, -1).T
+        ok = (idx[:, 0] >= 0) & (idx[:, 0] < nx) & (idx[:, 1] >= 0) & (idx[:, 1] < ny)
+        cells.append(idx[ok])
+    if not cells or sum(len(c) for c in cells) == 0:
+        return CompiledRules(q, ny, np.zeros((0, 2), np.int64), np.zeros((0, q), np.uint8), np.zeros((0, q)),
+                             dtype, device)
+    cells = np.unique(np.vstack(cells), axis=0)
+    cx, cy = cells[:, 0], cells[:, 1]
+
+    def probe(fout_vec, fin_vec):
+        fout = np.zeros((nx, ny, q))
+        fin = np.zeros((nx, ny, q))
+        if fout_vec is not None:
+            fout[cx, cy] = fout_vec
+        if fin_vec is not None:
+            fin[cx, cy] = fin_vec
+        return _run(bcs, fout, fin, step, names)[cx, cy]
+
+    c0 = probe(None, None)
+    eye = np.eye(q)
+    A = np.stack([probe(eye[k], None) - c0 for k in range(q)], axis=-1)   # (n, q_out, q_in)
+    B = np.stack([probe(None, eye[k]) - c0 for k in range(q)], axis=-1)
+    # (1 + c) - c is not exactly 1 in floating point: snap the probed
+    # coefficients to integers (a genuine scaling survives and is rejected below)
+    A = np.where(np.abs(A - np.round(A)) < 1e-9, np.round(A), A)
+    B = np.where(np.abs(B - np.round(B)) < 1e-9, np.round(B), B)
+
+    n = len(cells)
+    code = np.empty((n, q), dtype=np.uint8)
+    KEEP, NEG_KEEP, ZERO = 2 * q + 1, 2 * q + 2, 2 * q
+    for d in range(q):
+        a, b = A[:, d, :], B[:, d, :]
+        a_other = a.copy()
+        a_other[:, d] = 0
+        nz_a = np.abs(a_other).sum(axis=1) > 0
+        nb = (np.abs(b) > 0).sum(axis=1)
+        ad = a[:, d]
+        if np.any(nz_a):
+            raise NotImplementedError("boundary rule mixes streamed directions; not representable")
+        both = (ad != 0) & (nb > 0)
+        if np.any(both) or np.any(nb > 1):
+            raise NotImplementedError("boundary rule combines several sources; not representable")
+        bk = np.argmax(np.abs(b), axis=1)
+        bv = b[np.arange(n), bk]
+        cd = np.full(n, ZERO, dtype=np.int64)
+        cd[ad == 1] = KEEP
+        cd[ad == -1] = NEG_KEEP
+        cd[bv == 1] = bk[bv == 1]
+        cd[bv == -1] = q + bk[bv == -1]
+        bad = ((ad != 0) & (np.abs(ad) != 1)) | ((nb == 1) & (np.abs(bv) != 1))
+        if np.any(bad):
+            raise NotImplementedError("boundary rule scales a population; not representable")
+        code[:, d] = cd
+    rules = CompiledRules(q, ny, cells, code, c0, dtype, device)
+    if check:
+        _self_check(bcs, nx, ny, q, step, names, rules)
+    return rules
+
+
+def evaluate_rules(rules, cur, src):
+    """Apply compiled rules to per-cell vectors (host; used by the compile-time
+    self-check): ``cur``/``src`` are (n, q) arrays in ``rules.cells`` order."""
+    q = rules.q
+    code = rules.code_np.astype(np.int64)
+    out = np.empty_like(cur)
+    rows = np.arange(len(code))
+    for d in range(q):
+        cdv = code[:, d]
+        k = np.where(cdv < q, cdv, np.where(cdv < 2 * q, cdv - q, 0))
+        base = np.where(cdv < q, src[rows, k], np.where(cdv < 2 * q, -src[rows, k],
+                        np.where(cdv == 2 * q, 0.0, np.where(cdv == 2 * q + 1, cur[:, d], -cur[:, d]))))
+        out[:, d] = base + rules.cst_np[:, d]
+    return out
+
+
+def apply_rules_device(rules, fout, fin):
+    """Apply compiled rules to device fields of shape (nx, ny, q) (``apply_bc``
+    outside the fused sweep, e.g. to return post-collision populations)."""
+    out = fout.clone()
+    if rules.count == 0:
+        return out
+    q = rules.q
+    cx = torch.as_tensor(rules.cells[:, 0], device=fout.device)
+    cy = torch.as_tensor(rules.cells[:, 1], device=fout.device)
+    cur, src = fout[cx, cy], fin[cx, cy]
+    code = rules.code.view(-1, q).long()
+    k = torch.where(code < q, code, torch.where(code < 2 * q, code - q, torch.zeros_like(code)))
+    s = torch.gather(src, 1, k)
+    base = torch.where(code < q, s, torch.where(code < 2 * q, -s, torch.where(
+        code == 2 * q, torch.zeros_like(s), torch.where(code == 2 * q + 1, cur, -cur))))
+    out[cx, cy] = base + rules.cst.view(-1, q).to(fout.dtype)
+    return out
+
+
+def _self_check(bcs, nx, ny, q, step, names, rules):
+    if rules.count == 0:
+        return
+    rng = np.random.default_rng(1234)
+    fout = rng.standard_normal((nx, ny, q))
+    fin = rng.standard_normal((nx, ny, q))
+    ref = _run(bcs, fout.copy(), fin, step, names)
+    cx, cy = rules.cells[:, 0], rules.cells[:, 1]
+    got = evaluate_rules(rules, fout[cx, cy], fin[cx, cy])
+    scale = max(1.0, float(np.abs(ref[cx, cy]).max()))
+    if not np.allclose(got, ref[cx, cy], rtol=0, atol=1e-12 * scale):
+        raise NotImplementedError("boundary conditions are not cell-local affine maps; cannot compile them")
+    mask = np.ones((nx, ny), dtype=bool)
+    mask[cx, cy] = False
+    if not np.array_equal(ref[mask], fout[mask]):
+        raise NotImplementedError("boundary conditions modify cells outside their index sets")

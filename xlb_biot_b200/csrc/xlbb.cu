@@ -1,0 +1,728 @@
+// xlbb: B200 (sm_100a) kernels of the lattice-Boltzmann Biot hot path and
+// their C ABI (include/xlbb.h).  Reference: s-lunowa/xlb-biot src/elasticity.py,
+// src/darcy.py, src/poroelasticity.py.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+#include <string>
+
+#include "xlbb.h"
+#include "xlbb_common.cuh"
+#include "xlbb_sweep.cuh"
+
+namespace xlbb {
+
+static thread_local std::string g_last_error;
+
+static int fail(int code, const char* msg) {
+    g_last_error = msg;
+    return code;
+}
+
+static int check_launch(const char* what) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
+        return XLBB_ELAUNCH;
+    }
+    return XLBB_OK;
+}
+
+static bool grid_ok(const XlbbGrid* g) {
+    return g && g->nx > 0 && g->ny > 0 && g->pitch >= g->nx && g->plane >= (long long)g->pitch * g->ny;
+}
+
+static int g_num_sms = 0;
+static int num_sms() {
+    if (g_num_sms == 0) {
+        int dev = 0, n = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        g_num_sms = n > 0 ? n : 148;
+    }
+    return g_num_sms;
+}
+
+template <typename T, int Q>
+static RulesView<T, Q> rules_view(const XlbbRules& r) {
+    RulesView<T, Q> v;
+    v.count = r.row_ptr ? r.count : 0;
+    v.row_ptr = r.row_ptr;
+    v.cell_x = r.cell_x;
+    v.code = r.code;
+    v.cst = static_cast<const T*>(r.cst);
+    return v;
+}
+
+// ---------------------------------------------------------------------------
+// D2Q8 elasticity (src/elasticity.py:805-848 transfer matrices, :959-1000
+// collision, :1002-1058 moments).
+// ---------------------------------------------------------------------------
+template <typename T>
+struct ElastMat {
+    T cs, cd, h, n;   // uniform relaxation rates and m_to_f coefficients
+    const T* lam_f;   // optional per-cell Lame fields
+    const T* mu_f;
+};
+
+template <typename T>
+__host__ __device__ inline void elast_rates(T lam, T mu, T& cs, T& cd, T& h, T& n) {
+    // src/elasticity.py:810-813, :829-830, :973-974
+    T g = T(1.0) / (T(12.0) * (lam + mu) - T(4.0));
+    if (g > T(100) || g < T(-100)) g = T(0);
+    h = T(0.25) + T(0.5) * g;
+    n = T(-0.25) * g;
+    cs = (T(3) * (lam + mu) - T(1)) / (T(3) * (lam + mu) + T(1));
+    cd = (T(6) * mu - T(1)) / (T(6) * mu + T(1));
+}
+
+template <typename T>
+__device__ __forceinline__ void elast_collide(const T (&f)[8], bool hasF, T F0, T F1, T cs, T cd, T h, T n,
+                                              T (&o)[8]) {
+    const T m0 = f[0] - f[2] + f[4] - f[5] - f[6] + f[7];
+    const T m1 = f[1] - f[3] + f[4] + f[5] - f[6] - f[7];
+    const T m2 = f[0] + f[1] + f[2] + f[3] + T(2) * (f[4] + f[5] + f[6] + f[7]);
+    const T m3 = f[0] - f[1] + f[2] - f[3];
+    const T m4 = f[4] - f[5] + f[6] - f[7];
+    T M0 = m0, M1 = m1, M5 = m0 / T(3), M6 = m1 / T(3);
+    if (hasF) {
+        M0 = m0 + F0;
+        M1 = m1 + F1;
+        M5 = m0 / T(3) + F0 / T(6);
+        M6 = m1 / T(3) + F1 / T(6);
+    }
+    const T M2 = m2 * cs, M3 = m3 * cd, M4 = m4 * cd;
+    o[0] = T(0.5) * M0 + h * M2 + T(0.25) * M3 - T(0.5) * M5;
+    o[1] = T(0.5) * M1 + h * M2 - T(0.25) * M3 - T(0.5) * M6;
+    o[2] = T(-0.5) * M0 + h * M2 + T(0.25) * M3 + T(0.5) * M5;
+    o[3] = T(-0.5) * M1 + h * M2 - T(0.25) * M3 + T(0.5) * M6;
+    o[4] = n * M2 + T(0.25) * M4 + T(0.25) * M5 + T(0.25) * M6;
+    o[5] = n * M2 - T(0.25) * M4 - T(0.25) * M5 + T(0.25) * M6;
+    o[6] = n * M2 + T(0.25) * M4 - T(0.25) * M5 - T(0.25) * M6;
+    o[7] = n * M2 - T(0.25) * M4 + T(0.25) * M5 - T(0.25) * M6;
+}
+
+template <typename T_, bool RESID>
+struct ElastPhys {
+    using T = T_;
+    static constexpr int Q = 8;
+    __host__ __device__ static constexpr int cx(int i) { return cx8(i); }
+    __host__ __device__ static constexpr int cy(int i) { return cy8(i); }
+    struct Args {
+        SweepGeom geom;
+        const T* f_in;
+        T* f_out;
+        const T* force;
+        const T* fext;
+        const T* resid;
+        T a, b;
+        ElastMat<T> mat;
+        RulesView<T, 8> pc, ps;
+        double* sumsq;
+        int bx0, bx1, by0, by1;
+        T* div_out;
+        T div_scale;
+        int mix;   // 0: out = S; 1: out = a f + b S
+    };
+    struct In {
+        T f[8];
+        T r[RESID ? 8 : 1];
+        T F0, F1;
+    };
+    __device__ static void load(const Args& p, int y, int x, In& in) {
+        const size_t o = (size_t)y * p.geom.pitch + x;
+        const long long P = p.geom.plane;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) in.f[i] = __ldg(p.f_in + o + i * P);
+        if (RESID) {
+#pragma unroll
+            for (int i = 0; i < 8; ++i) in.r[i] = __ldg(p.resid + o + i * P);
+        }
+        T F0 = T(0), F1 = T(0);
+        if (p.force) { F0 = __ldg(p.force + o); F1 = __ldg(p.force + o + P); }
+        if (p.fext) {
+            const T e0 = __ldg(p.fext + o), e1 = __ldg(p.fext + o + P);
+            if (p.force) { F0 = F0 + e0; F1 = F1 + e1; } else { F0 = e0; F1 = e1; }
+        }
+        in.F0 = F0;
+        in.F1 = F1;
+    }
+    __device__ static void fin(const In& in, T (&g)[8]) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) g[i] = RESID ? in.f[i] - in.r[i] : in.f[i];
+    }
+    __device__ static T f_in(const In& in, int i) { return in.f[i]; }
+    __device__ static void collide(const Args& p, int y, int x, const In& in, T (&o)[8]) {
+        T g[8];
+        fin(in, g);
+        T cs = p.mat.cs, cd = p.mat.cd, h = p.mat.h, n = p.mat.n;
+        if (p.mat.mu_f) {
+            const size_t c = (size_t)y * p.geom.pitch + x;
+            elast_rates<T>(__ldg(p.mat.lam_f + c), __ldg(p.mat.mu_f + c), cs, cd, h, n);
+        }
+        elast_collide<T>(g, p.force != nullptr || p.fext != nullptr, in.F0, in.F1, cs, cd, h, n, o);
+    }
+    template <bool PREV>
+    __device__ static double store(const Args& p, int y, int x, T (&S)[8], const T* fprev) {
+        const size_t o = (size_t)y * p.geom.pitch + x;
+        const long long P = p.geom.plane;
+        double acc = 0.0;
+        T m2 = T(0);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            T v = S[i];
+            if constexpr (PREV) v = p.a * fprev[i] + p.b * S[i];
+            p.f_out[o + i * P] = v;
+            acc += (double)v * (double)v;
+            m2 += (i < 4 ? T(1) : T(2)) * v;
+        }
+        if (p.div_out) p.div_out[o] = p.div_scale * m2;
+        const bool in_box = x >= p.bx0 && x < p.bx1 && y >= p.by0 && y < p.by1;
+        return in_box ? acc : 0.0;
+    }
+};
+
+// ---------------------------------------------------------------------------
+// D2Q9 advection-diffusion-reaction BGK (src/darcy.py:106-129).
+// ---------------------------------------------------------------------------
+template <typename T_>
+struct DarcyPhys {
+    using T = T_;
+    static constexpr int Q = 9;
+    __host__ __device__ static constexpr int cx(int i) { return cx9(i); }
+    __host__ __device__ static constexpr int cy(int i) { return cy9(i); }
+    struct Args {
+        SweepGeom geom;
+        const T* f_in;
+        T* f_out;
+        T omega;
+        const T* omega_f;
+        const T* source;
+        const T* ext;
+        RulesView<T, 9> pc, ps;
+        double* sumsq;
+    };
+    struct In {
+        T f[9];
+        T S;
+        T om;
+    };
+    __device__ static void load(const Args& p, int y, int x, In& in) {
+        const size_t o = (size_t)y * p.geom.pitch + x;
+        const long long P = p.geom.plane;
+#pragma unroll
+        for (int i = 0; i < 9; ++i) in.f[i] = __ldg(p.f_in + o + i * P);
+        T S = T(0);
+        if (p.source) S = __ldg(p.source + o);
+        if (p.ext) S = p.source ? S + __ldg(p.ext + o) : __ldg(p.ext + o);
+        in.S = S;
+        in.om = p.omega_f ? __ldg(p.omega_f + o) : p.omega;
+    }
+    __device__ static void fin(const In& in, T (&g)[9]) {
+#pragma unroll
+        for (int i = 0; i < 9; ++i) g[i] = in.f[i];
+    }
+    __device__ static T f_in(const In& in, int i) { return in.f[i]; }
+    __device__ static void collide(const Args& p, int, int, const In& in, T (&o)[9]) {
+        const bool hasS = p.source != nullptr || p.ext != nullptr;
+        T rho = in.f[0];
+#pragma unroll
+        for (int i = 1; i < 9; ++i) rho += in.f[i];
+        if (hasS) rho = rho + T(0.5) * in.S;
+        const T om = in.om;
+        const T sf = T(1) - T(0.5) * om;
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            const T feq = rho * w9<T>(i);
+            T v = in.f[i] - om * (in.f[i] - feq);
+            if (hasS) v = v + in.S * (sf * w9<T>(i));
+            o[i] = v;
+        }
+    }
+    template <bool PREV>
+    __device__ static double store(const Args& p, int y, int x, T (&S)[9], const T* fprev) {
+        const size_t o = (size_t)y * p.geom.pitch + x;
+        const long long P = p.geom.plane;
+        double acc = 0.0;
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            p.f_out[o + i * P] = S[i];
+            if constexpr (PREV) {
+                const double d = (double)S[i] - (double)fprev[i];
+                acc += d * d;
+            }
+        }
+        return acc;
+    }
+};
+
+// Launch geometry of the sweeps: TX owned columns per CTA, strips of rows
+// chosen so that the grid holds about `waves` CTAs per SM.
+static constexpr int SWEEP_TX = 128;
+
+static dim3 sweep_grid(const XlbbGrid* g, int tx) {
+    const int nbx = (g->nx + tx - 1) / tx;
+    const int target = 6 * num_sms();
+    int nby = target / nbx;
+    const int max_by = g->ny / 8 > 0 ? g->ny / 8 : 1;   // strips of >= 8 rows
+    if (nby > max_by) nby = max_by;
+    if (nby < 1) nby = 1;
+    if (nby > g->ny) nby = g->ny;
+    return dim3(nbx, nby);
+}
+
+// ---------------------------------------------------------------------------
+// Small kernels: gradient, moments, equilibrium, transfers, reductions.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void gradient_kernel(SweepGeom G, const T* q, T scale, RulesView<T, 9> rules, const T* base, T* out) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    if (x >= G.nx) return;
+    T v[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+        const int xs = wrap(x - cx9(i), G.nx), ys = wrap(y - cy9(i), G.ny);
+        v[i] = __ldg(q + (size_t)ys * G.pitch + xs);
+    }
+    const size_t o = (size_t)y * G.pitch + x;
+    const int r = find_rule(rules, y, x);
+    if (r >= 0) {
+        const T qc = __ldg(q + o);   // every direction of the tiled input is q(x)
+#pragma unroll
+        for (int d = 0; d < 9; ++d) {
+            const uint8_t code = __ldg(rules.code + (size_t)r * 9 + d);
+            v[d] = rule_value<T, 9>(code, v[d], qc, rules.cst[(size_t)r * 9 + d]);
+        }
+    }
+    // src/darcy.py:104: sum_i p_i * (-3 * scale * w_i * c_i)
+    T gx = T(0), gy = T(0);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+        const T k = T(-3) * scale * w9<T>(i);
+        gx += v[i] * (k * T(cx9(i)));
+        gy += v[i] * (k * T(cy9(i)));
+    }
+    if (base) {
+        gx = base[o] + gx;
+        gy = base[o + G.plane] + gy;
+    }
+    out[o] = gx;
+    out[o + G.plane] = gy;
+}
+
+template <typename T>
+__global__ void elast_moments_kernel(SweepGeom G, ElastMat<T> mat, T lam, T mu, const T* f, const T* force,
+                                     const T* fext, T* eta, T* sigma, T* div, T div_scale) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    if (x >= G.nx) return;
+    const size_t o = (size_t)y * G.pitch + x;
+    const long long P = G.plane;
+    T v[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) v[i] = f[o + i * P];
+    const T m0 = v[0] - v[2] + v[4] - v[5] - v[6] + v[7];
+    const T m1 = v[1] - v[3] + v[4] + v[5] - v[6] - v[7];
+    const T m2 = v[0] + v[1] + v[2] + v[3] + T(2) * (v[4] + v[5] + v[6] + v[7]);
+    const T m3 = v[0] - v[1] + v[2] - v[3];
+    const T m4 = v[4] - v[5] + v[6] - v[7];
+    T l = lam, m = mu;
+    if (mat.mu_f) { l = mat.lam_f[o]; m = mat.mu_f[o]; }
+    if (eta) {
+        T e0 = m0, e1 = m1;
+        if (force) { e0 = e0 + T(0.5) * force[o]; e1 = e1 + T(0.5) * force[o + P]; }
+        if (fext) { e0 = e0 + T(0.5) * fext[o]; e1 = e1 + T(0.5) * fext[o + P]; }
+        eta[o] = e0;
+        eta[o + P] = e1;
+    }
+    if (sigma) {
+        const T cs = T(-1.5) * (l + m) / (T(3) * (l + m) + T(1));
+        const T cd = T(-3) * m / (T(6) * m + T(1));
+        const T ms = m2 * cs, md = m3 * cd;
+        sigma[o] = ms + md;
+        sigma[o + P] = (T(2) * cd) * m4;
+        sigma[o + 2 * P] = ms - md;
+    }
+    if (div) {
+        const T c = mat.mu_f ? T(-1.5) / (T(3) * (l + m) + T(1)) : div_scale;
+        div[o] = c * m2;
+    }
+}
+
+template <typename T>
+__global__ void elast_equilibrium_kernel(SweepGeom G, T lam, T mu, const T* lam_f, const T* mu_f, const T* eta,
+                                         const T* sigma, const T* force, const T* fext, T* fo) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    if (x >= G.nx) return;
+    const size_t o = (size_t)y * G.pitch + x;
+    const long long P = G.plane;
+    T l = lam, m = mu;
+    if (mu_f) { l = lam_f[o]; m = mu_f[o]; }
+    T h, n, cs_, cd_;
+    elast_rates<T>(l, m, cs_, cd_, h, n);
+    T e0 = eta[o], e1 = eta[o + P];
+    if (force) { e0 = e0 - T(0.5) * force[o]; e1 = e1 - T(0.5) * force[o + P]; }
+    if (fext) { e0 = e0 - T(0.5) * fext[o]; e1 = e1 - T(0.5) * fext[o + P]; }
+    const T cs = T(-1) - T(1) / (T(3) * (l + m));
+    const T cd = T(-1) - T(1) / (T(6) * m);
+    const T s0 = sigma[o], s1 = sigma[o + P], s2 = sigma[o + 2 * P];
+    const T M0 = e0, M1 = e1, M2 = (s0 + s2) * cs, M3 = (s0 - s2) * cd, M4 = s1 * cd;
+    const T M5 = e0 / T(3), M6 = e1 / T(3);
+    fo[o] = T(0.5) * M0 + h * M2 + T(0.25) * M3 - T(0.5) * M5;
+    fo[o + P] = T(0.5) * M1 + h * M2 - T(0.25) * M3 - T(0.5) * M6;
+    fo[o + 2 * P] = T(-0.5) * M0 + h * M2 + T(0.25) * M3 + T(0.5) * M5;
+    fo[o + 3 * P] = T(-0.5) * M1 + h * M2 - T(0.25) * M3 + T(0.5) * M6;
+    fo[o + 4 * P] = n * M2 + T(0.25) * M4 + T(0.25) * M5 + T(0.25) * M6;
+    fo[o + 5 * P] = n * M2 - T(0.25) * M4 - T(0.25) * M5 + T(0.25) * M6;
+    fo[o + 6 * P] = n * M2 + T(0.25) * M4 - T(0.25) * M5 - T(0.25) * M6;
+    fo[o + 7 * P] = n * M2 - T(0.25) * M4 + T(0.25) * M5 - T(0.25) * M6;
+}
+
+template <typename T>
+__global__ void darcy_moments_kernel(SweepGeom G, const T* f, T omega, const T* omega_f, const T* src,
+                                     const T* ext, T* rho, T* grad) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    if (x >= G.nx) return;
+    const size_t o = (size_t)y * G.pitch + x;
+    const long long P = G.plane;
+    T v[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) v[i] = f[o + i * P];
+    if (rho) {
+        T s = v[0];
+#pragma unroll
+        for (int i = 1; i < 9; ++i) s += v[i];
+        if (src && ext) s = s + T(0.5) * (src[o] + ext[o]);
+        else if (src) s = s + T(0.5) * src[o];
+        else if (ext) s = s + T(0.5) * ext[o];
+        rho[o] = s;
+    }
+    if (grad) {
+        const T k = T(-3) * (omega_f ? omega_f[o] : omega);
+        T gx = T(0), gy = T(0);
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            gx += v[i] * (k * T(cx9(i)));
+            gy += v[i] * (k * T(cy9(i)));
+        }
+        grad[o] = gx;
+        grad[o + P] = gy;
+    }
+}
+
+template <typename T>
+__global__ void restrict_kernel(SweepGeom F, SweepGeom C, int q, int x0, int y0, int nix, int niy, const T* res,
+                                T* rc) {
+    // one thread per coarse cell (all q planes); zero outside the coarse interior
+    const int X = blockIdx.x * blockDim.x + threadIdx.x;
+    const int Y = blockIdx.y;
+    if (X >= C.nx) return;
+    const size_t oc = (size_t)Y * C.pitch + X;
+    const int I = X - x0, J = Y - y0;
+    const bool inside = I >= 0 && I < nix && J >= 0 && J < niy;
+    for (int i = 0; i < q; ++i) {
+        T v = T(0);
+        if (inside) {
+            const size_t of = (size_t)(y0 + 2 * J) * F.pitch + (x0 + 2 * I) + (size_t)i * F.plane;
+            const T a = res[of], b = res[of + 1], c = res[of + F.pitch], d = res[of + F.pitch + 1];
+            v = a + c + b + d;   // conv window order (x, y): (0,0),(0,1),(1,0),(1,1) summed pairwise in y first
+        }
+        rc[oc + (size_t)i * C.plane] = v;
+    }
+}
+
+template <typename T>
+__global__ void prolong_add_kernel(SweepGeom F, SweepGeom C, int q, int x0, int y0, int nfx, int nfy,
+                                   const T* fc, T* ff) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    if (i >= nfx || j >= nfy) return;
+    const size_t of = (size_t)(y0 + j) * F.pitch + (x0 + i);
+    const size_t oc = (size_t)(y0 + j / 2) * C.pitch + (x0 + i / 2);
+    for (int k = 0; k < q; ++k) ff[of + (size_t)k * F.plane] += fc[oc + (size_t)k * C.plane];
+}
+
+template <typename T>
+__global__ void sumsq_kernel(SweepGeom G, int nplanes, const T* d, int bx0, int bx1, int by0, int by1,
+                             double* partials) {
+    __shared__ double red[8];
+    double acc = 0.0;
+    const long long n = (long long)(bx1 - bx0) * (by1 - by0);
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const int y = by0 + (int)(e / (bx1 - bx0));
+        const int x = bx0 + (int)(e % (bx1 - bx0));
+        const size_t o = (size_t)y * G.pitch + x;
+        for (int i = 0; i < nplanes; ++i) {
+            const double v = (double)d[o + (size_t)i * G.plane];
+            acc += v * v;
+        }
+    }
+    const double s = block_sum(acc, red);
+    if (threadIdx.x == 0) partials[blockIdx.x] = s;
+}
+
+__global__ void reduce_sum_kernel(const double* p, int n, double* out) {
+    __shared__ double red[32];
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) acc += p[i];
+    const double s = block_sum(acc, red);
+    if (threadIdx.x == 0) *out = s;
+}
+
+template <typename T>
+__global__ void axpby_kernel(long long n, T a, const T* x, T b, const T* y, T* o) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        o[i] = a * x[i] + b * y[i];
+}
+
+static SweepGeom geom(const XlbbGrid* g) { return SweepGeom{g->nx, g->ny, g->pitch, g->plane}; }
+
+template <typename T>
+static ElastMat<T> make_mat(const XlbbElastMaterial* m) {
+    ElastMat<T> e;
+    elast_rates<T>(T(m->lam), T(m->mu), e.cs, e.cd, e.h, e.n);
+    e.lam_f = static_cast<const T*>(m->lam_field);
+    e.mu_f = static_cast<const T*>(m->mu_field);
+    return e;
+}
+
+template <typename T, bool RESID, bool PREV>
+static int launch_elast(const XlbbGrid* g, const XlbbElastMaterial* mat, const XlbbElastSweep* s, cudaStream_t st) {
+    using Ph = ElastPhys<T, RESID>;
+    typename Ph::Args a;
+    a.geom = geom(g);
+    a.f_in = static_cast<const T*>(s->f_in);
+    a.f_out = static_cast<T*>(s->f_out);
+    a.force = s->use_force ? static_cast<const T*>(s->force) : nullptr;
+    a.fext = static_cast<const T*>(s->fext);
+    a.resid = static_cast<const T*>(s->resid);
+    a.a = T(s->a);
+    a.b = T(s->b);
+    a.mix = PREV ? 1 : 0;
+    a.mat = make_mat<T>(mat);
+    a.pc = rules_view<T, 8>(s->pc);
+    a.ps = rules_view<T, 8>(s->ps);
+    a.sumsq = s->sumsq;
+    a.bx0 = s->bx0; a.bx1 = s->bx1; a.by0 = s->by0; a.by1 = s->by1;
+    a.div_out = static_cast<T*>(s->div_out);
+    a.div_scale = T(-1.5 / (3.0 * (mat->lam + mat->mu) + 1.0));
+    const dim3 grid = sweep_grid(g, SWEEP_TX);
+    sweep_kernel<Ph, SWEEP_TX, PREV><<<grid, SWEEP_TX + 32, 0, st>>>(a);
+    return check_launch("xlbb_elast_sweep");
+}
+
+template <typename T>
+static int elast_sweep_t(const XlbbGrid* g, const XlbbElastMaterial* mat, const XlbbElastSweep* s, cudaStream_t st) {
+    const bool mix = !(s->a == 0.0 && s->b == 1.0);
+    if (s->resid) return mix ? launch_elast<T, true, true>(g, mat, s, st) : launch_elast<T, true, false>(g, mat, s, st);
+    return mix ? launch_elast<T, false, true>(g, mat, s, st) : launch_elast<T, false, false>(g, mat, s, st);
+}
+
+template <typename T>
+static int darcy_sweep_t(const XlbbGrid* g, const XlbbDarcySweep* s, cudaStream_t st) {
+    using Ph = DarcyPhys<T>;
+    typename Ph::Args a;
+    a.geom = geom(g);
+    a.f_in = static_cast<const T*>(s->f_in);
+    a.f_out = static_cast<T*>(s->f_out);
+    a.omega = T(s->omega);
+    a.omega_f = static_cast<const T*>(s->omega_field);
+    a.source = static_cast<const T*>(s->source);
+    a.ext = static_cast<const T*>(s->ext_source);
+    a.pc = rules_view<T, 9>(s->pc);
+    a.ps = rules_view<T, 9>(s->ps);
+    a.sumsq = s->sumsq;
+    const dim3 grid = sweep_grid(g, SWEEP_TX);
+    if (s->sumsq) sweep_kernel<Ph, SWEEP_TX, true><<<grid, SWEEP_TX + 32, 0, st>>>(a);
+    else sweep_kernel<Ph, SWEEP_TX, false><<<grid, SWEEP_TX + 32, 0, st>>>(a);
+    return check_launch("xlbb_darcy_sweep");
+}
+
+static inline dim3 row_grid(int nx, int ny, int bs) { return dim3((nx + bs - 1) / bs, ny); }
+
+}  // namespace xlbb
+
+using namespace xlbb;
+
+#define XLBB_STREAM(s) (static_cast<cudaStream_t>(s))
+
+extern "C" {
+
+int xlbb_version(void) { return 100; }
+
+const char* xlbb_last_error(void) { return g_last_error.c_str(); }
+
+int xlbb_elast_sweep_ctas(const XlbbGrid* g) {
+    if (!grid_ok(g)) return fail(XLBB_EBADARG, "xlbb_elast_sweep_ctas: bad grid");
+    const dim3 d = sweep_grid(g, SWEEP_TX);
+    return (int)(d.x * d.y);
+}
+
+int xlbb_darcy_sweep_ctas(const XlbbGrid* g) { return xlbb_elast_sweep_ctas(g); }
+
+int xlbb_elast_sweep(int dtype, const XlbbGrid* g, const XlbbElastMaterial* mat, const XlbbElastSweep* s,
+                     void* stream) {
+    if (!grid_ok(g) || !mat || !s || !s->f_in || !s->f_out) return fail(XLBB_EBADARG, "xlbb_elast_sweep: bad argument");
+    if (s->f_in == s->f_out) return fail(XLBB_EBADARG, "xlbb_elast_sweep: f_in and f_out must differ");
+    if ((mat->mu_field == nullptr) != (mat->lam_field == nullptr))
+        return fail(XLBB_EBADARG, "xlbb_elast_sweep: lam_field and mu_field go together");
+    if (dtype == XLBB_F32) return elast_sweep_t<float>(g, mat, s, XLBB_STREAM(stream));
+    if (dtype == XLBB_F64) return elast_sweep_t<double>(g, mat, s, XLBB_STREAM(stream));
+    return fail(XLBB_EUNSUPPORTED, "xlbb_elast_sweep: dtype");
+}
+
+int xlbb_darcy_sweep(int dtype, const XlbbGrid* g, const XlbbDarcySweep* s, void* stream) {
+    if (!grid_ok(g) || !s || !s->f_in || !s->f_out) return fail(XLBB_EBADARG, "xlbb_darcy_sweep: bad argument");
+    if (s->f_in == s->f_out) return fail(XLBB_EBADARG, "xlbb_darcy_sweep: f_in and f_out must differ");
+    if (dtype == XLBB_F32) return darcy_sweep_t<float>(g, s, XLBB_STREAM(stream));
+    if (dtype == XLBB_F64) return darcy_sweep_t<double>(g, s, XLBB_STREAM(stream));
+    return fail(XLBB_EUNSUPPORTED, "xlbb_darcy_sweep: dtype");
+}
+
+int xlbb_darcy_gradient(int dtype, const XlbbGrid* g, const void* q, double scale, const XlbbRules* rules,
+                        const void* base, void* out, void* stream) {
+    if (!grid_ok(g) || !q || !out) return fail(XLBB_EBADARG, "xlbb_darcy_gradient: bad argument");
+    XlbbRules none = {0, nullptr, nullptr, nullptr, nullptr};
+    const XlbbRules& r = rules ? *rules : none;
+    const dim3 grid = row_grid(g->nx, g->ny, 128);
+    if (dtype == XLBB_F32)
+        gradient_kernel<float><<<grid, 128, 0, XLBB_STREAM(stream)>>>(geom(g), (const float*)q, (float)scale,
+                                                                      rules_view<float, 9>(r), (const float*)base, (float*)out);
+    else if (dtype == XLBB_F64)
+        gradient_kernel<double><<<grid, 128, 0, XLBB_STREAM(stream)>>>(geom(g), (const double*)q, scale,
+                                                                       rules_view<double, 9>(r), (const double*)base, (double*)out);
+    else return fail(XLBB_EUNSUPPORTED, "xlbb_darcy_gradient: dtype");
+    return check_launch("xlbb_darcy_gradient");
+}
+
+int xlbb_elast_moments(int dtype, const XlbbGrid* g, const XlbbElastMaterial* mat, const void* f, const void* force,
+                       const void* fext, void* eta, void* sigma, void* div, double div_scale, void* stream) {
+    if (!grid_ok(g) || !mat || !f) return fail(XLBB_EBADARG, "xlbb_elast_moments: bad argument");
+    const dim3 grid = row_grid(g->nx, g->ny, 128);
+    if (dtype == XLBB_F32)
+        elast_moments_kernel<float><<<grid, 128, 0, XLBB_STREAM(stream)>>>(
+            geom(g), make_mat<float>(mat), (float)mat->lam, (float)mat->mu, (const float*)f, (const float*)force,
+            (const float*)fext, (float*)eta, (float*)sigma, (float*)div, (float)div_scale);
+    else if (dtype == XLBB_F64)
+        elast_moments_kernel<double><<<grid, 128, 0, XLBB_STREAM(stream)>>>(
+            geom(g), make_mat<double>(mat), mat->lam, mat->mu, (const double*)f, (const double*)force,
+            (const double*)fext, (double*)eta, (double*)sigma, (double*)div, div_scale);
+    else return fail(XLBB_EUNSUPPORTED, "xlbb_elast_moments: dtype");
+    return check_launch("xlbb_elast_moments");
+}
+
+int xlbb_elast_equilibrium(int dtype, const XlbbGrid* g, const XlbbElastMaterial* mat, const void* eta,
+                           const void* sigma, const void* force, const void* fext, void* f_out, void* stream) {
+    if (!grid_ok(g) || !mat || !eta || !sigma || !f_out) return fail(XLBB_EBADARG, "xlbb_elast_equilibrium: bad argument");
+    const dim3 grid = row_grid(g->nx, g->ny, 128);
+    if (dtype == XLBB_F32)
+        elast_equilibrium_kernel<float><<<grid, 128, 0, XLBB_STREAM(stream)>>>(
+            geom(g), (float)mat->lam, (float)mat->mu, (const float*)mat->lam_field, (const float*)mat->mu_field,
+            (const float*)eta, (const float*)sigma, (const float*)force, (const float*)fext, (float*)f_out);
+    else if (dtype == XLBB_F64)
+        elast_equilibrium_kernel<double><<<grid, 128, 0, XLBB_STREAM(stream)>>>(
+            geom(g), mat->lam, mat->mu, (const double*)mat->lam_field, (const double*)mat->mu_field,
+            (const double*)eta, (const double*)sigma, (const double*)force, (const double*)fext, (double*)f_out);
+    else return fail(XLBB_EUNSUPPORTED, "xlbb_elast_equilibrium: dtype");
+    return check_launch("xlbb_elast_equilibrium");
+}
+
+int xlbb_darcy_moments(int dtype, const XlbbGrid* g, const void* f, double omega, const void* omega_field,
+                       const void* source, const void* ext_source, void* rho, void* grad, void* stream) {
+    if (!grid_ok(g) || !f) return fail(XLBB_EBADARG, "xlbb_darcy_moments: bad argument");
+    const dim3 grid = row_grid(g->nx, g->ny, 128);
+    if (dtype == XLBB_F32)
+        darcy_moments_kernel<float><<<grid, 128, 0, XLBB_STREAM(stream)>>>(
+            geom(g), (const float*)f, (float)omega, (const float*)omega_field, (const float*)source,
+            (const float*)ext_source, (float*)rho, (float*)grad);
+    else if (dtype == XLBB_F64)
+        darcy_moments_kernel<double><<<grid, 128, 0, XLBB_STREAM(stream)>>>(
+            geom(g), (const double*)f, omega, (const double*)omega_field, (const double*)source,
+            (const double*)ext_source, (double*)rho, (double*)grad);
+    else return fail(XLBB_EUNSUPPORTED, "xlbb_darcy_moments: dtype");
+    return check_launch("xlbb_darcy_moments");
+}
+
+int xlbb_restrict(int dtype, const XlbbGrid* fine, const XlbbGrid* coarse, int q, int x0, int x1bc, int y0, int y1bc,
+                  const void* res, void* r_coarse, void* stream) {
+    if (!grid_ok(fine) || !grid_ok(coarse) || !res || !r_coarse || q <= 0)
+        return fail(XLBB_EBADARG, "xlbb_restrict: bad argument");
+    const int nfx = fine->nx - x0 - x1bc, nfy = fine->ny - y0 - y1bc;
+    if (nfx % 2 || nfy % 2 || coarse->nx != nfx / 2 + x0 + x1bc || coarse->ny != nfy / 2 + y0 + y1bc)
+        return fail(XLBB_EBADARG, "xlbb_restrict: coarse grid does not match the fine interior");
+    const dim3 grid = row_grid(coarse->nx, coarse->ny, 128);
+    if (dtype == XLBB_F32)
+        restrict_kernel<float><<<grid, 128, 0, XLBB_STREAM(stream)>>>(geom(fine), geom(coarse), q, x0, y0, nfx / 2,
+                                                                      nfy / 2, (const float*)res, (float*)r_coarse);
+    else if (dtype == XLBB_F64)
+        restrict_kernel<double><<<grid, 128, 0, XLBB_STREAM(stream)>>>(geom(fine), geom(coarse), q, x0, y0, nfx / 2,
+                                                                       nfy / 2, (const double*)res, (double*)r_coarse);
+    else return fail(XLBB_EUNSUPPORTED, "xlbb_restrict: dtype");
+    return check_launch("xlbb_restrict");
+}
+
+int xlbb_prolong_add(int dtype, const XlbbGrid* fine, const XlbbGrid* coarse, int q, int x0, int x1bc, int y0,
+                     int y1bc, const void* f_coarse, void* f_fine, void* stream) {
+    if (!grid_ok(fine) || !grid_ok(coarse) || !f_coarse || !f_fine || q <= 0)
+        return fail(XLBB_EBADARG, "xlbb_prolong_add: bad argument");
+    const int nfx = fine->nx - x0 - x1bc, nfy = fine->ny - y0 - y1bc;
+    if (nfx % 2 || nfy % 2 || coarse->nx != nfx / 2 + x0 + x1bc || coarse->ny != nfy / 2 + y0 + y1bc)
+        return fail(XLBB_EBADARG, "xlbb_prolong_add: coarse grid does not match the fine interior");
+    const dim3 grid = row_grid(nfx, nfy, 128);
+    if (dtype == XLBB_F32)
+        prolong_add_kernel<float><<<grid, 128, 0, XLBB_STREAM(stream)>>>(geom(fine), geom(coarse), q, x0, y0, nfx, nfy,
+                                                                         (const float*)f_coarse, (float*)f_fine);
+    else if (dtype == XLBB_F64)
+        prolong_add_kernel<double><<<grid, 128, 0, XLBB_STREAM(stream)>>>(geom(fine), geom(coarse), q, x0, y0, nfx, nfy,
+                                                                          (const double*)f_coarse, (double*)f_fine);
+    else return fail(XLBB_EUNSUPPORTED, "xlbb_prolong_add: dtype");
+    return check_launch("xlbb_prolong_add");
+}
+
+int xlbb_sumsq_ctas(const XlbbGrid* g) {
+    (void)g;
+    return 2 * num_sms();
+}
+
+int xlbb_sumsq(int dtype, const XlbbGrid* g, int nplanes, const void* data, int bx0, int bx1, int by0, int by1,
+               double* partials, void* stream) {
+    if (!grid_ok(g) || !data || !partials || nplanes <= 0 || bx0 < 0 || by0 < 0 || bx1 > g->nx || by1 > g->ny ||
+        bx1 <= bx0 || by1 <= by0)
+        return fail(XLBB_EBADARG, "xlbb_sumsq: bad argument");
+    const int nb = xlbb_sumsq_ctas(g);
+    if (dtype == XLBB_F32)
+        sumsq_kernel<float><<<nb, 256, 0, XLBB_STREAM(stream)>>>(geom(g), nplanes, (const float*)data, bx0, bx1, by0,
+                                                                 by1, partials);
+    else if (dtype == XLBB_F64)
+        sumsq_kernel<double><<<nb, 256, 0, XLBB_STREAM(stream)>>>(geom(g), nplanes, (const double*)data, bx0, bx1,
+                                                                  by0, by1, partials);
+    else return fail(XLBB_EUNSUPPORTED, "xlbb_sumsq: dtype");
+    return check_launch("xlbb_sumsq");
+}
+
+int xlbb_reduce_sum(const double* partials, int n, double* out, void* stream) {
+    if (!partials || !out || n <= 0) return fail(XLBB_EBADARG, "xlbb_reduce_sum: bad argument");
+    reduce_sum_kernel<<<1, 1024, 0, XLBB_STREAM(stream)>>>(partials, n, out);
+    return check_launch("xlbb_reduce_sum");
+}
+
+int xlbb_axpby(int dtype, long long n, double a, const void* x, double b, const void* y, void* out, void* stream) {
+    if (n < 0 || (n > 0 && (!x || !y || !out))) return fail(XLBB_EBADARG, "xlbb_axpby: bad argument");
+    if (n == 0) return XLBB_OK;
+    long long nb = (n + 255) / 256;
+    if (nb > 8 * num_sms()) nb = 8 * num_sms();
+    if (dtype == XLBB_F32)
+        axpby_kernel<float><<<(int)nb, 256, 0, XLBB_STREAM(stream)>>>(n, (float)a, (const float*)x, (float)b,
+                                                                      (const float*)y, (float*)out);
+    else if (dtype == XLBB_F64)
+        axpby_kernel<double><<<(int)nb, 256, 0, XLBB_STREAM(stream)>>>(n, a, (const double*)x, b, (const double*)y,
+                                                                       (double*)out);
+    else return fail(XLBB_EUNSUPPORTED, "xlbb_axpby: dtype");
+    return check_launch("xlbb_axpby");
+}
+
+}  // extern "C"

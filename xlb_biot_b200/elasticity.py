@@ -1,0 +1,687 @@
+"""D2Q8 linear-elasticity LBM with geometric multigrid on B200.
+
+Drop-in for ``src/elasticity.py`` of the reference: the class
+``LBMElasticity`` keeps the reference's constructor keywords, validation,
+hooks (``set_boundary_conditions``, ``get_force``,
+``initialize_macroscopic_fields``, ``output_data``) and public methods; the
+three elasticity boundary conditions keep their signatures.  Every sweep runs
+in the fused CUDA kernel ``xlbb_elast_sweep`` (collide + BCs + stream, with the
+multigrid smoother / residual algebra folded in); macroscopic fields, the
+equilibrium and the multigrid transfers have their own kernels.
+"""
+import time
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._common import make_policy, print_parameters, set_precisions, gathered
+from .bc_compile import apply_rules_device, compile_rules
+from .boundary_conditions import (BoundaryCondition, _at_add, _at_set, _take, grid_mask, solid_halo_voxels)
+from .fields import Layout, torch_dtype
+
+
+class LBMElasticity:
+    """``src/elasticity.py:30-1501``."""
+
+    def __init__(self, **kwargs):
+        self.lamda = kwargs.get("lambda")
+        self.mu = kwargs.get("mu")
+        self.nx = kwargs.get("nx")
+        self.ny = kwargs.get("ny")
+        self.nz = kwargs.get("nz")
+        self.mg_BCs = kwargs.get("MG_BCs", {})
+        self.levels = kwargs.get("MG_levels", 1)
+        self.gamma = kwargs.get("MG_relaxation", 0.75)
+        self.k_smooth = kwargs.get("MG_n_smoothing", 2)
+        self.precision = kwargs.get("precision")
+        self.precisionPolicy = make_policy(self.precision)
+        self.lattice = kwargs.get("lattice")
+        self.downsamplingFactor = kwargs.get("downsampling_factor", 1)
+        self.printInfoRate = kwargs.get("print_info_rate", 100)
+        self.ioRate = kwargs.get("io_rate", 0)
+        self.returnFpost = kwargs.get("return_fpost", False)
+        self.computeMLUPS = kwargs.get("compute_MLUPS", False)
+        self.nDevices = 1
+        self.backend = "cuda"
+        if self.computeMLUPS:
+            self.ioRate = 0
+            self.printInfoRate = 0
+        _lib.require_cuda()
+        _lib.lib()
+        self.c, self.q, self.w, self.dim = self.lattice.c, self.lattice.q, self.lattice.w, self.lattice.d
+        self._create_transfer_matrices()
+        self.show_simulation_parameters()
+        self.gridInfo = {"nx": self.nx, "ny": self.ny, "nz": self.nz, "dim": self.lattice.d, "lattice": self.lattice}
+        self.sharding = None
+        self._dtype = torch_dtype(self.precisionPolicy.compute_dtype)
+        self._dcode = _lib.dtype_code(self._dtype)
+        self._layouts = [Layout(*self.grid_size(l), self._dtype) for l in range(self.levels)]
+        self.boundingBoxIndices = self.bounding_box_indices()
+        self._create_boundary_data()
+        force = self.get_force()
+        self.force = self._layouts[0].field(force, 2) if force is not None else None
+        self._mat = _lib.ElastMaterial(float(self.lamda), float(self.mu), None, None)
+        self._lam_field = self._mu_field = None
+        self._div_scale = -1.5 / (3 * (self.lamda + self.mu) + 1)
+        self._partials = torch.empty(max(1, _lib.lib().xlbb_elast_sweep_ctas(self._layouts[0].grid())),
+                                     dtype=torch.float64, device=self._layouts[0].device)
+        self._scalar = torch.empty(1, dtype=torch.float64, device=self._layouts[0].device)
+
+    # ------------------------------------------------------------------ validation
+    @property
+    def lattice(self):
+        return self._lattice
+
+    @lattice.setter
+    def lattice(self, value):
+        if value is None:
+            raise ValueError("Lattice type must be provided.")
+        if self.nz == 0 and value.name not in ["D2Q8"]:
+            raise ValueError("For 2D simulations, lattice type must be LatticeD2Q8.")
+        if self.nz != 0:
+            raise ValueError("3D simulations are not supported.")
+        self._lattice = value
+
+    @property
+    def lamda(self):
+        return self._lamda
+
+    @lamda.setter
+    def lamda(self, value):
+        if value is None:
+            raise ValueError("lambda must be provided")
+        if not isinstance(value, float):
+            raise TypeError("lambda must be a float")
+        self._lamda = value
+
+    @property
+    def mu(self):
+        return self._mu
+
+    @mu.setter
+    def mu(self, value):
+        if value is None:
+            raise ValueError("mu must be provided")
+        if not isinstance(value, float):
+            raise TypeError("mu must be a float")
+        self._mu = value
+
+    @property
+    def levels(self):
+        return self._levels
+
+    @levels.setter
+    def levels(self, value):
+        if value is None:
+            raise ValueError("levels must be provided")
+        if not isinstance(value, int) or value <= 0:
+            raise TypeError("levels must be a positive int")
+        den = 2 ** (value - 1)
+        m = self.mg_BCs
+        if ((self.nx - int(m["left"]) - int(m["right"])) % den != 0
+                or (self.ny - int(m["bottom"]) - int(m["top"])) % den != 0
+                or (self.nz - int(m["front"]) - int(m["back"])) % den != 0):
+            raise ValueError("nx,ny,nz (-BCs) must be divisible by 2**(levels-1)")
+        self._levels = value
+
+    @property
+    def gamma(self):
+        return self._gamma
+
+    @gamma.setter
+    def gamma(self, value):
+        if value is None:
+            raise ValueError("gamma must be provided")
+        if not isinstance(value, float):
+            raise TypeError("gamma must be a float")
+        if value < 0.0 or value > 1.0:
+            raise ValueError("gamma must be between 0 and 1")
+        self._gamma = value
+
+    @property
+    def k_smooth(self):
+        return self._k_smooth
+
+    @k_smooth.setter
+    def k_smooth(self, value):
+        if value is None:
+            raise ValueError("k_smooth must be provided")
+        if not isinstance(value, int):
+            raise TypeError("k_smooth must be an integer")
+        if value < 1:
+            raise ValueError("k_smooth must be positive")
+        self._k_smooth = value
+
+    @property
+    def mg_BCs(self):
+        return self._mg_BCs
+
+    @mg_BCs.setter
+    def mg_BCs(self, value):
+        if not isinstance(value, dict):
+            raise TypeError("mg_BCs must be a dictionary")
+        for key, bc in value.items():
+            if key not in ["left", "right", "bottom", "top", "front", "back"]:
+                raise ValueError(f"Invalid key '{key}' in mg_BCs. Valid keys are 'left', 'right', 'bottom', "
+                                 "'top', 'front', 'back'.")
+            if not isinstance(bc, bool):
+                raise TypeError("All values in mg_BCs must be boolean values")
+        self._mg_BCs = {"left": False, "right": False, "bottom": False, "top": False, "front": False,
+                        "back": False}
+        self._mg_BCs.update(value)
+
+    def _int_prop(name, label):
+        def getter(self):
+            return getattr(self, "_" + name)
+
+        def setter(self, value):
+            if value is None and label in ("nx", "ny", "nz"):
+                raise ValueError(f"{label} must be provided")
+            if not isinstance(value, int) or isinstance(value, bool):
+                raise TypeError(f"{label} must be an integer")
+            setattr(self, "_" + name, value)
+        return property(getter, setter)
+
+    nx = _int_prop("nx", "nx")
+    ny = _int_prop("ny", "ny")
+    nz = _int_prop("nz", "nz")
+    downsamplingFactor = _int_prop("downsamplingFactor", "downsamplingFactor")
+    printInfoRate = _int_prop("printInfoRate", "printInfoRate")
+    ioRate = _int_prop("ioRate", "ioRate")
+    nDevices = _int_prop("nDevices", "nDevices")
+
+    def _bool_prop(name, label):
+        def getter(self):
+            return getattr(self, "_" + name)
+
+        def setter(self, value):
+            if not isinstance(value, bool):
+                raise TypeError(f"{label} must be a boolean")
+            setattr(self, "_" + name, value)
+        return property(getter, setter)
+
+    returnFpost = _bool_prop("returnFpost", "returnFpost")
+    computeMLUPS = _bool_prop("computeMLUPS", "computeMLUPS")
+    del _int_prop, _bool_prop
+
+    @property
+    def precision(self):
+        return self._precision
+
+    @precision.setter
+    def precision(self, value):
+        if not isinstance(value, str):
+            raise TypeError("precision must be a string")
+        self._precision = value
+
+    def show_simulation_parameters(self):
+        attrs = ['lamda', 'mu', 'nx', 'ny', 'nz', 'dim', 'levels', 'gamma', 'k_smooth', 'precision', 'lattice',
+                 'downsamplingFactor', 'printInfoRate', 'ioRate', 'computeMLUPS', 'backend', 'nDevices']
+        names = {'lamda': 'Lambda', 'mu': 'Mu', 'nx': 'Grid Points in X', 'ny': 'Grid Points in Y',
+                 'nz': 'Grid Points in Z', 'dim': 'Dimensionality', 'levels': 'Multigrid levels',
+                 'gamma': 'Multigrid relaxation factor', 'k_smooth': 'Multigrid smoothing steps',
+                 'precision': 'Precision Policy', 'lattice': 'Lattice Type',
+                 'downsamplingFactor': 'Downsampling Factor', 'printInfoRate': 'Print Info Rate',
+                 'ioRate': 'I/O Rate', 'computeMLUPS': 'Compute MLUPS', 'backend': 'Backend',
+                 'nDevices': 'Number of Devices'}
+        print_parameters(self, attrs, names)
+
+    # ------------------------------------------------------------------ set-up
+    def set_precisions(self, precision):
+        return set_precisions(precision)
+
+    def _create_transfer_matrices(self):
+        """``:805-848`` (kept for API parity; the kernels hard-code the same matrices)."""
+        g = 1.0 / (12.0 * (self.lamda + self.mu) - 4.0)
+        if abs(g) > 100:
+            print("Warning: scaling value is too large. Reset last moment to default. Boundary conditions may fail.")
+            g = 0.0
+        dt = self.precisionPolicy.compute_dtype
+        self.f_to_m = np.array([[1, 0, -1, 0, 1, -1, -1, 1], [0, 1, 0, -1, 1, 1, -1, -1],
+                                [1, 1, 1, 1, 2, 2, 2, 2], [1, -1, 1, -1, 0, 0, 0, 0],
+                                [0, 0, 0, 0, 1, -1, 1, -1]], dtype=dt).T
+        h, n = 0.25 + 0.5 * g, -0.25 * g
+        self.m_to_f = np.array([[0.5, 0, h, 0.25, 0, -0.5, 0], [0, 0.5, h, -0.25, 0, 0, -0.5],
+                                [-0.5, 0, h, 0.25, 0, 0.5, 0], [0, -0.5, h, -0.25, 0, 0, 0.5],
+                                [0, 0, n, 0, 0.25, 0.25, 0.25], [0, 0, n, 0, -0.25, -0.25, 0.25],
+                                [0, 0, n, 0, 0.25, -0.25, -0.25], [0, 0, n, 0, -0.25, 0.25, -0.25]], dtype=dt).T
+
+    def grid_size(self, level=0):
+        """``:501-529``."""
+        if level == 0:
+            return self.nx, self.ny
+        nxb = int(self.mg_BCs["left"]) + int(self.mg_BCs["right"])
+        nyb = int(self.mg_BCs["bottom"]) + int(self.mg_BCs["top"])
+        return (self.nx - nxb) // 2 ** level + nxb, (self.ny - nyb) // 2 ** level + nyb
+
+    def grid_info(self, level=0):
+        nx, ny = self.grid_size(level)
+        return {"nx": nx, "ny": ny, "nz": self.nz, "dim": self.lattice.d, "lattice": self.lattice}
+
+    def bounding_box_indices(self, level=0):
+        """``:563-589``."""
+        nx, ny = self.grid_size(level)
+        return {"bottom": np.array([[i, 0] for i in range(nx)], dtype=int),
+                "top": np.array([[i, ny - 1] for i in range(nx)], dtype=int),
+                "left": np.array([[0, i] for i in range(ny)], dtype=int),
+                "right": np.array([[nx - 1, i] for i in range(ny)], dtype=int)}
+
+    def create_grid_mask(self, solid_halo_voxels, level=0):
+        nx, ny = self.grid_size(level)
+        return grid_mask(nx, ny, self.lattice, solid_halo_voxels)
+
+    def _create_boundary_data(self):
+        """``:396-436``, then compilation of each level's BC list into kernel rules."""
+        self.BCs = []
+        self.BCs_MG = {level: [] for level in range(1, self.levels)}
+        self.set_boundary_conditions()
+        t0 = time.time()
+        for level in range(self.levels):
+            bcs = self.BCs if level == 0 else self.BCs_MG[level]
+            gm = self.create_grid_mask(solid_halo_voxels(bcs), level)
+            for bc in bcs:
+                assert bc.implementationStep in ['PostStreaming', 'PostCollision']
+                bc.create_local_mask_and_normal_arrays(gm)
+        self._compile_rules()
+        print("Time to create the grid masks and boundary rules:", time.time() - t0)
+
+    def _compile_rules(self):
+        self._rules = []
+        for level in range(self.levels):
+            bcs = self.BCs if level == 0 else self.BCs_MG[level]
+            L = self._layouts[level]
+            pc = compile_rules(bcs, L.nx, L.ny, 8, self._dtype, L.device, step="PostCollision")
+            ps = compile_rules(bcs, L.nx, L.ny, 8, self._dtype, L.device, step="PostStreaming")
+            self._rules.append((pc, ps))
+
+    def distributed_array_init(self, shape, type, init_val=0, sharding=None):
+        """A device field of ``shape`` filled with ``init_val`` (``:438-458``)."""
+        dt = torch_dtype(type)
+        if len(shape) == 3:
+            return Layout(shape[0], shape[1], dt).field(init_val, shape[2])
+        x = torch.as_tensor(np.asarray(init_val) if not isinstance(init_val, torch.Tensor) else init_val)
+        return torch.broadcast_to(x.to(device="cuda", dtype=dt), shape).clone()
+
+    # ------------------------------------------------------------------ hooks
+    def initialize_macroscopic_fields(self):
+        print("WARNING: Default initial conditions assumed: displacement = 0, stress = 0")
+        print("         To set explicit initial displacement and stress, use self.initialize_macroscopic_fields.")
+        return None, None
+
+    def output_data(self, **kwargs):
+        pass
+
+    def set_boundary_conditions(self):
+        pass
+
+    def get_force(self):
+        pass
+
+    # ------------------------------------------------------------------ fields
+    def _L(self, level=0):
+        return self._layouts[level]
+
+    def _f(self, f, level=0):
+        return self._L(level).field(f, 8)
+
+    def assign_fields_sharded(self):
+        """``:647-679``."""
+        eta0, sigma0 = self.initialize_macroscopic_fields()
+        if eta0 is None or sigma0 is None:
+            return self._L().zeros(8)
+        return self.initialize_populations(eta0, sigma0)
+
+    def initialize_populations(self, eta0, sigma0):
+        return self.equilibrium(eta0, sigma0)
+
+    def equilibrium(self, eta, sigma, cast_output=True, external_force=None):
+        """``:909-957`` (kernel ``xlbb_elast_equilibrium``)."""
+        L = self._L()
+        out = L.empty(8)
+        fe = L.field(external_force, 2)
+        # device copies must stay referenced until the asynchronous launch is enqueued:
+        # a freed temporary's block is handed to the next allocation on the stream
+        eta_d, sigma_d = L.field(eta, 2), L.field(sigma, 3)
+        _lib.check(_lib.lib().xlbb_elast_equilibrium(
+            self._dcode, L.grid(), self._mat, _lib.ptr(eta_d), _lib.ptr(sigma_d),
+            _lib.ptr(self.force), _lib.ptr(fe), _lib.ptr(out), _lib.stream_ptr()), "xlbb_elast_equilibrium")
+        return out
+
+    def update_macroscopic(self, f, external_force=None):
+        """``:1002-1038`` (kernel ``xlbb_elast_moments``)."""
+        L = self._L()
+        f = self._f(f)
+        eta, sigma = L.empty(2), L.empty(3)
+        fe = L.field(external_force, 2)
+        _lib.check(_lib.lib().xlbb_elast_moments(
+            self._dcode, L.grid(), self._mat, _lib.ptr(f), _lib.ptr(self.force), _lib.ptr(fe),
+            _lib.ptr(eta), _lib.ptr(sigma), None, 0.0, _lib.stream_ptr()), "xlbb_elast_moments")
+        return eta, sigma
+
+    def update_divergence(self, f, level=None):
+        """``:1040-1058`` (kernel ``xlbb_elast_moments``)."""
+        if level is None:
+            level = self._level_of(f)
+        L = self._L(level)
+        f = self._f(f, level)
+        div = L.empty(1)
+        _lib.check(_lib.lib().xlbb_elast_moments(
+            self._dcode, L.grid(), self._mat, _lib.ptr(f), None, None, None, None, _lib.ptr(div),
+            self._div_scale, _lib.stream_ptr()), "xlbb_elast_moments")
+        return div
+
+    def _level_of(self, f):
+        shape = tuple(f.shape[:2])
+        for level in range(self.levels):
+            if shape == self.grid_size(level):
+                return level
+        raise ValueError(f"array of shape {tuple(f.shape)} matches no multigrid level")
+
+    # ------------------------------------------------------------------ reference-compatible pieces
+    def collision(self, f, external_force, use_force=True):
+        """``:959-1000``: the collision alone (API compatibility; the time loop
+        uses the fused sweep).  Computed on the device with tensor algebra."""
+        level = self._level_of(f)
+        fd = self._f(f, level).permute(0, 1, 2)
+        F = None
+        if use_force and self.force is not None and external_force is not None:
+            F = self.force + self._L(level).field(external_force, 2)
+        elif external_force is not None:
+            F = self._L(level).field(external_force, 2)
+        elif use_force and self.force is not None:
+            F = self.force
+        f2m = torch.as_tensor(self.f_to_m, device=fd.device, dtype=fd.dtype)
+        m2f = torch.as_tensor(self.m_to_f, device=fd.device, dtype=fd.dtype)
+        m = fd @ f2m
+        cs = (3 * (self.lamda + self.mu) - 1) / (3 * (self.lamda + self.mu) + 1)
+        cd = (6 * self.mu - 1) / (6 * self.mu + 1)
+        if F is not None:
+            m = torch.cat([m[..., 0:2] + F, m[..., 2:3] * cs, m[..., 3:5] * cd, m[..., 0:2] / 3.0 + F / 6.0], -1)
+        else:
+            m = torch.cat([m[..., 0:2], m[..., 2:3] * cs, m[..., 3:5] * cd, m[..., 0:2] / 3.0], -1)
+        return self._L(level).field(m @ m2f, 8)
+
+    def streaming(self, f):
+        """Periodic pull streaming (``:738-803``; API compatibility)."""
+        out = torch.empty_like(f)
+        for i in range(self.q):
+            out[..., i] = torch.roll(f[..., i], (int(self.c[0, i]), int(self.c[1, i])), dims=(0, 1))
+        return out
+
+    def apply_bc(self, fout, fin, timestep, implementation_step, level=0):
+        """``:1061-1091`` (API compatibility) with the compiled rules."""
+        pc, ps = self._rules[level]
+        return apply_rules_device(pc if implementation_step == "PostCollision" else ps, fout, fin)
+
+    def apply_mg_bc(self, fout, fin, timestep, implementation_step, level):
+        return self.apply_bc(fout, fin, timestep, implementation_step, level)
+
+    def _interior(self, shape):
+        return (slice(int(self.mg_BCs["left"]), shape[0] - int(self.mg_BCs["right"])),
+                slice(int(self.mg_BCs["bottom"]), shape[1] - int(self.mg_BCs["top"])))
+
+    def _box(self, level):
+        nx, ny = self.grid_size(level)
+        m = self.mg_BCs
+        return int(m["left"]), nx - int(m["right"]), int(m["bottom"]), ny - int(m["top"])
+
+    def substract_residual(self, f, residual):
+        """``:1314-1344``."""
+        if residual is None:
+            return f
+        level = self._level_of(f)
+        out = self._f(f, level).clone()
+        out[self._interior(out.shape)] -= residual.to(out.dtype)
+        return out
+
+    def _restrict(self, f):
+        """``:850-865``: returns the 2x2 block sums of the interior (reference shape)."""
+        level = self._level_of(f)
+        rc = self._restrict_full(self._f(f, level), level)
+        return rc[self._interior(rc.shape)]
+
+    def _prolong(self, f):
+        """``:878-894``: injection of the coarse interior to twice its size."""
+        s = f[self._interior(f.shape)]
+        return s.repeat_interleave(2, dim=0).repeat_interleave(2, dim=1)
+
+    # ------------------------------------------------------------------ kernels
+    def _sweep(self, f, level, a=0.0, b=1.0, resid=None, fext=None, out=None, sumsq=False, div_out=None):
+        L = self._L(level)
+        out = L.empty(8) if out is None else out
+        pc, ps = self._rules[level]
+        bx0, bx1, by0, by1 = self._box(level)
+        s = _lib.ElastSweep(f.data_ptr(), out.data_ptr(), self.force.data_ptr() if self.force is not None else None,
+                            1 if level == 0 else 0, fext.data_ptr() if fext is not None else None,
+                            resid.data_ptr() if resid is not None else None, float(a), float(b),
+                            pc.struct(), ps.struct(), self._partials.data_ptr() if sumsq else None,
+                            bx0, bx1, by0, by1, div_out.data_ptr() if div_out is not None else None)
+        _lib.check(_lib.lib().xlbb_elast_sweep(self._dcode, L.grid(), self._mat, s, _lib.stream_ptr()),
+                   "xlbb_elast_sweep")
+        return out
+
+    def _restrict_full(self, res, level):
+        Lf, Lc = self._L(level), self._L(level + 1)
+        rc = Lc.empty(8)
+        m = self.mg_BCs
+        _lib.check(_lib.lib().xlbb_restrict(self._dcode, Lf.grid(), Lc.grid(), 8, int(m["left"]), int(m["right"]),
+                                            int(m["bottom"]), int(m["top"]), res.data_ptr(), rc.data_ptr(),
+                                            _lib.stream_ptr()), "xlbb_restrict")
+        return rc
+
+    def _prolong_add(self, fc, ff, level):
+        Lf, Lc = self._L(level), self._L(level + 1)
+        m = self.mg_BCs
+        _lib.check(_lib.lib().xlbb_prolong_add(self._dcode, Lf.grid(), Lc.grid(), 8, int(m["left"]), int(m["right"]),
+                                               int(m["bottom"]), int(m["top"]), fc.data_ptr(), ff.data_ptr(),
+                                               _lib.stream_ptr()), "xlbb_prolong_add")
+
+    def _ext_force(self, external_force, nonlinear_force, f, level):
+        """external_force + nonlinear_force(f) on level ``level`` (``:1259-1265``)."""
+        L = self._L(level)
+        if callable(nonlinear_force):
+            if hasattr(nonlinear_force, "evaluate"):
+                return nonlinear_force.evaluate(self, f, level, external_force)
+            nl = L.field(nonlinear_force(f), 2)
+            return nl if external_force is None else L.field(external_force + nl, 2)
+        return external_force
+
+    def step(self, f_poststreaming, timestep, return_fpost=False, external_force=None, nonlinear_force=None):
+        """``:1128-1167``."""
+        if self.levels == 1:
+            f = self._f(f_poststreaming)
+            ext = self._L().field(external_force, 2)
+            if callable(nonlinear_force):
+                ext = self._ext_force(ext, nonlinear_force, f, 0)
+            return self._step(f, timestep, return_fpost, ext)
+        return self._mg_step(f_poststreaming, timestep, external_force=external_force,
+                             nonlinear_force=nonlinear_force)
+
+    def _step(self, f_poststreaming, timestep, return_fpost=False, external_force=None, level=0):
+        """``:1169-1219``: one fused sweep."""
+        L = self._L(level)
+        f = L.field(f_poststreaming, 8)
+        fe = L.field(external_force, 2)
+        out = self._sweep(f, level, fext=fe)
+        if return_fpost:
+            fpost = self.collision(f, fe, level == 0)
+            return out, self.apply_bc(fpost, f, timestep, "PostCollision", level)
+        return out, None
+
+    def _mg_step(self, f_poststreaming, timestep, level=0, residual=None, external_force=None,
+                 nonlinear_force=None):
+        """``:1221-1312``: V-cycle.  Smoothing sweeps are ``a=1-gamma, b=gamma``
+        fused sweeps, the residual a ``a=1, b=-1`` sweep whose FP64 sum of squares
+        over the interior is reduced on the device, restriction / prolongation
+        are kernels, the coarse problem starts from zero."""
+        L = self._L(level)
+        f = L.field(f_poststreaming, 8)
+        fe = L.field(external_force, 2)
+        g = self.gamma
+        for _ in range(self.k_smooth):
+            ext = self._ext_force(fe, nonlinear_force, f, level)
+            f = self._sweep(f, level, 1.0 - g, g, resid=residual, fext=ext)
+        res_norm = None
+        if level < self.levels - 1:
+            ext = self._ext_force(fe, nonlinear_force, f, level)
+            res = self._sweep(f, level, 1.0, -1.0, resid=residual, fext=ext, sumsq=(level == 0))
+            if level == 0:
+                n = self._partials.numel()
+                _lib.check(_lib.lib().xlbb_reduce_sum(self._partials.data_ptr(), n, self._scalar.data_ptr(),
+                                                      _lib.stream_ptr()), "xlbb_reduce_sum")
+                res_norm = torch.sqrt(self._scalar[0].clone())
+            rc = self._restrict_full(res, level)
+            fc = self._L(level + 1).zeros(8)
+            fc = self._mg_step(fc, timestep, level + 1, rc, nonlinear_force=nonlinear_force)
+            self._prolong_add(fc, f, level)
+        for _ in range(self.k_smooth):
+            ext = self._ext_force(fe, nonlinear_force, f, level)
+            f = self._sweep(f, level, 1.0 - g, g, resid=residual, fext=ext)
+        if level == 0:
+            return f, res_norm
+        return f
+
+    # ------------------------------------------------------------------ driver
+    def run(self, t_max):
+        """``:1346-1425``: t_max + 1 steps with I/O through ``output_data``."""
+        f = self.assign_fields_sharded()
+        start = time.time()
+        for timestep in range(0, t_max + 1):
+            io_flag = self.ioRate > 0 and (timestep % self.ioRate == 0 or timestep == t_max)
+            print_iter_flag = self.printInfoRate > 0 and timestep % self.printInfoRate == 0
+            if io_flag:
+                eta_prev, sigma_prev = self.update_macroscopic(f)
+                eta_prev, sigma_prev = gathered(eta_prev), gathered(sigma_prev)
+            f, fstar = self.step(f, timestep, return_fpost=self.returnFpost)
+            if print_iter_flag:
+                print(f"Timestep {timestep} of {t_max} completed")
+            if io_flag:
+                eta, sigma = self.update_macroscopic(f)
+                if isinstance(fstar, torch.Tensor) and fstar.dim() == 0:
+                    fstar = float(fstar)
+                self.handle_io_timestep(timestep, f, fstar, gathered(eta), gathered(sigma), eta_prev, sigma_prev)
+            if self.computeMLUPS and timestep == 1:
+                torch.cuda.synchronize()
+                start = time.time()
+        if self.computeMLUPS:
+            torch.cuda.synchronize()
+            end = time.time()
+            print(f"Domain: {self.nx} x {self.ny}")
+            print(f"Number of voxels: {self.nx * self.ny}")
+            print(f"MLUPS: {self.nx * self.ny * t_max / (end - start) / 1e6}")
+        return f
+
+    def handle_io_timestep(self, timestep, f, fstar, eta, sigma, eta_prev, sigma_prev):
+        self.output_data(timestep=timestep, eta=eta, eta_prev=eta_prev, sigma=sigma, sigma_prev=sigma_prev,
+                         f_poststreaming=f, f_postcollision=fstar)
+
+
+class ElasticityBounceBackFullway(BoundaryCondition):
+    """``src/elasticity.py:1503-1550``: post-collision full-way bounce-back with an
+    optional wall displacement ``eta``."""
+
+    def __init__(self, indices, gridInfo, precision_policy, eta=None):
+        super().__init__(indices, gridInfo, precision_policy)
+        self.name = "ElasticityBounceBackFullway"
+        self.implementationStep = "PostCollision"
+        self.eta = None if eta is None else np.asarray(eta, dtype=np.float64)
+
+    def apply(self, fout, fin):
+        out = _take(fin, self.indices)[..., self.lattice.opp_indices]
+        if self.eta is None:
+            return out
+        c = np.array(self.lattice.c, dtype=np.float64)
+        return out + 6.0 * self.lattice.w.astype(np.float64) * np.dot(self.eta, c)
+
+
+class ElasticityBounceBack(BoundaryCondition):
+    """``src/elasticity.py:1552-1646``: halfway bounce-back (Dirichlet)."""
+
+    def __init__(self, indices, gridInfo, precision_policy, eta=None):
+        super().__init__(indices, gridInfo, precision_policy)
+        self.name = "ElasticityBounceBack"
+        self.implementationStep = "PostStreaming"
+        self.needsExtraConfiguration = True
+        self.isSolid = True
+        self.eta = None if eta is None else np.asarray(eta, dtype=np.float64)
+
+    def configure(self, boundaryMask):
+        nbd_orig = len(self.indices[0])
+        first = self._halfway_index_shift(boundaryMask)
+        nbd = len(self.indices[0])
+        if nbd_orig != nbd and self.eta is not None:
+            if self.eta.shape == (self.lattice.d,):
+                self.eta = np.tile(self.eta, (nbd, 1))
+            else:
+                print("WARNING: Assuming a correct displacement vector to impose at the BC cells!")
+                self.eta = self.eta[first]
+        elif self.eta is not None and self.eta.shape == (self.lattice.d,):
+            self.eta = np.tile(self.eta, (nbd, 1))
+
+    def impose_boundary_displacement(self, fbd, bindex):
+        c = np.array(self.lattice.c, dtype=np.float64)
+        cu = 6.0 * self.lattice.w.astype(np.float64) * np.dot(self.eta, c)
+        return _at_add(fbd, (bindex, self.imissing), cu[bindex, self.imissing])
+
+    def apply(self, fout, fin):
+        nbd = len(self.indices[0])
+        bindex = np.arange(nbd)[:, None]
+        fbd = np.array(_take(fout, self.indices))
+        _at_set(fbd, (bindex, self.imissing), _take(fin, self.indices)[bindex, self.iknown])
+        if self.eta is not None:
+            fbd = self.impose_boundary_displacement(fbd, bindex)
+        return fbd
+
+
+class ElasticityAntiBounceBack(BoundaryCondition):
+    """``src/elasticity.py:1648-1750``: halfway anti-bounce-back (Neumann /
+    traction ``T``)."""
+
+    def __init__(self, indices, gridInfo, precision_policy, T=None):
+        super().__init__(indices, gridInfo, precision_policy)
+        self.name = "ElasticityAntiBounceBack"
+        self.implementationStep = "PostStreaming"
+        self.needsExtraConfiguration = True
+        self.isSolid = True
+        self.T = None if T is None else np.asarray(T, dtype=np.float64)
+
+    def configure(self, boundaryMask):
+        nbd_orig = len(self.indices[0])
+        first = self._halfway_index_shift(boundaryMask)
+        nbd = len(self.indices[0])
+        if nbd_orig != nbd and self.T is not None:
+            if self.T.shape == (self.lattice.d,):
+                self.T = np.tile(self.T, (nbd, 1))
+            else:
+                print("WARNING: Assuming a correct normal stress vector to impose at the BC cells!")
+                self.T = self.T[first]
+        elif self.T is not None and self.T.shape == (self.lattice.d,):
+            self.T = np.tile(self.T, (nbd, 1))
+
+    def get_missing_mask(self, boundaryMask):
+        if self.T is not None:
+            normals = self.get_normals(boundaryMask)
+            T = self.T
+            if np.all(normals[:, 0] == -1):
+                self.i_update = (0, 4, 7)
+                self.T_update = np.stack((T[:, 0], 0.5 * T[:, 1], -0.5 * T[:, 1]), axis=-1)
+            elif np.all(normals[:, 0] == 1):
+                self.i_update = (2, 5, 6)
+                self.T_update = np.stack((-T[:, 0], 0.5 * T[:, 1], -0.5 * T[:, 1]), axis=-1)
+            elif np.all(normals[:, 1] == -1):
+                self.i_update = (1, 4, 5)
+                self.T_update = np.stack((T[:, 1], 0.5 * T[:, 0], -0.5 * T[:, 0]), axis=-1)
+            elif np.all(normals[:, 1] == 1):
+                self.i_update = (3, 6, 7)
+                self.T_update = np.stack((-T[:, 1], -0.5 * T[:, 0], 0.5 * T[:, 0]), axis=-1)
+            else:
+                raise NotImplementedError
+        return super().get_missing_mask(boundaryMask)
+
+    def apply(self, fout, fin):
+        fbd = np.array(_take(fout, self.indices))
+        fbd[self.imissingMask] = -_take(fin, self.indices)[self.iknownMask]
+        if self.T is not None:
+            fbd[:, list(self.i_update)] += self.T_update
+        return fbd
