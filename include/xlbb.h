@@ -57,7 +57,22 @@ typedef struct {
     const int* cell_x;       /* count entries */
     const uint8_t* code;     /* count*q entries */
     const void* cst;         /* count*q entries, compute dtype */
+    const uint32_t* mask;    /* ny*words_per_row words: bit (x%32) of word x/32 set on rule cells */
+    const int* word_base;    /* rule index of the first rule cell of each mask word */
+    int words_per_row;       /* >= ceil(nx/32) */
 } XlbbRules;
+
+/*
+ * Launch shape of the fused sweeps (kernel 0: elasticity, 1: Darcy):
+ * tx owned columns per CTA (64, 128 or 256), depth rows of prefetch (1..3),
+ * strips sized for ctas_per_sm CTAs per SM but never shorter than min_rows.
+ */
+typedef struct {
+    int tx, depth, ctas_per_sm, min_rows;
+} XlbbSweepConfig;
+
+int xlbb_sweep_set_config(int kernel, const XlbbSweepConfig* cfg);
+int xlbb_sweep_get_config(int kernel, XlbbSweepConfig* cfg);
 
 typedef struct {
     double lam, mu;          /* uniform Lame parameters (lattice units)       */

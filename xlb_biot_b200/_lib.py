@@ -26,7 +26,13 @@ class Grid(ctypes.Structure):
 
 class Rules(ctypes.Structure):
     _fields_ = [("count", ctypes.c_int), ("row_ptr", ctypes.c_void_p), ("cell_x", ctypes.c_void_p),
-                ("code", ctypes.c_void_p), ("cst", ctypes.c_void_p)]
+                ("code", ctypes.c_void_p), ("cst", ctypes.c_void_p), ("mask", ctypes.c_void_p),
+                ("word_base", ctypes.c_void_p), ("words_per_row", ctypes.c_int)]
+
+
+class SweepConfig(ctypes.Structure):
+    _fields_ = [("tx", ctypes.c_int), ("depth", ctypes.c_int), ("ctas_per_sm", ctypes.c_int),
+                ("min_rows", ctypes.c_int)]
 
 
 class ElastMaterial(ctypes.Structure):
@@ -67,6 +73,8 @@ SIGNATURES = {
     "xlbb_sumsq": (I, [I, PG, I, P, I, I, I, I, P, P]),
     "xlbb_sumsq_ctas": (I, [PG]),
     "xlbb_axpby": (I, [I, ctypes.c_longlong, D, P, D, P, P, P]),
+    "xlbb_sweep_set_config": (I, [I, ctypes.POINTER(SweepConfig)]),
+    "xlbb_sweep_get_config": (I, [I, ctypes.POINTER(SweepConfig)]),
     "xlbb_last_error": (ctypes.c_char_p, []),
     "xlbb_version": (I, []),
 }

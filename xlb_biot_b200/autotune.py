@@ -1,0 +1,94 @@
+"""Autotuner of the fused sweeps' launch shape.
+
+The sweeps take a runtime launch shape (``XlbbSweepConfig``: owned columns per
+CTA, prefetch depth in rows, CTAs per SM, minimum strip height).  ``tune``
+times every candidate on the caller's own sweep (CUDA events on the current
+stream, after a warm-up) and keeps the fastest; results are cached per GPU,
+kernel family, dtype and grid size in a JSON file so later runs skip the
+search.  The cache path is ``$XLBB_TUNE_CACHE`` or ``~/.cache/xlbb_tune.json``.
+"""
+import itertools
+import json
+import os
+
+import torch
+
+from . import _lib
+
+ELASTICITY, DARCY = 0, 1
+TX = (64, 128, 256)
+DEPTH = (1, 2, 3)
+CTAS_PER_SM = (2, 3, 4, 6, 8)
+MIN_ROWS = (8, 16)
+
+
+def get_config(kernel):
+    c = _lib.SweepConfig()
+    _lib.check(_lib.lib().xlbb_sweep_get_config(kernel, c), "xlbb_sweep_get_config")
+    return {"tx": c.tx, "depth": c.depth, "ctas_per_sm": c.ctas_per_sm, "min_rows": c.min_rows}
+
+
+def set_config(kernel, tx, depth, ctas_per_sm, min_rows):
+    c = _lib.SweepConfig(int(tx), int(depth), int(ctas_per_sm), int(min_rows))
+    _lib.check(_lib.lib().xlbb_sweep_set_config(kernel, c), "xlbb_sweep_set_config")
+
+
+def _cache_path():
+    return os.environ.get("XLBB_TUNE_CACHE", os.path.join(os.path.expanduser("~"), ".cache", "xlbb_tune.json"))
+
+
+def _load():
+    try:
+        with open(_cache_path()) as fh:
+            return json.load(fh)
+    except (OSError, ValueError):
+        return {}
+
+
+def _store(cache):
+    path = _cache_path()
+    try:
+        os.makedirs(os.path.dirname(path), exist_ok=True)
+        with open(path, "w") as fh:
+            json.dump(cache, fh, indent=1, sort_keys=True)
+    except OSError:
+        pass
+
+
+def _time(run, reps):
+    run()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(reps):
+        run()
+    b.record()
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / reps
+
+
+def tune(kernel, run, key, reps=5, candidates=None, use_cache=True):
+    """Pick the fastest launch shape for ``run`` (a callable issuing the sweeps
+    to tune, e.g. 20 sweeps of the production grid).  ``key`` identifies the
+    problem (dtype, grid).  Returns (config, ms, table)."""
+    dev = torch.cuda.get_device_name()
+    full_key = f"{dev}|{kernel}|{key}"
+    cache = _load() if use_cache else {}
+    if full_key in cache:
+        cfg = cache[full_key]["config"]
+        set_config(kernel, **cfg)
+        return cfg, cache[full_key]["ms"], None
+    if candidates is None:
+        candidates = [dict(tx=t, depth=d, ctas_per_sm=c, min_rows=m)
+                      for t, d, c, m in itertools.product(TX, DEPTH, CTAS_PER_SM, MIN_ROWS)]
+    table = []
+    for cfg in candidates:
+        set_config(kernel, **cfg)
+        table.append((_time(run, reps), cfg))
+    table.sort(key=lambda e: e[0])
+    ms, best = table[0]
+    set_config(kernel, **best)
+    if use_cache:
+        cache[full_key] = {"config": best, "ms": ms}
+        _store(cache)
+    return best, ms, table

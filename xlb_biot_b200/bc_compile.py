@@ -24,9 +24,10 @@ from .boundary_conditions import apply_in_order
 class CompiledRules:
     """Device-resident rule table of one grid and one phase."""
 
-    def __init__(self, q, ny, cells, code, cst, dtype, device):
+    def __init__(self, q, ny, cells, code, cst, dtype, device, nx=None):
         self.q = q
         self.count = len(cells)
+        self.nx = int(nx) if nx is not None else (int(cells[:, 0].max()) + 1 if len(cells) else 1)
         order = np.lexsort((cells[:, 0], cells[:, 1])) if self.count else np.zeros(0, dtype=np.int64)
         cells = cells[order]
         self.cells = cells
@@ -36,25 +37,37 @@ class CompiledRules:
         if self.count:
             np.add.at(row_ptr, cells[:, 1] + 1, 1)
         row_ptr = np.cumsum(row_ptr).astype(np.int32)
+        # one bit per cell and the index of the first rule of every 32-cell word:
+        # the sweeps find a cell's rule as word_base + popcount(bits below it)
+        self.words_per_row = (self.nx + 31) // 32
         if self.count:
+            words = cells[:, 1] * self.words_per_row + cells[:, 0] // 32
+            mask = np.zeros(ny * self.words_per_row, dtype=np.uint64)
+            np.bitwise_or.at(mask, words, (np.uint64(1) << (cells[:, 0] % 32).astype(np.uint64)))
+            first = np.full(ny * self.words_per_row, self.count, dtype=np.int64)
+            np.minimum.at(first, words, np.arange(self.count))
+            word_base = np.minimum.accumulate(first[::-1])[::-1].astype(np.int32)
             self.row_ptr = torch.as_tensor(row_ptr, device=device)
             self.cell_x = torch.as_tensor(cells[:, 0].astype(np.int32), device=device)
             self.code = torch.as_tensor(self.code_np.astype(np.uint8).reshape(-1), device=device)
             self.cst = torch.as_tensor(self.cst_np.reshape(-1), device=device).to(dtype)
+            self.mask = torch.as_tensor(mask.astype(np.uint32).view(np.int32), device=device)
+            self.word_base = torch.as_tensor(word_base, device=device)
         else:
-            self.row_ptr = self.cell_x = self.code = self.cst = None
+            self.row_ptr = self.cell_x = self.code = self.cst = self.mask = self.word_base = None
 
     def struct(self):
         if self.count == 0:
-            return _lib.Rules(0, None, None, None, None)
+            return _lib.Rules(0, None, None, None, None, None, None, self.words_per_row)
         return _lib.Rules(self.count, self.row_ptr.data_ptr(), self.cell_x.data_ptr(), self.code.data_ptr(),
-                          self.cst.data_ptr())
+                          self.cst.data_ptr(), self.mask.data_ptr(), self.word_base.data_ptr(),
+                          self.words_per_row)
 
     def restricted(self, nx, ny, dtype, device):
         """The same rules on a smaller grid: cells outside it are dropped (the
         reference's coarse-level gradient gathers clamp and scatters drop)."""
         keep = (self.cells[:, 0] < nx) & (self.cells[:, 1] < ny) if self.count else np.zeros(0, bool)
-        return CompiledRules(self.q, ny, self.cells[keep], self.code_np[keep], self.cst_np[keep], dtype, device)
+        return CompiledRules(self.q, ny, self.cells[keep], self.code_np[keep], self.cst_np[keep], dtype, device, nx)
 
 
 def _run(bcs, fout, fin, step, names):
@@ -75,7 +88,7 @@ def compile_rules(bcs, nx, ny, q, dtype, device, step=None, names=None, check=Tr
         cells.append(idx[ok])
     if not cells or sum(len(c) for c in cells) == 0:
         return CompiledRules(q, ny, np.zeros((0, 2), np.int64), np.zeros((0, q), np.uint8), np.zeros((0, q)),
-                             dtype, device)
+                             dtype, device, nx)
     cells = np.unique(np.vstack(cells), axis=0)
     cx, cy = cells[:, 0], cells[:, 1]
 
@@ -123,7 +136,7 @@ def compile_rules(bcs, nx, ny, q, dtype, device, step=None, names=None, check=Tr
         if np.any(bad):
             raise NotImplementedError("boundary rule scales a population; not representable")
         code[:, d] = cd
-    rules = CompiledRules(q, ny, cells, code, c0, dtype, device)
+    rules = CompiledRules(q, ny, cells, code, c0, dtype, device, nx)
     if check:
         _self_check(bcs, nx, ny, q, step, names, rules)
     return rules

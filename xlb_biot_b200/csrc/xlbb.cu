@@ -52,7 +52,24 @@ static RulesView<T, Q> rules_view(const XlbbRules& r) {
     v.cell_x = r.cell_x;
     v.code = r.code;
     v.cst = static_cast<const T*>(r.cst);
+    v.mask = r.mask;
+    v.word_base = r.word_base;
+    v.words_per_row = r.words_per_row;
+    if (v.count > 0 && (r.mask == nullptr || r.word_base == nullptr)) v.count = 0;
     return v;
+}
+
+static bool rules_ok(const XlbbRules& r, const XlbbGrid* g) {
+    if (r.count <= 0 || r.row_ptr == nullptr) return true;
+    return r.cell_x && r.code && r.cst && r.mask && r.word_base && r.words_per_row * 32 >= g->nx;
+}
+
+// Launch shapes of the sweeps, per kernel family (0: elasticity, 1: Darcy).
+static XlbbSweepConfig g_cfg[2] = {{128, 2, 4, 8}, {128, 2, 4, 8}};
+
+static bool cfg_ok(const XlbbSweepConfig& c) {
+    return (c.tx == 64 || c.tx == 128 || c.tx == 256) && c.depth >= 1 && c.depth <= 3 && c.ctas_per_sm >= 1 &&
+           c.ctas_per_sm <= 32 && c.min_rows >= 1;
 }
 
 // ---------------------------------------------------------------------------
@@ -257,19 +274,41 @@ struct DarcyPhys {
     }
 };
 
-// Launch geometry of the sweeps: TX owned columns per CTA, strips of rows
-// chosen so that the grid holds about `waves` CTAs per SM.
-static constexpr int SWEEP_TX = 128;
-
-static dim3 sweep_grid(const XlbbGrid* g, int tx) {
-    const int nbx = (g->nx + tx - 1) / tx;
-    const int target = 6 * num_sms();
+// Launch geometry of the sweeps: tx owned columns per CTA, strips of rows
+// chosen so that the grid holds about ctas_per_sm CTAs per SM (one wave),
+// never shorter than min_rows rows (each strip recomputes two halo rows).
+static dim3 sweep_grid(const XlbbGrid* g, const XlbbSweepConfig& c) {
+    const int nbx = (g->nx + c.tx - 1) / c.tx;
+    const int target = c.ctas_per_sm * num_sms();
     int nby = target / nbx;
-    const int max_by = g->ny / 8 > 0 ? g->ny / 8 : 1;   // strips of >= 8 rows
+    const int max_by = g->ny / c.min_rows > 0 ? g->ny / c.min_rows : 1;
     if (nby > max_by) nby = max_by;
     if (nby < 1) nby = 1;
     if (nby > g->ny) nby = g->ny;
     return dim3(nbx, nby);
+}
+
+// Runtime (tx, depth) -> template instance.
+template <class Ph, bool PREV>
+static void launch_sweep(const XlbbSweepConfig& c, dim3 grid, cudaStream_t st, const typename Ph::Args& a) {
+#define XLBB_CASE(TX_, D_)                                                            \
+    if (c.tx == TX_ && c.depth == D_) {                                                \
+        sweep_kernel<Ph, TX_, D_, PREV><<<grid, TX_ + 32, 0, st>>>(a);                 \
+        return;                                                                        \
+    }
+    XLBB_CASE(64, 1) XLBB_CASE(64, 2) XLBB_CASE(64, 3)
+    XLBB_CASE(128, 1) XLBB_CASE(128, 2) XLBB_CASE(128, 3)
+    if constexpr (sizeof(typename Ph::T) == 4) {   // FP64 rings of 256 columns exceed 48 KB
+        XLBB_CASE(256, 1) XLBB_CASE(256, 2) XLBB_CASE(256, 3)
+    }
+#undef XLBB_CASE
+}
+
+// The configuration a launch actually uses (FP64 caps tx at 128).
+static XlbbSweepConfig effective_cfg(int kernel, int dtype) {
+    XlbbSweepConfig c = g_cfg[kernel];
+    if (dtype == XLBB_F64 && c.tx > 128) c.tx = 128;
+    return c;
 }
 
 // ---------------------------------------------------------------------------
@@ -510,8 +549,8 @@ static int launch_elast(const XlbbGrid* g, const XlbbElastMaterial* mat, const X
     a.bx0 = s->bx0; a.bx1 = s->bx1; a.by0 = s->by0; a.by1 = s->by1;
     a.div_out = static_cast<T*>(s->div_out);
     a.div_scale = T(-1.5 / (3.0 * (mat->lam + mat->mu) + 1.0));
-    const dim3 grid = sweep_grid(g, SWEEP_TX);
-    sweep_kernel<Ph, SWEEP_TX, PREV><<<grid, SWEEP_TX + 32, 0, st>>>(a);
+    const XlbbSweepConfig c = effective_cfg(0, sizeof(T) == 4 ? XLBB_F32 : XLBB_F64);
+    launch_sweep<Ph, PREV>(c, sweep_grid(g, c), st, a);
     return check_launch("xlbb_elast_sweep");
 }
 
@@ -536,9 +575,9 @@ static int darcy_sweep_t(const XlbbGrid* g, const XlbbDarcySweep* s, cudaStream_
     a.pc = rules_view<T, 9>(s->pc);
     a.ps = rules_view<T, 9>(s->ps);
     a.sumsq = s->sumsq;
-    const dim3 grid = sweep_grid(g, SWEEP_TX);
-    if (s->sumsq) sweep_kernel<Ph, SWEEP_TX, true><<<grid, SWEEP_TX + 32, 0, st>>>(a);
-    else sweep_kernel<Ph, SWEEP_TX, false><<<grid, SWEEP_TX + 32, 0, st>>>(a);
+    const XlbbSweepConfig c = effective_cfg(1, sizeof(T) == 4 ? XLBB_F32 : XLBB_F64);
+    if (s->sumsq) launch_sweep<Ph, true>(c, sweep_grid(g, c), st, a);
+    else launch_sweep<Ph, false>(c, sweep_grid(g, c), st, a);
     return check_launch("xlbb_darcy_sweep");
 }
 
@@ -558,16 +597,33 @@ const char* xlbb_last_error(void) { return g_last_error.c_str(); }
 
 int xlbb_elast_sweep_ctas(const XlbbGrid* g) {
     if (!grid_ok(g)) return fail(XLBB_EBADARG, "xlbb_elast_sweep_ctas: bad grid");
-    const dim3 d = sweep_grid(g, SWEEP_TX);
-    return (int)(d.x * d.y);
+    const dim3 a = sweep_grid(g, effective_cfg(0, XLBB_F32)), b = sweep_grid(g, effective_cfg(0, XLBB_F64));
+    return (int)max(a.x * a.y, b.x * b.y);
 }
 
-int xlbb_darcy_sweep_ctas(const XlbbGrid* g) { return xlbb_elast_sweep_ctas(g); }
+int xlbb_darcy_sweep_ctas(const XlbbGrid* g) {
+    if (!grid_ok(g)) return fail(XLBB_EBADARG, "xlbb_darcy_sweep_ctas: bad grid");
+    const dim3 a = sweep_grid(g, effective_cfg(1, XLBB_F32)), b = sweep_grid(g, effective_cfg(1, XLBB_F64));
+    return (int)max(a.x * a.y, b.x * b.y);
+}
+
+int xlbb_sweep_set_config(int kernel, const XlbbSweepConfig* cfg) {
+    if ((kernel != 0 && kernel != 1) || !cfg || !cfg_ok(*cfg)) return fail(XLBB_EBADARG, "xlbb_sweep_set_config: bad argument");
+    g_cfg[kernel] = *cfg;
+    return XLBB_OK;
+}
+
+int xlbb_sweep_get_config(int kernel, XlbbSweepConfig* cfg) {
+    if ((kernel != 0 && kernel != 1) || !cfg) return fail(XLBB_EBADARG, "xlbb_sweep_get_config: bad argument");
+    *cfg = g_cfg[kernel];
+    return XLBB_OK;
+}
 
 int xlbb_elast_sweep(int dtype, const XlbbGrid* g, const XlbbElastMaterial* mat, const XlbbElastSweep* s,
                      void* stream) {
     if (!grid_ok(g) || !mat || !s || !s->f_in || !s->f_out) return fail(XLBB_EBADARG, "xlbb_elast_sweep: bad argument");
     if (s->f_in == s->f_out) return fail(XLBB_EBADARG, "xlbb_elast_sweep: f_in and f_out must differ");
+    if (!rules_ok(s->pc, g) || !rules_ok(s->ps, g)) return fail(XLBB_EBADARG, "xlbb_elast_sweep: incomplete rules");
     if ((mat->mu_field == nullptr) != (mat->lam_field == nullptr))
         return fail(XLBB_EBADARG, "xlbb_elast_sweep: lam_field and mu_field go together");
     if (dtype == XLBB_F32) return elast_sweep_t<float>(g, mat, s, XLBB_STREAM(stream));
@@ -578,6 +634,7 @@ int xlbb_elast_sweep(int dtype, const XlbbGrid* g, const XlbbElastMaterial* mat,
 int xlbb_darcy_sweep(int dtype, const XlbbGrid* g, const XlbbDarcySweep* s, void* stream) {
     if (!grid_ok(g) || !s || !s->f_in || !s->f_out) return fail(XLBB_EBADARG, "xlbb_darcy_sweep: bad argument");
     if (s->f_in == s->f_out) return fail(XLBB_EBADARG, "xlbb_darcy_sweep: f_in and f_out must differ");
+    if (!rules_ok(s->pc, g) || !rules_ok(s->ps, g)) return fail(XLBB_EBADARG, "xlbb_darcy_sweep: incomplete rules");
     if (dtype == XLBB_F32) return darcy_sweep_t<float>(g, s, XLBB_STREAM(stream));
     if (dtype == XLBB_F64) return darcy_sweep_t<double>(g, s, XLBB_STREAM(stream));
     return fail(XLBB_EUNSUPPORTED, "xlbb_darcy_sweep: dtype");

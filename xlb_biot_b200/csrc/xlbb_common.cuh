@@ -24,6 +24,9 @@ struct RulesView {
     const int* cell_x;
     const uint8_t* code;
     const T* cst;
+    const uint32_t* mask;    // one bit per cell, words_per_row words per row
+    const int* word_base;    // index of the first rule cell of each mask word
+    int words_per_row;
 };
 
 // Index of the rule of cell (x, y), or -1.  Rows are CSR, x sorted.

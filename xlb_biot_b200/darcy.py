@@ -38,8 +38,8 @@ class AdvectionDiffusionReactionBGK(LBMBase):
         self.source = self._layout.field(src, 1) if src is not None else None
         om = kwargs.get("omega_field", None)
         self.omega_field = self._layout.field(om, 1) if om is not None else None
-        self._partials = torch.empty(max(1, _lib.lib().xlbb_darcy_sweep_ctas(self._layout.grid())),
-                                     dtype=torch.float64, device=self._layout.device)
+        self._partials = torch.empty(0, dtype=torch.float64, device=self._layout.device)
+        self._n_partials = 0
         self._grad_rules_by_shape = {}
 
     def _compile_rules(self):
@@ -119,6 +119,11 @@ class AdvectionDiffusionReactionBGK(LBMBase):
     def _sweep(self, f, external_source=None, out=None, sumsq=False):
         L = self._layout
         out = L.empty(9) if out is None else out
+        if sumsq:
+            # one FP64 partial per CTA of the current launch shape
+            self._n_partials = _lib.check(_lib.lib().xlbb_darcy_sweep_ctas(L.grid()), "xlbb_darcy_sweep_ctas")
+            if self._partials.numel() < self._n_partials:
+                self._partials = torch.empty(self._n_partials, dtype=torch.float64, device=L.device)
         s = _lib.DarcySweep(f.data_ptr(), out.data_ptr(), float(self.omega),
                             self.omega_field.data_ptr() if self.omega_field is not None else None,
                             self.source.data_ptr() if self.source is not None else None,
@@ -146,7 +151,7 @@ class AdvectionDiffusionReactionBGK(LBMBase):
     def residual_sumsq(self, out_scalar):
         """FP64 sum of (f_new - f_old)^2 of the last sweep run with ``sumsq=True``
         (deterministic two-pass reduction), written into a device scalar."""
-        _lib.check(_lib.lib().xlbb_reduce_sum(self._partials.data_ptr(), self._partials.numel(),
+        _lib.check(_lib.lib().xlbb_reduce_sum(self._partials.data_ptr(), self._n_partials,
                                               out_scalar.data_ptr(), _lib.stream_ptr()), "xlbb_reduce_sum")
         return out_scalar
 

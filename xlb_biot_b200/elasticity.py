@@ -64,8 +64,8 @@ class LBMElasticity:
         self._mat = _lib.ElastMaterial(float(self.lamda), float(self.mu), None, None)
         self._lam_field = self._mu_field = None
         self._div_scale = -1.5 / (3 * (self.lamda + self.mu) + 1)
-        self._partials = torch.empty(max(1, _lib.lib().xlbb_elast_sweep_ctas(self._layouts[0].grid())),
-                                     dtype=torch.float64, device=self._layouts[0].device)
+        self._partials = torch.empty(0, dtype=torch.float64, device=self._layouts[0].device)
+        self._n_partials = 0
         self._scalar = torch.empty(1, dtype=torch.float64, device=self._layouts[0].device)
 
     # ------------------------------------------------------------------ validation
@@ -450,6 +450,11 @@ class LBMElasticity:
     def _sweep(self, f, level, a=0.0, b=1.0, resid=None, fext=None, out=None, sumsq=False, div_out=None):
         L = self._L(level)
         out = L.empty(8) if out is None else out
+        if sumsq:
+            # one FP64 partial per CTA of the current launch shape
+            self._n_partials = _lib.check(_lib.lib().xlbb_elast_sweep_ctas(L.grid()), "xlbb_elast_sweep_ctas")
+            if self._partials.numel() < self._n_partials:
+                self._partials = torch.empty(self._n_partials, dtype=torch.float64, device=L.device)
         pc, ps = self._rules[level]
         bx0, bx1, by0, by1 = self._box(level)
         s = _lib.ElastSweep(f.data_ptr(), out.data_ptr(), self.force.data_ptr() if self.force is not None else None,
@@ -527,8 +532,8 @@ class LBMElasticity:
             ext = self._ext_force(fe, nonlinear_force, f, level)
             res = self._sweep(f, level, 1.0, -1.0, resid=residual, fext=ext, sumsq=(level == 0))
             if level == 0:
-                n = self._partials.numel()
-                _lib.check(_lib.lib().xlbb_reduce_sum(self._partials.data_ptr(), n, self._scalar.data_ptr(),
+                _lib.check(_lib.lib().xlbb_reduce_sum(self._partials.data_ptr(), self._n_partials,
+                                                      self._scalar.data_ptr(),
                                                       _lib.stream_ptr()), "xlbb_reduce_sum")
                 res_norm = torch.sqrt(self._scalar[0].clone())
             rc = self._restrict_full(res, level)
