@@ -192,7 +192,16 @@ def run_ours(args):
         for _ in range(10):
             solver._sweep(x, None, out=y)
             x, y = y, x
-    tuned, tuned_ms, _ = autotune.tune(autotune.DARCY, tune_run, key=f"f32|{N}x{N}|omega_field", use_cache=False)
+    if args.launch_shape:
+        tx, depth, cps, mrows, pipe = (int(v) for v in args.launch_shape.split(","))
+        autotune.set_config(autotune.DARCY, tx, depth, cps, mrows, pipe)
+        tuned, table = autotune.get_config(autotune.DARCY), []
+    else:
+        tuned, tuned_ms, table = autotune.tune(autotune.DARCY, tune_run, key=f"f32|{N}x{N}|omega_field",
+                                               use_cache=False)
+    if os.environ.get("XLBB_TUNE_VERBOSE"):
+        for ms, cfg in table[:20]:
+            print(f"tune {ms / 10 * 1e3:8.2f} us/sweep {cfg}", file=sys.stderr)
     del bufs
     loop = solver.sweep_graph(SWEEPS_PER_STEP)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")     # 256 MiB > L2
@@ -303,6 +312,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--launch-shape", default="",
+                    help="tx,depth,ctas_per_sm,min_rows,pipeline of the Darcy sweep (skips the autotuner)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -64,15 +64,27 @@ typedef struct {
 
 /*
  * Launch shape of the fused sweeps (kernel 0: elasticity, 1: Darcy):
- * tx owned columns per CTA (64, 128 or 256), depth rows of prefetch (1..3),
- * strips sized for ctas_per_sm CTAs per SM but never shorter than min_rows.
+ * tx owned columns per CTA (128 or 256), strips sized for ctas_per_sm CTAs per
+ * SM but never shorter than min_rows rows, and the pipeline:
+ *   0: CTA row ring in shared memory, register prefetch of depth (1, 2) rows;
+ *   1: as 0, inputs in a shared-memory ring of depth (2, 4, 6) rows filled by
+ *      cp.async.bulk copies on mbarriers (needs 16-byte aligned planes and
+ *      pitch, otherwise pipeline 0 is used);
+ *   2: independent warps of 30 output columns (tx ignored), post-collision
+ *      rows in registers, streaming by warp shuffles, no barrier; register
+ *      prefetch of depth (1, 2) rows; ctas_per_sm counts CTAs of 4 warps.
+ * FP64 sweeps cap tx at 128.
  */
 typedef struct {
-    int tx, depth, ctas_per_sm, min_rows;
+    int tx, depth, ctas_per_sm, min_rows, pipeline;
 } XlbbSweepConfig;
 
 int xlbb_sweep_set_config(int kernel, const XlbbSweepConfig* cfg);
 int xlbb_sweep_get_config(int kernel, XlbbSweepConfig* cfg);
+
+/* Device status word of the kernels' bounded waits (0, or XLBB_ETIMEOUT if a
+ * wait gave up); synchronous; reset != 0 clears it. */
+int xlbb_device_status(int* status, int reset);
 
 typedef struct {
     double lam, mu;          /* uniform Lame parameters (lattice units)       */

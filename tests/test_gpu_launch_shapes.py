@@ -1,0 +1,97 @@
+"""Every launch shape of the fused sweeps (register-prefetch and bulk-copy
+pipelines, 128/256 columns, each prefetch depth) gives bitwise the same
+populations, and those match the oracle; the bounded waits report no timeout."""
+import numpy as np
+import pytest
+import torch
+
+import oracle.api as O
+from problems import elastic_material, make_walled_elasticity, make_darcy
+
+pytestmark = pytest.mark.gpu
+LAM, MU = elastic_material()
+
+
+@pytest.fixture(scope="module")
+def G():
+    import xlb_biot_b200.api as api
+    return api
+
+
+@pytest.fixture(scope="module")
+def shapes():
+    from xlb_biot_b200 import autotune
+    out = []
+    for c in autotune.candidates(4):
+        if c["min_rows"] == 8 and c["ctas_per_sm"] in (1, 3):
+            out.append(c)
+    return out
+
+
+def _run_darcy(G, prec, n_sweeps=12):
+    kw = dict(omega=1.0 / (3 * 0.1 + 0.5), nx=300, ny=70, nz=0, precision=prec)
+    s = make_darcy(G, "anti")(lattice=G.LatticeD2Q9(prec), **kw)
+    ext = 1e-3 * np.random.default_rng(4).standard_normal((300, 70, 1))
+    f = s.assign_fields_sharded()
+    for t in range(n_sweeps):
+        f, _ = s.step(f, t, external_source=ext)
+    return f.cpu().numpy(), s
+
+
+@pytest.mark.parametrize("prec", ["f32/f32", "f64/f64"])
+def test_darcy_all_shapes_identical(G, shapes, prec):
+    from xlb_biot_b200 import autotune
+    saved = autotune.get_config(autotune.DARCY)
+    try:
+        results = []
+        for c in shapes:
+            if prec == "f64/f64" and (c["tx"] > 128 or c["depth"] > 4):
+                continue
+            autotune.set_config(autotune.DARCY, **c)
+            results.append((c, _run_darcy(G, prec)[0]))
+        for c, r in results[1:]:
+            assert np.array_equal(r, results[0][1]), c
+        so = make_darcy(O, "anti")(lattice=O.LatticeD2Q9(prec), omega=1.0 / (3 * 0.1 + 0.5), nx=300, ny=70, nz=0,
+                                   precision=prec)
+        ext = 1e-3 * np.random.default_rng(4).standard_normal((300, 70, 1))
+        fo = so.assign_fields_sharded()
+        for t in range(12):
+            fo, _ = so.step(fo, t, external_source=ext)
+        tol = 1e-12 if prec == "f64/f64" else 1e-5
+        assert np.abs(results[0][1] - fo).max() / np.abs(fo).max() < tol
+        assert autotune.device_status() == 0
+    finally:
+        autotune.set_config(autotune.DARCY, **saved)
+
+
+@pytest.mark.parametrize("prec", ["f32/f32", "f64/f64"])
+def test_elasticity_multigrid_all_shapes_identical(G, shapes, prec):
+    """V-cycles exercise the plain, damped (a, b) and residual (resid) sweeps."""
+    from xlb_biot_b200 import autotune
+    saved = autotune.get_config(autotune.ELASTICITY)
+    kw = dict(**{"lambda": LAM}, mu=MU, nx=258, ny=66, nz=0, precision=prec, MG_levels=3,
+              MG_BCs={"top": True, "bottom": True, "left": True, "right": True})
+    rng = np.random.default_rng(9)
+    f0 = 1e-3 * rng.standard_normal((258, 66, 8))
+    try:
+        results = []
+        for c in shapes:
+            if prec == "f64/f64" and (c["tx"] > 128 or c["depth"] > 4):
+                continue
+            autotune.set_config(autotune.ELASTICITY, **c)
+            s = make_walled_elasticity(G, "dirichlet")(lattice=G.LatticeD2Q8(prec), **kw)
+            f, r = s.step(f0, 0)
+            f, r = s.step(f, 1)
+            results.append((c, f.cpu().numpy(), float(r)))
+        for c, f, r in results[1:]:
+            assert np.array_equal(f, results[0][1]), c
+            # the FP64 norm sums one partial per CTA: the order depends on the grid
+            assert abs(r - results[0][2]) <= 1e-13 * abs(results[0][2]), c
+        so = make_walled_elasticity(O, "dirichlet")(lattice=O.LatticeD2Q8(prec), **kw)
+        fo, ro = so.step(f0.astype(so.precisionPolicy.compute_dtype), 0)
+        fo, ro = so.step(fo, 1)
+        tol = 1e-12 if prec == "f64/f64" else 1e-5
+        assert np.abs(results[0][1] - fo).max() / np.abs(fo).max() < 10 * tol
+        assert autotune.device_status() == 0
+    finally:
+        autotune.set_config(autotune.ELASTICITY, **saved)

@@ -32,7 +32,7 @@ class Rules(ctypes.Structure):
 
 class SweepConfig(ctypes.Structure):
     _fields_ = [("tx", ctypes.c_int), ("depth", ctypes.c_int), ("ctas_per_sm", ctypes.c_int),
-                ("min_rows", ctypes.c_int)]
+                ("min_rows", ctypes.c_int), ("pipeline", ctypes.c_int)]
 
 
 class ElastMaterial(ctypes.Structure):
@@ -75,6 +75,7 @@ SIGNATURES = {
     "xlbb_axpby": (I, [I, ctypes.c_longlong, D, P, D, P, P, P]),
     "xlbb_sweep_set_config": (I, [I, ctypes.POINTER(SweepConfig)]),
     "xlbb_sweep_get_config": (I, [I, ctypes.POINTER(SweepConfig)]),
+    "xlbb_device_status": (I, [ctypes.POINTER(ctypes.c_int), I]),
     "xlbb_last_error": (ctypes.c_char_p, []),
     "xlbb_version": (I, []),
 }

@@ -16,21 +16,41 @@ import torch
 from . import _lib
 
 ELASTICITY, DARCY = 0, 1
-TX = (64, 128, 256)
-DEPTH = (1, 2, 3)
-CTAS_PER_SM = (2, 3, 4, 6, 8)
-MIN_ROWS = (8, 16)
+TX = (128, 256)
+DEPTH = {0: (1, 2), 1: (2, 4, 6), 2: (1, 2)}   # per pipeline: CTA+registers / CTA+bulk ring / warps
+CTAS_PER_SM = (1, 2, 3, 4, 6)
+MIN_ROWS = (8, 16, 32)
 
 
 def get_config(kernel):
     c = _lib.SweepConfig()
     _lib.check(_lib.lib().xlbb_sweep_get_config(kernel, c), "xlbb_sweep_get_config")
-    return {"tx": c.tx, "depth": c.depth, "ctas_per_sm": c.ctas_per_sm, "min_rows": c.min_rows}
+    return {"tx": c.tx, "depth": c.depth, "ctas_per_sm": c.ctas_per_sm, "min_rows": c.min_rows,
+            "pipeline": c.pipeline}
 
 
-def set_config(kernel, tx, depth, ctas_per_sm, min_rows):
-    c = _lib.SweepConfig(int(tx), int(depth), int(ctas_per_sm), int(min_rows))
+def set_config(kernel, tx, depth, ctas_per_sm, min_rows, pipeline=0):
+    c = _lib.SweepConfig(int(tx), int(depth), int(ctas_per_sm), int(min_rows), int(pipeline))
     _lib.check(_lib.lib().xlbb_sweep_set_config(kernel, c), "xlbb_sweep_set_config")
+
+
+def candidates(dtype_bytes=4):
+    """Every launch shape the library instantiates for the given element size."""
+    out = []
+    for pipe, depths in DEPTH.items():
+        for t, d, c, m in itertools.product(TX if pipe != 2 else (128,), depths, CTAS_PER_SM, MIN_ROWS):
+            if dtype_bytes == 8 and (t > 128 or d > 4):
+                continue
+            out.append(dict(tx=t, depth=d, ctas_per_sm=c, min_rows=m, pipeline=pipe))
+    return out
+
+
+def device_status(reset=True):
+    """Status word of the kernels' bounded waits (0 or XLBB_ETIMEOUT)."""
+    import ctypes
+    v = ctypes.c_int(0)
+    _lib.check(_lib.lib().xlbb_device_status(ctypes.byref(v), 1 if reset else 0), "xlbb_device_status")
+    return v.value
 
 
 def _cache_path():
@@ -67,7 +87,7 @@ def _time(run, reps):
     return a.elapsed_time(b) / reps
 
 
-def tune(kernel, run, key, reps=5, candidates=None, use_cache=True):
+def tune(kernel, run, key, reps=5, cands_override=None, use_cache=True):
     """Pick the fastest launch shape for ``run`` (a callable issuing the sweeps
     to tune, e.g. 20 sweeps of the production grid).  ``key`` identifies the
     problem (dtype, grid).  Returns (config, ms, table)."""
@@ -78,11 +98,9 @@ def tune(kernel, run, key, reps=5, candidates=None, use_cache=True):
         cfg = cache[full_key]["config"]
         set_config(kernel, **cfg)
         return cfg, cache[full_key]["ms"], None
-    if candidates is None:
-        candidates = [dict(tx=t, depth=d, ctas_per_sm=c, min_rows=m)
-                      for t, d, c, m in itertools.product(TX, DEPTH, CTAS_PER_SM, MIN_ROWS)]
+    cands = candidates() if cands_override is None else cands_override
     table = []
-    for cfg in candidates:
+    for cfg in cands:
         set_config(kernel, **cfg)
         table.append((_time(run, reps), cfg))
     table.sort(key=lambda e: e[0])

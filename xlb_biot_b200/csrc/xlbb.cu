@@ -65,11 +65,14 @@ static bool rules_ok(const XlbbRules& r, const XlbbGrid* g) {
 }
 
 // Launch shapes of the sweeps, per kernel family (0: elasticity, 1: Darcy).
-static XlbbSweepConfig g_cfg[2] = {{128, 2, 4, 8}, {128, 2, 4, 8}};
+static XlbbSweepConfig g_cfg[2] = {{256, 1, 3, 8, 0}, {256, 1, 3, 8, 0}};
+
+static constexpr int WARP_COLS = 30;   // output columns of one warp of sweep_warp_kernel
 
 static bool cfg_ok(const XlbbSweepConfig& c) {
-    return (c.tx == 64 || c.tx == 128 || c.tx == 256) && c.depth >= 1 && c.depth <= 3 && c.ctas_per_sm >= 1 &&
-           c.ctas_per_sm <= 32 && c.min_rows >= 1;
+    const bool depth_ok = c.pipeline == 1 ? (c.depth == 2 || c.depth == 4 || c.depth == 6) : (c.depth == 1 || c.depth == 2);
+    return (c.tx == 128 || c.tx == 256) && depth_ok && c.ctas_per_sm >= 1 && c.ctas_per_sm <= 32 &&
+           c.min_rows >= 1 && c.pipeline >= 0 && c.pipeline <= 2;
 }
 
 // ---------------------------------------------------------------------------
@@ -141,12 +144,43 @@ struct ElastPhys {
         T* div_out;
         T div_scale;
         int mix;   // 0: out = S; 1: out = a f + b S
+        static constexpr int PMAX = 20;
+        const T* planes[PMAX];   // input planes in from_smem order (bulk-copy kernel)
+        int np;
     };
     struct In {
         T f[8];
         T r[RESID ? 8 : 1];
         T F0, F1;
     };
+    // Input planes: f[0..7], resid[0..7] (RESID), force[0..1], fext[0..1].
+    static int make_planes(Args& a) {
+        int k = 0;
+        for (int i = 0; i < 8; ++i) a.planes[k++] = a.f_in + i * a.geom.plane;
+        if (RESID)
+            for (int i = 0; i < 8; ++i) a.planes[k++] = a.resid + i * a.geom.plane;
+        if (a.force) { a.planes[k++] = a.force; a.planes[k++] = a.force + a.geom.plane; }
+        if (a.fext) { a.planes[k++] = a.fext; a.planes[k++] = a.fext + a.geom.plane; }
+        a.np = k;
+        return k;
+    }
+    __device__ static void from_smem(const Args& p, const T* s, int rs, int col, In& in) {
+        int k = 0;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) in.f[i] = s[(k++) * rs + col];
+        if (RESID) {
+#pragma unroll
+            for (int i = 0; i < 8; ++i) in.r[i] = s[(k++) * rs + col];
+        }
+        T F0 = T(0), F1 = T(0);
+        if (p.force) { F0 = s[k * rs + col]; F1 = s[(k + 1) * rs + col]; k += 2; }
+        if (p.fext) {
+            const T e0 = s[k * rs + col], e1 = s[(k + 1) * rs + col];
+            if (p.force) { F0 = F0 + e0; F1 = F1 + e1; } else { F0 = e0; F1 = e1; }
+        }
+        in.F0 = F0;
+        in.F1 = F1;
+    }
     __device__ static void load(const Args& p, int y, int x, In& in) {
         const size_t o = (size_t)y * p.geom.pitch + x;
         const long long P = p.geom.plane;
@@ -219,12 +253,35 @@ struct DarcyPhys {
         const T* ext;
         RulesView<T, 9> pc, ps;
         double* sumsq;
+        static constexpr int PMAX = 12;
+        const T* planes[PMAX];   // input planes in from_smem order (bulk-copy kernel)
+        int np;
     };
     struct In {
         T f[9];
         T S;
         T om;
     };
+    // Input planes: f[0..8], omega (per cell), source, ext_source.
+    static int make_planes(Args& a) {
+        int k = 0;
+        for (int i = 0; i < 9; ++i) a.planes[k++] = a.f_in + i * a.geom.plane;
+        if (a.omega_f) a.planes[k++] = a.omega_f;
+        if (a.source) a.planes[k++] = a.source;
+        if (a.ext) a.planes[k++] = a.ext;
+        a.np = k;
+        return k;
+    }
+    __device__ static void from_smem(const Args& p, const T* s, int rs, int col, In& in) {
+        int k = 0;
+#pragma unroll
+        for (int i = 0; i < 9; ++i) in.f[i] = s[(k++) * rs + col];
+        in.om = p.omega_f ? s[(k++) * rs + col] : p.omega;
+        T S = T(0);
+        if (p.source) S = s[(k++) * rs + col];
+        if (p.ext) S = p.source ? S + s[(k++) * rs + col] : s[(k++) * rs + col];
+        in.S = S;
+    }
     __device__ static void load(const Args& p, int y, int x, In& in) {
         const size_t o = (size_t)y * p.geom.pitch + x;
         const long long P = p.geom.plane;
@@ -277,7 +334,26 @@ struct DarcyPhys {
 // Launch geometry of the sweeps: tx owned columns per CTA, strips of rows
 // chosen so that the grid holds about ctas_per_sm CTAs per SM (one wave),
 // never shorter than min_rows rows (each strip recomputes two halo rows).
+struct WarpGrid {
+    int nbx, nstrips, ctas;
+};
+
+static WarpGrid warp_grid(const XlbbGrid* g, const XlbbSweepConfig& c) {
+    WarpGrid w;
+    w.nbx = (g->nx + WARP_COLS - 1) / WARP_COLS;
+    const int target = c.ctas_per_sm * 4 * num_sms();
+    int ns = target / w.nbx;
+    const int max_s = g->ny / c.min_rows > 0 ? g->ny / c.min_rows : 1;
+    if (ns > max_s) ns = max_s;
+    if (ns < 1) ns = 1;
+    if (ns > g->ny) ns = g->ny;
+    w.nstrips = ns;
+    w.ctas = (w.nbx * ns + 3) / 4;
+    return w;
+}
+
 static dim3 sweep_grid(const XlbbGrid* g, const XlbbSweepConfig& c) {
+    if (c.pipeline == 2) return dim3(warp_grid(g, c).ctas, 1);
     const int nbx = (g->nx + c.tx - 1) / c.tx;
     const int target = c.ctas_per_sm * num_sms();
     int nby = target / nbx;
@@ -289,19 +365,68 @@ static dim3 sweep_grid(const XlbbGrid* g, const XlbbSweepConfig& c) {
 }
 
 // Runtime (tx, depth) -> template instance.
+template <class Ph, int TX, int D, bool PREV>
+static void launch_bulk(dim3 grid, cudaStream_t st, const typename Ph::Args& a) {
+    using T = typename Ph::T;
+    static size_t configured = 0;   // max dynamic smem already granted to this instance
+    const size_t bytes = bulk_smem_bytes<T, Ph::Q, TX, D>(a.np);
+    auto k = sweep_bulk_kernel<Ph, TX, D, PREV>;
+    if (bytes > configured) {
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+        configured = bytes;
+    }
+    k<<<grid, TX + 32, bytes, st>>>(a);
+}
+
+// 16-byte alignment of every input plane and of the row pitch: the bulk copies need it.
+template <class Ph>
+static bool bulk_aligned(const typename Ph::Args& a) {
+    using T = typename Ph::T;
+    if ((a.geom.pitch * sizeof(T)) % 16 != 0) return false;
+    for (int k = 0; k < a.np; ++k)
+        if (reinterpret_cast<uintptr_t>(a.planes[k]) % 16 != 0) return false;
+    return true;
+}
+
+// Runtime (bulk, tx, depth) -> template instance.  The register-prefetch
+// kernel takes depth 1..2, the bulk-copy ring depth 2, 4 or 6; FP64 uses
+// tx = 128 (larger rings exceed the shared memory of one SM).
 template <class Ph, bool PREV>
-static void launch_sweep(const XlbbSweepConfig& c, dim3 grid, cudaStream_t st, const typename Ph::Args& a) {
+static void launch_sweep(XlbbSweepConfig c, const XlbbGrid* g, cudaStream_t st, typename Ph::Args& a) {
+    constexpr bool F32 = sizeof(typename Ph::T) == 4;
+    const dim3 grid = sweep_grid(g, c);
+    if (c.pipeline == 2) {
+        const WarpGrid wg = warp_grid(g, c);
+        if (c.depth == 2) sweep_warp_kernel<Ph, 2, PREV><<<wg.ctas, 128, 0, st>>>(a, wg.nbx, wg.nstrips);
+        else sweep_warp_kernel<Ph, 1, PREV><<<wg.ctas, 128, 0, st>>>(a, wg.nbx, wg.nstrips);
+        return;
+    }
+    Ph::make_planes(a);
+    if (c.pipeline == 1 && !bulk_aligned<Ph>(a)) {
+        c.pipeline = 0;
+        c.depth = c.depth > 2 ? 2 : c.depth;
+    }
+    if (c.pipeline == 1) {
+#define XLBB_BULK(TX_, D_)                                              \
+    if (c.tx == TX_ && c.depth == D_) {                                  \
+        launch_bulk<Ph, TX_, D_, PREV>(grid, st, a);                     \
+        return;                                                          \
+    }
+        XLBB_BULK(128, 2) XLBB_BULK(128, 4)
+        if constexpr (F32) { XLBB_BULK(128, 6) XLBB_BULK(256, 2) XLBB_BULK(256, 4) XLBB_BULK(256, 6) }
+#undef XLBB_BULK
+        launch_bulk<Ph, 128, 2, PREV>(grid, st, a);
+        return;
+    }
 #define XLBB_CASE(TX_, D_)                                                            \
     if (c.tx == TX_ && c.depth == D_) {                                                \
         sweep_kernel<Ph, TX_, D_, PREV><<<grid, TX_ + 32, 0, st>>>(a);                 \
         return;                                                                        \
     }
-    XLBB_CASE(64, 1) XLBB_CASE(64, 2) XLBB_CASE(64, 3)
-    XLBB_CASE(128, 1) XLBB_CASE(128, 2) XLBB_CASE(128, 3)
-    if constexpr (sizeof(typename Ph::T) == 4) {   // FP64 rings of 256 columns exceed 48 KB
-        XLBB_CASE(256, 1) XLBB_CASE(256, 2) XLBB_CASE(256, 3)
-    }
+    XLBB_CASE(128, 1) XLBB_CASE(128, 2)
+    if constexpr (F32) { XLBB_CASE(256, 1) XLBB_CASE(256, 2) }
 #undef XLBB_CASE
+    sweep_kernel<Ph, 128, 1, PREV><<<grid, 128 + 32, 0, st>>>(a);
 }
 
 // The configuration a launch actually uses (FP64 caps tx at 128).
@@ -550,7 +675,7 @@ static int launch_elast(const XlbbGrid* g, const XlbbElastMaterial* mat, const X
     a.div_out = static_cast<T*>(s->div_out);
     a.div_scale = T(-1.5 / (3.0 * (mat->lam + mat->mu) + 1.0));
     const XlbbSweepConfig c = effective_cfg(0, sizeof(T) == 4 ? XLBB_F32 : XLBB_F64);
-    launch_sweep<Ph, PREV>(c, sweep_grid(g, c), st, a);
+    launch_sweep<Ph, PREV>(c, g, st, a);
     return check_launch("xlbb_elast_sweep");
 }
 
@@ -576,8 +701,8 @@ static int darcy_sweep_t(const XlbbGrid* g, const XlbbDarcySweep* s, cudaStream_
     a.ps = rules_view<T, 9>(s->ps);
     a.sumsq = s->sumsq;
     const XlbbSweepConfig c = effective_cfg(1, sizeof(T) == 4 ? XLBB_F32 : XLBB_F64);
-    if (s->sumsq) launch_sweep<Ph, true>(c, sweep_grid(g, c), st, a);
-    else launch_sweep<Ph, false>(c, sweep_grid(g, c), st, a);
+    if (s->sumsq) launch_sweep<Ph, true>(c, g, st, a);
+    else launch_sweep<Ph, false>(c, g, st, a);
     return check_launch("xlbb_darcy_sweep");
 }
 
@@ -613,6 +738,17 @@ int xlbb_sweep_set_config(int kernel, const XlbbSweepConfig* cfg) {
     return XLBB_OK;
 }
 
+int xlbb_device_status(int* status, int reset) {
+    if (!status) return fail(XLBB_EBADARG, "xlbb_device_status: bad argument");
+    cudaError_t e = cudaMemcpyFromSymbol(status, g_xlbb_status, sizeof(int));
+    if (e == cudaSuccess && reset) {
+        const int zero = 0;
+        e = cudaMemcpyToSymbol(g_xlbb_status, &zero, sizeof(int));
+    }
+    if (e != cudaSuccess) return fail(XLBB_ELAUNCH, cudaGetErrorString(e));
+    return XLBB_OK;
+}
+
 int xlbb_sweep_get_config(int kernel, XlbbSweepConfig* cfg) {
     if ((kernel != 0 && kernel != 1) || !cfg) return fail(XLBB_EBADARG, "xlbb_sweep_get_config: bad argument");
     *cfg = g_cfg[kernel];
@@ -624,6 +760,7 @@ int xlbb_elast_sweep(int dtype, const XlbbGrid* g, const XlbbElastMaterial* mat,
     if (!grid_ok(g) || !mat || !s || !s->f_in || !s->f_out) return fail(XLBB_EBADARG, "xlbb_elast_sweep: bad argument");
     if (s->f_in == s->f_out) return fail(XLBB_EBADARG, "xlbb_elast_sweep: f_in and f_out must differ");
     if (!rules_ok(s->pc, g) || !rules_ok(s->ps, g)) return fail(XLBB_EBADARG, "xlbb_elast_sweep: incomplete rules");
+
     if ((mat->mu_field == nullptr) != (mat->lam_field == nullptr))
         return fail(XLBB_EBADARG, "xlbb_elast_sweep: lam_field and mu_field go together");
     if (dtype == XLBB_F32) return elast_sweep_t<float>(g, mat, s, XLBB_STREAM(stream));
@@ -635,6 +772,7 @@ int xlbb_darcy_sweep(int dtype, const XlbbGrid* g, const XlbbDarcySweep* s, void
     if (!grid_ok(g) || !s || !s->f_in || !s->f_out) return fail(XLBB_EBADARG, "xlbb_darcy_sweep: bad argument");
     if (s->f_in == s->f_out) return fail(XLBB_EBADARG, "xlbb_darcy_sweep: f_in and f_out must differ");
     if (!rules_ok(s->pc, g) || !rules_ok(s->ps, g)) return fail(XLBB_EBADARG, "xlbb_darcy_sweep: incomplete rules");
+
     if (dtype == XLBB_F32) return darcy_sweep_t<float>(g, s, XLBB_STREAM(stream));
     if (dtype == XLBB_F64) return darcy_sweep_t<double>(g, s, XLBB_STREAM(stream));
     return fail(XLBB_EUNSUPPORTED, "xlbb_darcy_sweep: dtype");
