@@ -144,6 +144,27 @@ int xlbb_darcy_sweep(int dtype, const XlbbGrid* g, const XlbbDarcySweep* s, void
 int xlbb_darcy_sweep_ctas(const XlbbGrid* g);
 
 /*
+ * Darcy sweep plus its FP64 convergence residual, allocating nothing.
+ * No counterpart in the reference: it exists for callers that cannot allocate
+ * device memory (inside a CUDA-graph capture, host runtimes that hand the
+ * library only the buffers they own, processes with a fixed memory budget).
+ * The caller passes the sweep's inputs and outputs as for xlbb_darcy_sweep
+ * (s->sumsq is ignored) plus sumsq_out, one device double that receives
+ * sum((f_out - f_in)^2).  The per-CTA partial sums go to a scratch array built
+ * into the library: XLBB_NOALLOC_MAX_PARTIALS doubles (128 KiB) held by every
+ * GPU that loads the library until exit; launch shapes needing more CTAs are
+ * rejected with XLBB_EBADARG.  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress), so make that first call
+ * before any stream capture.  All calls share the array, which keeps the last
+ * call's contents (each used slot is rewritten before it is read, so nothing
+ * needs clearing); calls that overlap on the GPU (concurrent streams) race.
+ */
+#define XLBB_NOALLOC_MAX_PARTIALS 16384
+#define XLBB_NOALLOC_MAX_DEVICES 64
+int xlbb_darcy_sweep_residual_noalloc(int dtype, const XlbbGrid* g, const XlbbDarcySweep* s,
+                                      double* sumsq_out, void* stream);
+
+/*
  * Isotropic 9-point gradient of a scalar field with the ADR (anti-)bounce-back
  * rules applied to the shifted copies (AdvectionDiffusionReactionBGK.gradient,
  * src/darcy.py:75-104):  out = base + gradient(q, scale)  (2 planes; base may

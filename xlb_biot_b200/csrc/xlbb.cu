@@ -5,6 +5,7 @@
 #include <stdint.h>
 #include <stdio.h>
 #include <string.h>
+#include <mutex>
 #include <string>
 
 #include "xlbb.h"
@@ -897,6 +898,68 @@ int xlbb_sumsq(int dtype, const XlbbGrid* g, int nplanes, const void* data, int 
                                                                   by0, by1, partials);
     else return fail(XLBB_EUNSUPPORTED, "xlbb_sumsq: dtype");
     return check_launch("xlbb_sumsq");
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Darcy sweep + FP64 residual without caller-provided scratch.
+//
+// Some callers cannot allocate device memory: code running inside a CUDA
+// graph being captured, a host runtime that hands this library only the
+// buffers it owns (inputs and outputs), or a process whose allocator is not
+// allowed to grow.  For them the per-CTA FP64 partial sums of the residual
+// live in this file-scope device array (XLBB_NOALLOC_MAX_PARTIALS doubles,
+// 128 KiB, held by every GPU that loads the library until the process exits).
+// Host code only uses the array's device address, obtained once per device
+// with cudaGetSymbolAddress while that device is current.
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) double g_noalloc_partials[XLBB_NOALLOC_MAX_PARTIALS];
+
+static std::mutex g_noalloc_mutex;
+static double* g_noalloc_addr[XLBB_NOALLOC_MAX_DEVICES] = {nullptr};
+
+// Device address of the scratch array on the current device (looked up on the
+// first call per device).
+static int noalloc_scratch(double** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return fail(XLBB_ELAUNCH, cudaGetErrorString(e));
+    if (dev < 0 || dev >= XLBB_NOALLOC_MAX_DEVICES)
+        return fail(XLBB_EUNSUPPORTED, "xlbb_darcy_sweep_residual_noalloc: device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (g_noalloc_addr[dev] == nullptr) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_partials);
+        if (e != cudaSuccess || p == nullptr) {
+            g_last_error = std::string("xlbb_darcy_sweep_residual_noalloc: cudaGetSymbolAddress failed: ") +
+                           cudaGetErrorString(e);
+            return XLBB_ELAUNCH;
+        }
+        g_noalloc_addr[dev] = static_cast<double*>(p);
+    }
+    *out = g_noalloc_addr[dev];
+    return XLBB_OK;
+}
+
+extern "C" {
+
+int xlbb_darcy_sweep_residual_noalloc(int dtype, const XlbbGrid* g, const XlbbDarcySweep* s, double* sumsq_out,
+                                      void* stream) {
+    if (!grid_ok(g) || !s || !sumsq_out) return fail(XLBB_EBADARG, "xlbb_darcy_sweep_residual_noalloc: bad argument");
+    const int n = xlbb_darcy_sweep_ctas(g);
+    if (n < 0) return n;
+    if (n > XLBB_NOALLOC_MAX_PARTIALS)
+        return fail(XLBB_EBADARG, "xlbb_darcy_sweep_residual_noalloc: the launch shape needs more CTA partials than "
+                                  "the 16384 of the built-in scratch (lower ctas_per_sm)");
+    double* scratch = nullptr;
+    const int rc = noalloc_scratch(&scratch);
+    if (rc != XLBB_OK) return rc;
+    XlbbDarcySweep local = *s;
+    local.sumsq = scratch;      // every used slot is written by its CTA before the reduction reads it
+    const int st = xlbb_darcy_sweep(dtype, g, &local, stream);
+    if (st != XLBB_OK) return st;
+    return xlbb_reduce_sum(scratch, n, sumsq_out, stream);
 }
 
 int xlbb_reduce_sum(const double* partials, int n, double* out, void* stream) {
