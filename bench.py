@@ -305,6 +305,99 @@ def run_ours(args):
     return 0
 
 
+def _timed(fn):
+    import torch
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    out = fn()
+    b.record()
+    torch.cuda.synchronize()
+    return out, a.elapsed_time(b) * 1e-3
+
+
+def run_c1(args):
+    """Plain elasticity, 128^2 periodic, lam = mu = 1, manufactured force, zero
+    start, pseudo-time to a relative residual of 1e-8 (graph-captured sweeps,
+    FP64 residual every 200 sweeps); FP32 and FP64 runs."""
+    import numpy as np
+    import torch
+    import xlb_biot_b200.api as G
+    from xlb_biot_b200.workloads import plain_elasticity_128
+    res = {}
+    for prec in ("f32/f32", "f64/f64"):
+        s, u = plain_elasticity_128(G, precision=prec)
+        s.solve(tol=1e-3, check_every=200)                 # warm-up (module load, capture)
+        (f, it, rel), t = _timed(lambda: s.solve(tol=1e-8, check_every=200))
+        eta, _ = s.update_macroscopic(f)
+        res[prec] = (eta.double().cpu().numpy(), it, rel, t, s.stalled)
+    e32, it, rel, t, stalled = res["f32/f32"]
+    e64, it64, rel64, t64, _ = res["f64/f64"]
+    _, u = plain_elasticity_128(G, precision="f64/f64")
+    line = {"workload": "c1_plain_elasticity_128x128_periodic", "metric": "GLUPS",
+            "value": 128 * 128 * it64 / t64 / 1e9, "unit": "GLUPS", "dtype": "f64 (reaches 1e-8)",
+            "time_to_solution_s": t64, "sweeps": it64, "relative_residual": rel64,
+            "rel_err_vs_exact": float(np.linalg.norm(e64 - u) / np.linalg.norm(u)),
+            "fp32": {"glups": 128 * 128 * it / t / 1e9, "seconds": t, "sweeps": it, "relative_residual": rel,
+                     "stalled_at_rounding_floor": bool(stalled),
+                     "rel_err_vs_exact": float(np.linalg.norm(e32 - u) / np.linalg.norm(u)),
+                     "rel_err_vs_fp64": float(np.linalg.norm(e32 - e64) / np.linalg.norm(e64))},
+            "note": "L2-resident 0.5 MB problem: launch/latency bound, sweeps replayed as CUDA graphs; "
+                    "FP32 residuals cannot fall below ~1e-5 of the first update"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_c3(args):
+    """Periodic Biot 1024^2, 5-level V-cycle elasticity (FP32, FP64 coarsest
+    level, 8 V-cycles per step as the reference's fixed N_E), FP64 pressure;
+    compared with the all-FP64 run."""
+    import numpy as np
+    import torch
+    import xlb_biot_b200.api as G
+    from xlb_biot_b200.workloads import periodic_biot_1024
+    steps = args.biot_steps
+
+    def run(prec, dprec, coarse):
+        sim = periodic_biot_1024(G, precision=prec, darcy_precision=dprec, coarsest_precision=coarse)
+        el, da, dt = sim.init_state()
+        sim.step(el, da, dt, 0)                              # warm-up step
+        el, da, dt = sim.init_state()
+        cycles = 0
+
+        def body():
+            nonlocal el, da, dt, cycles
+            out = None
+            for t in range(steps):
+                out = sim.step(el, da, dt, t)
+                el, da, dt = out[0], out[1], out[4]
+                cycles += getattr(sim, "last_inner_cycles", sim.elasticitySteps) \
+                    if sim.elasticityTol is not None else sim.elasticitySteps
+            return out
+        out, secs = _timed(body)
+        return sim, out, cycles, secs
+
+    sim, out, cycles, secs = run("f32/f32", "f64/f64", "f64")
+    n, L, k = 1024, 5, sim.elasticity.k_smooth
+    sizes = [(n // 2 ** l) ** 2 for l in range(L)]
+    lu_cycle = sum((2 * k + 1) * s for s in sizes[:-1]) + 2 * k * sizes[-1]
+    lus = cycles * lu_cycle + steps * n * n
+    ref = run("f64/f64", "f64/f64", None)
+    eta = sim.elasticity.update_macroscopic(out[0])[0].double().cpu().numpy()
+    eta_r = ref[0].elasticity.update_macroscopic(ref[1][0])[0].cpu().numpy()
+    p, p_r = out[5].double().cpu().numpy(), ref[1][5].cpu().numpy()
+    line = {"workload": "c3_periodic_biot_1024x1024_mg5", "metric": "GLUPS", "value": lus / secs / 1e9,
+            "unit": "GLUPS", "biot_steps": steps, "vcycles": cycles, "lattice_updates": lus,
+            "seconds": secs, "dtype": "f32 elasticity, f64 coarsest level, f64 pressure",
+            "material": "E=0.11, nu=0.8 (reference periodic examples); lam=2, mu=1 diverges in the reference's V-cycle",
+            "inner_solve": f"{sim.elasticitySteps} V-cycles per step (the reference's fixed N_E)",
+            "rel_err_u_vs_fp64": float(np.linalg.norm(eta - eta_r) / np.linalg.norm(eta_r)),
+            "rel_err_p_vs_fp64": float(np.linalg.norm(p - p_r) / np.linalg.norm(p_r)),
+            "fp64": {"seconds": ref[3], "vcycles": ref[2]}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -314,11 +407,18 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--launch-shape", default="",
                     help="tx,depth,ctas_per_sm,min_rows,pipeline of the Darcy sweep (skips the autotuner)")
+    ap.add_argument("--workload", choices=["darcy", "c1", "c3"], default="darcy",
+                    help="darcy: the headline line; c1/c3: the other configurations (one JSON line each)")
+    ap.add_argument("--biot-steps", type=int, default=100)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "c1":
+        return run_c1(args)
+    if args.workload == "c3":
+        return run_c3(args)
     return run_ours(args)
 
 

@@ -101,8 +101,9 @@ typedef struct {
  * a=1-gamma,b=gamma the damped smoothing sweep of _mg_step (:1258-1267);
  * a=1,b=-1 the residual f - STEP(f - r) (:1285-1286).
  * STEP applies force (if use_force) + fext as in collision() (:959-1000).
- * If sumsq != NULL, each CTA writes sum(out^2) over the box [bx0,bx1)x[by0,by1)
- * into sumsq[cta] (FP64; reduce with xlbb_reduce_sum); count via
+ * If sumsq != NULL, each CTA writes sum(out^2) (sumsq_diff = 0) or
+ * sum((out - f_in)^2) (sumsq_diff = 1) over the box [bx0,bx1)x[by0,by1) into
+ * sumsq[cta] (FP64; reduce with xlbb_reduce_sum); count via
  * xlbb_elast_sweep_ctas().  If div_out != NULL the divergence moment of out
  * (update_divergence, :1040-1058) is written as a side output.
  */
@@ -118,6 +119,7 @@ typedef struct {
     double* sumsq;
     int bx0, bx1, by0, by1;
     void* div_out;
+    int sumsq_diff;
 } XlbbElastSweep;
 
 int xlbb_elast_sweep(int dtype, const XlbbGrid* g, const XlbbElastMaterial* mat,
@@ -202,10 +204,12 @@ int xlbb_darcy_moments(int dtype, const XlbbGrid* g, const void* f, double omega
  * the coarse grid's interior and zeros outside it; prolong_add adds the coarse
  * interior, injected, into the fine interior.
  */
-int xlbb_restrict(int dtype, const XlbbGrid* fine, const XlbbGrid* coarse, int q,
+int xlbb_restrict(int dtype_fine, int dtype_coarse, const XlbbGrid* fine, const XlbbGrid* coarse, int q,
                   int x0, int x1bc, int y0, int y1bc, const void* res, void* r_coarse, void* stream);
-int xlbb_prolong_add(int dtype, const XlbbGrid* fine, const XlbbGrid* coarse, int q,
+int xlbb_prolong_add(int dtype_fine, int dtype_coarse, const XlbbGrid* fine, const XlbbGrid* coarse, int q,
                      int x0, int x1bc, int y0, int y1bc, const void* f_coarse, void* f_fine, void* stream);
+/* dtype pairs (fine, coarse): (F32, F32), (F32, F64) -- an FP64 coarsest level
+ * under FP32 levels -- and (F64, F64). */
 
 /* Deterministic FP64 sum of n partials (fixed order) into *out. */
 int xlbb_reduce_sum(const double* partials, int n, double* out, void* stream);

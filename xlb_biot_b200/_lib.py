@@ -45,7 +45,8 @@ class ElastSweep(ctypes.Structure):
                 ("use_force", ctypes.c_int), ("fext", ctypes.c_void_p), ("resid", ctypes.c_void_p),
                 ("a", ctypes.c_double), ("b", ctypes.c_double), ("pc", Rules), ("ps", Rules),
                 ("sumsq", ctypes.c_void_p), ("bx0", ctypes.c_int), ("bx1", ctypes.c_int),
-                ("by0", ctypes.c_int), ("by1", ctypes.c_int), ("div_out", ctypes.c_void_p)]
+                ("by0", ctypes.c_int), ("by1", ctypes.c_int), ("div_out", ctypes.c_void_p),
+                ("sumsq_diff", ctypes.c_int)]
 
 
 class DarcySweep(ctypes.Structure):
@@ -68,8 +69,8 @@ SIGNATURES = {
     "xlbb_elast_moments": (I, [I, PG, ctypes.POINTER(ElastMaterial), P, P, P, P, P, P, D, P]),
     "xlbb_elast_equilibrium": (I, [I, PG, ctypes.POINTER(ElastMaterial), P, P, P, P, P, P]),
     "xlbb_darcy_moments": (I, [I, PG, P, D, P, P, P, P, P, P]),
-    "xlbb_restrict": (I, [I, PG, PG, I, I, I, I, I, P, P, P]),
-    "xlbb_prolong_add": (I, [I, PG, PG, I, I, I, I, I, P, P, P]),
+    "xlbb_restrict": (I, [I, I, PG, PG, I, I, I, I, I, P, P, P]),
+    "xlbb_prolong_add": (I, [I, I, PG, PG, I, I, I, I, I, P, P, P]),
     "xlbb_reduce_sum": (I, [P, I, P, P]),
     "xlbb_sumsq": (I, [I, PG, I, P, I, I, I, I, P, P]),
     "xlbb_sumsq_ctas": (I, [PG]),

@@ -7,6 +7,7 @@
 #include <string.h>
 #include <mutex>
 #include <string>
+#include <type_traits>
 
 #include "xlbb.h"
 #include "xlbb_common.cuh"
@@ -145,6 +146,7 @@ struct ElastPhys {
         T* div_out;
         T div_scale;
         int mix;   // 0: out = S; 1: out = a f + b S
+        int sumsq_diff;   // sumsq of (out - f_in) instead of out
         static constexpr int PMAX = 20;
         const T* planes[PMAX];   // input planes in from_smem order (bulk-copy kernel)
         int np;
@@ -224,9 +226,15 @@ struct ElastPhys {
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
             T v = S[i];
-            if constexpr (PREV) v = p.a * fprev[i] + p.b * S[i];
+            if constexpr (PREV) {
+                if (p.mix) v = p.a * fprev[i] + p.b * S[i];
+            }
             p.f_out[o + i * P] = v;
-            acc += (double)v * (double)v;
+            double d = (double)v;
+            if constexpr (PREV) {
+                if (p.sumsq_diff) d -= (double)fprev[i];
+            }
+            acc += d * d;
             m2 += (i < 4 ? T(1) : T(2)) * v;
         }
         if (p.div_out) p.div_out[o] = p.div_scale * m2;
@@ -579,10 +587,13 @@ __global__ void darcy_moments_kernel(SweepGeom G, const T* f, T omega, const T* 
     }
 }
 
-template <typename T>
-__global__ void restrict_kernel(SweepGeom F, SweepGeom C, int q, int x0, int y0, int nix, int niy, const T* res,
-                                T* rc) {
+// Tf: fine-level type, Tc: coarse-level type (a multigrid may run its coarsest
+// level in FP64 under FP32 levels; the sum is formed in the wider type).
+template <typename Tf, typename Tc>
+__global__ void restrict_kernel(SweepGeom F, SweepGeom C, int q, int x0, int y0, int nix, int niy, const Tf* res,
+                                Tc* rc) {
     // one thread per coarse cell (all q planes); zero outside the coarse interior
+    using Ts = typename std::conditional<(sizeof(Tf) > sizeof(Tc)), Tf, Tc>::type;
     const int X = blockIdx.x * blockDim.x + threadIdx.x;
     const int Y = blockIdx.y;
     if (X >= C.nx) return;
@@ -590,25 +601,25 @@ __global__ void restrict_kernel(SweepGeom F, SweepGeom C, int q, int x0, int y0,
     const int I = X - x0, J = Y - y0;
     const bool inside = I >= 0 && I < nix && J >= 0 && J < niy;
     for (int i = 0; i < q; ++i) {
-        T v = T(0);
+        Ts v = Ts(0);
         if (inside) {
             const size_t of = (size_t)(y0 + 2 * J) * F.pitch + (x0 + 2 * I) + (size_t)i * F.plane;
-            const T a = res[of], b = res[of + 1], c = res[of + F.pitch], d = res[of + F.pitch + 1];
-            v = a + c + b + d;   // conv window order (x, y): (0,0),(0,1),(1,0),(1,1) summed pairwise in y first
+            const Ts a = res[of], b = res[of + 1], c = res[of + F.pitch], d = res[of + F.pitch + 1];
+            v = a + c + b + d;
         }
-        rc[oc + (size_t)i * C.plane] = v;
+        rc[oc + (size_t)i * C.plane] = Tc(v);
     }
 }
 
-template <typename T>
+template <typename Tf, typename Tc>
 __global__ void prolong_add_kernel(SweepGeom F, SweepGeom C, int q, int x0, int y0, int nfx, int nfy,
-                                   const T* fc, T* ff) {
+                                   const Tc* fc, Tf* ff) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y;
     if (i >= nfx || j >= nfy) return;
     const size_t of = (size_t)(y0 + j) * F.pitch + (x0 + i);
     const size_t oc = (size_t)(y0 + j / 2) * C.pitch + (x0 + i / 2);
-    for (int k = 0; k < q; ++k) ff[of + (size_t)k * F.plane] += fc[oc + (size_t)k * C.plane];
+    for (int k = 0; k < q; ++k) ff[of + (size_t)k * F.plane] = Tf(ff[of + (size_t)k * F.plane] + fc[oc + (size_t)k * C.plane]);
 }
 
 template <typename T>
@@ -667,7 +678,8 @@ static int launch_elast(const XlbbGrid* g, const XlbbElastMaterial* mat, const X
     a.resid = static_cast<const T*>(s->resid);
     a.a = T(s->a);
     a.b = T(s->b);
-    a.mix = PREV ? 1 : 0;
+    a.mix = (s->a == 0.0 && s->b == 1.0) ? 0 : 1;
+    a.sumsq_diff = (s->sumsq != nullptr && s->sumsq_diff) ? 1 : 0;
     a.mat = make_mat<T>(mat);
     a.pc = rules_view<T, 8>(s->pc);
     a.ps = rules_view<T, 8>(s->ps);
@@ -682,7 +694,8 @@ static int launch_elast(const XlbbGrid* g, const XlbbElastMaterial* mat, const X
 
 template <typename T>
 static int elast_sweep_t(const XlbbGrid* g, const XlbbElastMaterial* mat, const XlbbElastSweep* s, cudaStream_t st) {
-    const bool mix = !(s->a == 0.0 && s->b == 1.0);
+    // the previous populations are kept when mixed or differenced
+    const bool mix = !(s->a == 0.0 && s->b == 1.0) || (s->sumsq != nullptr && s->sumsq_diff);
     if (s->resid) return mix ? launch_elast<T, true, true>(g, mat, s, st) : launch_elast<T, true, false>(g, mat, s, st);
     return mix ? launch_elast<T, false, true>(g, mat, s, st) : launch_elast<T, false, false>(g, mat, s, st);
 }
@@ -843,39 +856,41 @@ int xlbb_darcy_moments(int dtype, const XlbbGrid* g, const void* f, double omega
     return check_launch("xlbb_darcy_moments");
 }
 
-int xlbb_restrict(int dtype, const XlbbGrid* fine, const XlbbGrid* coarse, int q, int x0, int x1bc, int y0, int y1bc,
-                  const void* res, void* r_coarse, void* stream) {
+int xlbb_restrict(int dtype_fine, int dtype_coarse, const XlbbGrid* fine, const XlbbGrid* coarse, int q, int x0,
+                  int x1bc, int y0, int y1bc, const void* res, void* r_coarse, void* stream) {
     if (!grid_ok(fine) || !grid_ok(coarse) || !res || !r_coarse || q <= 0)
         return fail(XLBB_EBADARG, "xlbb_restrict: bad argument");
     const int nfx = fine->nx - x0 - x1bc, nfy = fine->ny - y0 - y1bc;
     if (nfx % 2 || nfy % 2 || coarse->nx != nfx / 2 + x0 + x1bc || coarse->ny != nfy / 2 + y0 + y1bc)
         return fail(XLBB_EBADARG, "xlbb_restrict: coarse grid does not match the fine interior");
     const dim3 grid = row_grid(coarse->nx, coarse->ny, 128);
-    if (dtype == XLBB_F32)
-        restrict_kernel<float><<<grid, 128, 0, XLBB_STREAM(stream)>>>(geom(fine), geom(coarse), q, x0, y0, nfx / 2,
-                                                                      nfy / 2, (const float*)res, (float*)r_coarse);
-    else if (dtype == XLBB_F64)
-        restrict_kernel<double><<<grid, 128, 0, XLBB_STREAM(stream)>>>(geom(fine), geom(coarse), q, x0, y0, nfx / 2,
-                                                                       nfy / 2, (const double*)res, (double*)r_coarse);
-    else return fail(XLBB_EUNSUPPORTED, "xlbb_restrict: dtype");
+    cudaStream_t st = XLBB_STREAM(stream);
+#define XLBB_R(TF, TC) \
+    restrict_kernel<TF, TC><<<grid, 128, 0, st>>>(geom(fine), geom(coarse), q, x0, y0, nfx / 2, nfy / 2, (const TF*)res, (TC*)r_coarse)
+    if (dtype_fine == XLBB_F32 && dtype_coarse == XLBB_F32) XLBB_R(float, float);
+    else if (dtype_fine == XLBB_F32 && dtype_coarse == XLBB_F64) XLBB_R(float, double);
+    else if (dtype_fine == XLBB_F64 && dtype_coarse == XLBB_F64) XLBB_R(double, double);
+    else return fail(XLBB_EUNSUPPORTED, "xlbb_restrict: dtype pair");
+#undef XLBB_R
     return check_launch("xlbb_restrict");
 }
 
-int xlbb_prolong_add(int dtype, const XlbbGrid* fine, const XlbbGrid* coarse, int q, int x0, int x1bc, int y0,
-                     int y1bc, const void* f_coarse, void* f_fine, void* stream) {
+int xlbb_prolong_add(int dtype_fine, int dtype_coarse, const XlbbGrid* fine, const XlbbGrid* coarse, int q, int x0,
+                     int x1bc, int y0, int y1bc, const void* f_coarse, void* f_fine, void* stream) {
     if (!grid_ok(fine) || !grid_ok(coarse) || !f_coarse || !f_fine || q <= 0)
         return fail(XLBB_EBADARG, "xlbb_prolong_add: bad argument");
     const int nfx = fine->nx - x0 - x1bc, nfy = fine->ny - y0 - y1bc;
     if (nfx % 2 || nfy % 2 || coarse->nx != nfx / 2 + x0 + x1bc || coarse->ny != nfy / 2 + y0 + y1bc)
         return fail(XLBB_EBADARG, "xlbb_prolong_add: coarse grid does not match the fine interior");
     const dim3 grid = row_grid(nfx, nfy, 128);
-    if (dtype == XLBB_F32)
-        prolong_add_kernel<float><<<grid, 128, 0, XLBB_STREAM(stream)>>>(geom(fine), geom(coarse), q, x0, y0, nfx, nfy,
-                                                                         (const float*)f_coarse, (float*)f_fine);
-    else if (dtype == XLBB_F64)
-        prolong_add_kernel<double><<<grid, 128, 0, XLBB_STREAM(stream)>>>(geom(fine), geom(coarse), q, x0, y0, nfx, nfy,
-                                                                          (const double*)f_coarse, (double*)f_fine);
-    else return fail(XLBB_EUNSUPPORTED, "xlbb_prolong_add: dtype");
+    cudaStream_t st = XLBB_STREAM(stream);
+#define XLBB_P(TF, TC) \
+    prolong_add_kernel<TF, TC><<<grid, 128, 0, st>>>(geom(fine), geom(coarse), q, x0, y0, nfx, nfy, (const TC*)f_coarse, (TF*)f_fine)
+    if (dtype_fine == XLBB_F32 && dtype_coarse == XLBB_F32) XLBB_P(float, float);
+    else if (dtype_fine == XLBB_F32 && dtype_coarse == XLBB_F64) XLBB_P(float, double);
+    else if (dtype_fine == XLBB_F64 && dtype_coarse == XLBB_F64) XLBB_P(double, double);
+    else return fail(XLBB_EUNSUPPORTED, "xlbb_prolong_add: dtype pair");
+#undef XLBB_P
     return check_launch("xlbb_prolong_add");
 }
 

@@ -79,6 +79,7 @@ class AdvectionDiffusionReactionBGK(LBMBase):
         nx, ny = int(q.shape[0]), int(q.shape[1])
         L = self._layout if (nx, ny) == (self.nx, self.ny) else Layout(nx, ny, self._dtype)
         qf = L.field(q, 1)
+        base = L.field(base, 2)     # other precision / layout -> this grid (kept alive over the launch)
         out = L.empty(2) if out is None else out
         rules = self.gradient_rules(nx, ny)
         _lib.check(_lib.lib().xlbb_darcy_gradient(

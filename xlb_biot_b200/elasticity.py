@@ -56,7 +56,12 @@ class LBMElasticity:
         self.sharding = None
         self._dtype = torch_dtype(self.precisionPolicy.compute_dtype)
         self._dcode = _lib.dtype_code(self._dtype)
-        self._layouts = [Layout(*self.grid_size(l), self._dtype) for l in range(self.levels)]
+        # Extension: ``coarsest_precision="f64"`` runs the coarsest multigrid level
+        # in FP64 under FP32 levels (transfers convert in the kernels).
+        self._level_dtypes = [self._dtype] * self.levels
+        if kwargs.get("coarsest_precision") == "f64" and self.levels > 1:
+            self._level_dtypes[-1] = torch.float64
+        self._layouts = [Layout(*self.grid_size(l), self._level_dtypes[l]) for l in range(self.levels)]
         self.boundingBoxIndices = self.bounding_box_indices()
         self._create_boundary_data()
         force = self.get_force()
@@ -291,8 +296,8 @@ class LBMElasticity:
         for level in range(self.levels):
             bcs = self.BCs if level == 0 else self.BCs_MG[level]
             L = self._layouts[level]
-            pc = compile_rules(bcs, L.nx, L.ny, 8, self._dtype, L.device, step="PostCollision")
-            ps = compile_rules(bcs, L.nx, L.ny, 8, self._dtype, L.device, step="PostStreaming")
+            pc = compile_rules(bcs, L.nx, L.ny, 8, L.dtype, L.device, step="PostCollision")
+            ps = compile_rules(bcs, L.nx, L.ny, 8, L.dtype, L.device, step="PostStreaming")
             self._rules.append((pc, ps))
 
     def distributed_array_init(self, shape, type, init_val=0, sharding=None):
@@ -367,7 +372,7 @@ class LBMElasticity:
         f = self._f(f, level)
         div = L.empty(1)
         _lib.check(_lib.lib().xlbb_elast_moments(
-            self._dcode, L.grid(), self._mat, _lib.ptr(f), None, None, None, None, _lib.ptr(div),
+            _lib.dtype_code(L.dtype), L.grid(), self._mat, _lib.ptr(f), None, None, None, None, _lib.ptr(div),
             self._div_scale, _lib.stream_ptr()), "xlbb_elast_moments")
         return div
 
@@ -447,9 +452,12 @@ class LBMElasticity:
         return s.repeat_interleave(2, dim=0).repeat_interleave(2, dim=1)
 
     # ------------------------------------------------------------------ kernels
-    def _sweep(self, f, level, a=0.0, b=1.0, resid=None, fext=None, out=None, sumsq=False, div_out=None):
+    def _sweep(self, f, level, a=0.0, b=1.0, resid=None, fext=None, out=None, sumsq=False, div_out=None,
+               sumsq_diff=False):
         L = self._L(level)
         out = L.empty(8) if out is None else out
+        if fext is not None and not L.conforms(fext, 2):
+            fext = L.field(fext, 2)      # e.g. a coupling force computed in another precision
         if sumsq:
             # one FP64 partial per CTA of the current launch shape
             self._n_partials = _lib.check(_lib.lib().xlbb_elast_sweep_ctas(L.grid()), "xlbb_elast_sweep_ctas")
@@ -461,16 +469,62 @@ class LBMElasticity:
                             1 if level == 0 else 0, fext.data_ptr() if fext is not None else None,
                             resid.data_ptr() if resid is not None else None, float(a), float(b),
                             pc.struct(), ps.struct(), self._partials.data_ptr() if sumsq else None,
-                            bx0, bx1, by0, by1, div_out.data_ptr() if div_out is not None else None)
-        _lib.check(_lib.lib().xlbb_elast_sweep(self._dcode, L.grid(), self._mat, s, _lib.stream_ptr()),
+                            bx0, bx1, by0, by1, div_out.data_ptr() if div_out is not None else None,
+                            1 if sumsq_diff else 0)
+        _lib.check(_lib.lib().xlbb_elast_sweep(_lib.dtype_code(L.dtype), L.grid(), self._mat, s, _lib.stream_ptr()),
                    "xlbb_elast_sweep")
         return out
+
+    def _reduce_partials(self, out_scalar):
+        _lib.check(_lib.lib().xlbb_reduce_sum(self._partials.data_ptr(), self._n_partials, out_scalar.data_ptr(),
+                                              _lib.stream_ptr()), "xlbb_reduce_sum")
+        return out_scalar
+
+    # ------------------------------------------------------------------ tolerance drivers
+    def solve(self, f=None, tol=1e-8, check_every=100, max_sweeps=10 ** 7, external_force=None, stall_checks=20):
+        """Pseudo-time iteration to a relative residual ``||f^{n+1} - f^n|| /
+        ||f^1 - f^0|| < tol`` (FP64 norms on the device).  Single level: sweeps
+        run as one CUDA graph of ``check_every`` sweeps between host checks.
+        Multigrid: V-cycles until the level-0 residual norm drops by ``tol``.
+        Returns ``(f, iterations, relative_residual)``."""
+        f = self.assign_fields_sharded() if f is None else self._f(f)
+        if self.levels > 1:
+            f, r0 = self.step(f, 0, external_force=external_force)
+            r0 = float(r0)
+            it, rel = 1, 1.0
+            while it < max_sweeps:
+                f, r = self.step(f, it, external_force=external_force)
+                it += 1
+                rel = float(r) / r0 if r0 > 0 else 0.0
+                if rel < tol:
+                    break
+            return f, it, rel
+        loop = ElasticLoop(self, check_every, external_force)
+        r0 = loop.first(f)
+        it, rel = 1, 1.0
+        best, since_best = np.inf, 0
+        self.stalled = False
+        while it < max_sweeps:
+            loop.replay()
+            it += loop.n
+            rel = (float(loop.sumsq[0]) ** 0.5) / r0 if r0 > 0 else 0.0
+            if rel < tol or not np.isfinite(rel):
+                break
+            # stop when the residual no longer falls (rounding floor of the precision)
+            if rel < 0.99 * best:
+                best, since_best = rel, 0
+            else:
+                since_best += 1
+                if since_best >= stall_checks:
+                    self.stalled = True
+                    break
+        return loop.result, it, rel
 
     def _restrict_full(self, res, level):
         Lf, Lc = self._L(level), self._L(level + 1)
         rc = Lc.empty(8)
         m = self.mg_BCs
-        _lib.check(_lib.lib().xlbb_restrict(self._dcode, Lf.grid(), Lc.grid(), 8, int(m["left"]), int(m["right"]),
+        _lib.check(_lib.lib().xlbb_restrict(_lib.dtype_code(Lf.dtype), _lib.dtype_code(Lc.dtype), Lf.grid(), Lc.grid(), 8, int(m["left"]), int(m["right"]),
                                             int(m["bottom"]), int(m["top"]), res.data_ptr(), rc.data_ptr(),
                                             _lib.stream_ptr()), "xlbb_restrict")
         return rc
@@ -478,7 +532,7 @@ class LBMElasticity:
     def _prolong_add(self, fc, ff, level):
         Lf, Lc = self._L(level), self._L(level + 1)
         m = self.mg_BCs
-        _lib.check(_lib.lib().xlbb_prolong_add(self._dcode, Lf.grid(), Lc.grid(), 8, int(m["left"]), int(m["right"]),
+        _lib.check(_lib.lib().xlbb_prolong_add(_lib.dtype_code(Lf.dtype), _lib.dtype_code(Lc.dtype), Lf.grid(), Lc.grid(), 8, int(m["left"]), int(m["right"]),
                                                int(m["bottom"]), int(m["top"]), fc.data_ptr(), ff.data_ptr(),
                                                _lib.stream_ptr()), "xlbb_prolong_add")
 
@@ -690,3 +744,42 @@ class ElasticityAntiBounceBack(BoundaryCondition):
         if self.T is not None:
             fbd[:, list(self.i_update)] += self.T_update
         return fbd
+
+
+class ElasticLoop:
+    """``n`` plain elasticity sweeps captured once as a CUDA graph; the last sweep
+    reduces the FP64 residual sum((f_n - f_{n-1})^2) into ``sumsq``."""
+
+    def __init__(self, solver, n, external_force=None):
+        L = solver._L(0)
+        self.solver, self.n = solver, int(n) + (int(n) % 2)   # even: the result lands in ``state``
+        self.state, self._other = L.empty(8), L.empty(8)
+        self.ext = L.field(external_force, 2)
+        self.sumsq = torch.zeros(1, dtype=torch.float64, device=L.device)
+        self.launches_per_replay = self.n + 1
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            self._body()
+        torch.cuda.current_stream().wait_stream(s)
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            self._body()
+        self.result = self.state if self.n % 2 == 0 else self._other
+
+    def _body(self):
+        a, b = self.state, self._other
+        for k in range(self.n):
+            self.solver._sweep(a, 0, fext=self.ext, out=b, sumsq=(k == self.n - 1), sumsq_diff=True)
+            a, b = b, a
+        self.solver._reduce_partials(self.sumsq)
+
+    def first(self, f0):
+        """One sweep from ``f0`` into ``state``; returns ||f^1 - f^0|| (FP64)."""
+        self.solver._sweep(f0, 0, fext=self.ext, out=self.state, sumsq=True, sumsq_diff=True)
+        self.solver._reduce_partials(self.sumsq)
+        return float(self.sumsq[0]) ** 0.5
+
+    def replay(self):
+        self.graph.replay()
+        return self.result

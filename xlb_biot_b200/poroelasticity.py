@@ -40,12 +40,20 @@ class LBMPoroelasticity:
         kwargs_elasticity['MG_levels'] = kwargs.pop('elasticity_MG_levels', 1)
         self.elasticity = LBMElasticity(**kwargs_elasticity)
         kwargs['lattice'] = kwargs.pop('lattice_darcy')
-        self.darcy = LBMDarcy(**kwargs)
+        # Extension: ``darcy_precision`` runs the pressure equation in another
+        # precision than the elasticity solve (e.g. FP64 pressure, FP32 elasticity).
+        kwargs_darcy = dict(kwargs)
+        if kwargs.get('darcy_precision'):
+            kwargs_darcy['precision'] = kwargs['darcy_precision']
+        self.darcy = LBMDarcy(**kwargs_darcy)
         self.elasticitySteps = kwargs.get('elasticity_steps', 1)
         self.alpha = kwargs.get('alpha')
         self.epsilon = kwargs.get('epsilon', 1 / self.elasticity.nx)
         self.couplingMethod = kwargs.get('coupling_method', 'centered')
         self.alternative_gradient = kwargs.get('alternative_gradient', False)
+        self.elasticityTol = kwargs.get('elasticity_tol', None)
+        if self.elasticityTol is not None and self.elasticity.levels < 2:
+            raise ValueError("elasticity_tol needs a multigrid elasticity solver (elasticity_MG_levels > 1)")
         self.downsamplingFactor = kwargs.get("downsampling_factor", 1)
         self.printInfoRate = kwargs.get("print_info_rate", 100)
         self.ioRate = kwargs.get("io_rate", 0)
@@ -244,8 +252,21 @@ class LBMPoroelasticity:
             force = force + self._dyn_force(timestep)
         force = el._L().field(force, 2)
         nonlinear_force = DivGradForce(el, da, 0.5 * th * a ** 2)
-        for _ in range(self.elasticitySteps):
-            f_elasticity, *_ = el.step(f_elasticity, timestep, False, force, nonlinear_force=nonlinear_force)
+        if self.elasticityTol is None:
+            for _ in range(self.elasticitySteps):
+                f_elasticity, *_ = el.step(f_elasticity, timestep, False, force, nonlinear_force=nonlinear_force)
+        else:
+            # Extension: V-cycles until the level-0 residual norm fell by elasticity_tol
+            # (FP64 norm on the device, read once per cycle); elasticity_steps caps the cycles.
+            r0 = None
+            self.last_inner_cycles = 0
+            for k in range(self.elasticitySteps):
+                f_elasticity, r = el.step(f_elasticity, timestep, False, force, nonlinear_force=nonlinear_force)
+                self.last_inner_cycles = k + 1
+                r = float(r)
+                r0 = r if r0 is None else r0
+                if r0 == 0.0 or r / r0 < self.elasticityTol:
+                    break
         eta, sigma = el.update_macroscopic(f_elasticity, nonlinear_force.evaluate(el, f_elasticity, 0, force))
         dt_div_eta = el.update_divergence(f_elasticity - fprev)
         source = da._layout.field(source_base - (th * a / eps) * dt_div_eta, 1)

@@ -49,6 +49,87 @@ def _corner_patched(m):
     return patch(m.ADR_Neumann_BounceBack), patch(m.ADR_AntiBounceBack)
 
 
+def manufactured_elasticity(n, lam, mu):
+    """Displacement u = (sin 2pi x sin 2pi y, cos 2pi x sin 2pi y) on cell centres
+    x = (i + 1/2)/n and the body force eps^2 (-div sigma(u)), eps = 1/n, of plane
+    linear elasticity sigma = lam tr(e) I + 2 mu e (the convention of the
+    reference's periodic example).  Returns (u, force) of shape (n, n, 2)."""
+    x = (np.arange(n) + 0.5) / n
+    X, Y = np.meshgrid(x, x, indexing="ij")
+    s, c = np.sin(2 * np.pi * X), np.cos(2 * np.pi * X)
+    sy, cy = np.sin(2 * np.pi * Y), np.cos(2 * np.pi * Y)
+    u = np.stack((s * sy, c * sy), axis=-1)
+    k2 = 4 * np.pi ** 2
+    # -div sigma = -(lam + mu) grad(div u) - mu lap(u)
+    fx = (lam + mu) * k2 * (s * sy + s * cy) + 2 * k2 * mu * s * sy
+    fy = -(lam + mu) * k2 * (c * cy - c * sy) + 2 * k2 * mu * c * sy
+    return u, np.stack((fx, fy), axis=-1) / n ** 2
+
+
+def plain_elasticity_128(m, n=128, lam=1.0, mu=1.0, precision="f32/f32"):
+    """Plain D2Q8 elasticity on an n x n periodic grid with the manufactured
+    force (no multigrid); populations start at zero."""
+    u, force = manufactured_elasticity(n, lam, mu)
+
+    class Manufactured(m.LBMElasticity):
+        def get_force(self):
+            return self.distributed_array_init((n, n, 2), self.precisionPolicy.compute_dtype, init_val=force)
+
+        def initialize_macroscopic_fields(self):
+            return None, None
+
+    solver = Manufactured(lattice=m.LatticeD2Q8(precision), **{"lambda": lam}, mu=mu, nx=n, ny=n, nz=0,
+                          precision=precision, print_info_rate=0)
+    return solver, u
+
+
+EXAMPLE_E, EXAMPLE_NU = 0.11, 0.8     # material of the reference's periodic examples
+
+
+def periodic_biot_1024(m, n=1024, levels=5, lam=None, mu=None, alpha=1.0, K=0.1, precision="f32/f32",
+                       darcy_precision=None, coarsest_precision=None, tol=None, max_cycles=8):
+    """Periodic Biot consolidation with the initial pressure sin 2pi x sin 2pi y:
+    elasticity with an L-level V-cycle per time step (``max_cycles`` cycles, or
+    until the residual fell by ``tol``), Darcy with K = 0.1 (omega = 1.25),
+    alpha = 1, centred coupling.  The default material is the one of the
+    reference's periodic examples (E = 0.11, nu = 0.8, plane stress); with
+    lam = 2, mu = 1 in lattice units the reference's V-cycle diverges.  The
+    storativity enters through the pressure unit (p in units of 1/c0)."""
+    if lam is None:
+        lam = EXAMPLE_E * EXAMPLE_NU / (1 - EXAMPLE_NU ** 2)
+    if mu is None:
+        mu = 0.5 * EXAMPLE_E / (1 + EXAMPLE_NU)
+    x = (np.arange(n) + 0.5) / n
+    X, Y = np.meshgrid(x, x, indexing="ij")
+    p0 = (np.sin(2 * np.pi * X) * np.sin(2 * np.pi * Y))[..., None]
+
+    class PD(m.AdvectionDiffusionReactionBGK):
+        def initialize_macroscopic_fields(self):
+            return (self.distributed_array_init((n, n, 1), self.precisionPolicy.output_dtype, init_val=p0),
+                    self.distributed_array_init((n, n, 2), self.precisionPolicy.output_dtype, init_val=0.0))
+
+    class PE(m.LBMElasticity):
+        def initialize_macroscopic_fields(self):
+            return (self.distributed_array_init((n, n, 2), self.precisionPolicy.output_dtype, init_val=0.0),
+                    self.distributed_array_init((n, n, 3), self.precisionPolicy.output_dtype, init_val=0.0))
+
+    class PB(m.LBMPoroelasticity):
+        def __init__(self, **kw):
+            super().__init__(PE, PD, **kw)
+
+    kw = dict(lattice_elasticity=m.LatticeD2Q8(precision), lattice_darcy=m.LatticeD2Q9(darcy_precision or precision),
+              **{"lambda": lam}, mu=mu, omega=1.0 / (3 * K + 0.5), alpha=alpha, nx=n, ny=n, nz=0,
+              precision=precision, elasticity_MG_levels=levels, elasticity_steps=max_cycles,
+              coupling_method="centered", print_info_rate=0)
+    if darcy_precision:
+        kw["darcy_precision"] = darcy_precision
+    if coarsest_precision:
+        kw["coarsest_precision"] = coarsest_precision
+    if tol is not None:
+        kw["elasticity_tol"] = tol
+    return PB(**kw)
+
+
 def darcy_lognormal(m, n=1024, ell=16.0, sigma=1.0, seed=0, precision="f32/f32"):
     """Construct the workload's solver in namespace ``m``.  Returns
     ``(solver, k_field)``; the solver carries the per-cell omega field
