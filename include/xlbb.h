@@ -33,6 +33,7 @@ extern "C" {
 
 #define XLBB_F32 0
 #define XLBB_F64 1
+#define XLBB_F32_ACC64 2   /* FP32 storage, FP64 arithmetic (elasticity sweeps only) */
 
 typedef struct {
     int nx, ny;        /* logical grid size (cells)                        */
@@ -124,7 +125,7 @@ typedef struct {
 
 int xlbb_elast_sweep(int dtype, const XlbbGrid* g, const XlbbElastMaterial* mat,
                      const XlbbElastSweep* s, void* stream);
-int xlbb_elast_sweep_ctas(const XlbbGrid* g);
+int xlbb_elast_sweep_ctas(int dtype, const XlbbGrid* g);   /* CTAs of the next launch of this dtype */
 
 /*
  * One D2Q9 advection-diffusion-reaction BGK sweep (AdvectionDiffusionReactionBGK.step,
@@ -143,7 +144,7 @@ typedef struct {
 } XlbbDarcySweep;
 
 int xlbb_darcy_sweep(int dtype, const XlbbGrid* g, const XlbbDarcySweep* s, void* stream);
-int xlbb_darcy_sweep_ctas(const XlbbGrid* g);
+int xlbb_darcy_sweep_ctas(int dtype, const XlbbGrid* g);
 
 /*
  * Darcy sweep plus its FP64 convergence residual, allocating nothing.
@@ -210,6 +211,60 @@ int xlbb_prolong_add(int dtype_fine, int dtype_coarse, const XlbbGrid* fine, con
                      int x0, int x1bc, int y0, int y1bc, const void* f_coarse, void* f_fine, void* stream);
 /* dtype pairs (fine, coarse): (F32, F32), (F32, F64) -- an FP64 coarsest level
  * under FP32 levels -- and (F64, F64). */
+
+/*
+ * Batched elasticity multigrid (no counterpart in the reference, which runs
+ * one instance per solver object): many independent periodic D2Q8 instances
+ * of different sizes and Lame parameters advance in one launch per sweep.
+ * xlbb_batch_upload converts host instance records into the device
+ * descriptor array `dev` (xlbb_batch_desc_bytes(dtype) bytes each; the caller
+ * owns it).  A sweep runs every tile of `tiles_dev`: tile = (instance, x0,
+ * row range), CTAs of 128 owned columns looping over the list; the algebra is
+ * the one of xlbb_elast_sweep (out = a f + b STEP(f - resid)); tile_sumsq (one
+ * double per tile, or NULL) receives sum(out^2) / sum((out - f_in)^2), reduced
+ * per instance by xlbb_segment_sum over tile ranges begin[i]..begin[i+1].
+ */
+typedef struct {
+    const void* f_in;
+    void* f_out;
+    const void* force;       /* static force (2 planes) or NULL */
+    const void* resid;       /* residual (8 planes) or NULL */
+    int nx, ny, pitch;
+    long long plane;
+    double lam, mu;
+} XlbbBatchInstance;
+
+typedef struct {
+    int inst, x0, ys, ye;
+} XlbbBatchTile;
+
+typedef struct {
+    const void* fine;        /* fine residual (restrict) / fine populations (prolong) */
+    void* coarse;            /* coarse residual (restrict) / coarse correction (prolong) */
+    int nx_f, ny_f, pitch_f, pitch_c;
+    long long plane_f, plane_c;
+} XlbbBatchTransfer;
+
+int xlbb_batch_desc_bytes(int dtype);
+int xlbb_batch_upload(int dtype, const XlbbBatchInstance* host, int ninst, void* dev, void* stream);
+int xlbb_batched_elast_sweep(int dtype, const void* inst_dev, const XlbbBatchTile* tiles_dev, int ntiles,
+                             int ctas, double a, double b, int use_force, int has_resid, int sumsq_diff,
+                             double* tile_sumsq, void* stream);
+int xlbb_batched_restrict(int dtype_fine, int dtype_coarse, const XlbbBatchTransfer* tr_dev, int ninst,
+                          void* stream);
+int xlbb_batched_prolong_add(int dtype_fine, int dtype_coarse, const XlbbBatchTransfer* tr_dev, int ninst,
+                             void* stream);
+/*
+ * Prolongation plus the FP64 norms that track the smooth error: as
+ * xlbb_batched_prolong_add, and norms[2 i] = sum over instance i of the
+ * prolongated correction^2, norms[2 i + 1] = sum of the corrected fine
+ * populations^2 (deterministic).  parts: caller scratch of
+ * 2 * XLBB_PROLONG_BLOCKS * ninst doubles.
+ */
+#define XLBB_PROLONG_BLOCKS 32
+int xlbb_batched_prolong_add_norms(int dtype_fine, int dtype_coarse, const XlbbBatchTransfer* tr_dev, int ninst,
+                                   double* parts, double* norms, void* stream);
+int xlbb_segment_sum(const double* parts, const int* begin_dev, int nseg, double* out, void* stream);
 
 /* Deterministic FP64 sum of n partials (fixed order) into *out. */
 int xlbb_reduce_sum(const double* partials, int n, double* out, void* stream);

@@ -1,0 +1,103 @@
+"""Batched multigrid against independent single-instance solvers.
+
+Every instance of a heterogeneous batch (sizes, Lame parameters, forces) must
+follow the single-instance ``LBMElasticity`` V-cycle (which is itself checked
+against the oracle) after the same number of cycles, and its level-0 residual
+norm must match.
+"""
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+def _single(G, n, lam, mu, force, prec, levels, cycles, coarsest_precision=None, residual_precision=None):
+    class E(G.LBMElasticity):
+        def get_force(self):
+            return self.distributed_array_init((n, n, 2), self.precisionPolicy.compute_dtype, init_val=force)
+    s = E(lattice=G.LatticeD2Q8(prec), **{"lambda": float(lam)}, mu=float(mu), nx=n, ny=n, nz=0, precision=prec,
+          MG_levels=levels, coarsest_precision=coarsest_precision, residual_precision=residual_precision,
+          print_info_rate=0)
+    f = s.assign_fields_sharded()
+    norms = []
+    for t in range(cycles):
+        f, r = s.step(f, t)
+        norms.append(float(r))
+    return f.double().cpu().numpy(), norms
+
+
+@pytest.mark.parametrize("prec,tol", [("f64/f64", 1e-12), ("f32/f32", 1e-5)])
+def test_batched_vcycles_match_single_instances(prec, tol):
+    import xlb_biot_b200.api as G
+    from xlb_biot_b200.batched import BatchedElasticity
+    from xlb_biot_b200.workloads import batch_instances
+    sizes, lams, mus, forces = batch_instances(count=5, sizes=(32, 48, 64, 160), seed=3)
+    b = BatchedElasticity(sizes, lams, mus, forces, levels=3, precision=prec)
+    b.reset()
+    norms = []
+    for c in range(3):
+        b.vcycle()
+        norms.append(torch.sqrt(b.norm2).cpu().numpy().copy())
+    for i, (nx, ny) in enumerate(sizes):
+        f, ns = _single(G, nx, lams[i], mus[i], forces[i], prec, 3, 3)
+        got = b.populations(i).double().cpu().numpy()
+        assert np.abs(got - f).max() <= tol * np.abs(f).max(), i
+        for c in range(3):
+            assert abs(norms[c][i] - ns[c]) <= 10 * tol * ns[c], (i, c)
+
+
+def test_batched_solve_converges():
+    from xlb_biot_b200.batched import BatchedElasticity
+    from xlb_biot_b200.workloads import batch_instances
+    sizes, lams, mus, forces = batch_instances(count=8, sizes=(64, 96), seed=1)
+    b = BatchedElasticity(sizes, lams, mus, forces, levels=4, precision="f32/f32", coarsest_precision="f64")
+    cycles, rel = b.solve(tol=1e-4, max_cycles=80)
+    assert np.all(rel < 1e-4) and cycles < 80
+
+
+@pytest.mark.parametrize("prec,tol,rp", [("f64/f64", 1e-12, None), ("f32/f32", 1e-5, None), ("f32/f32", 1e-5, "f64")])
+def test_batched_per_instance_levels_fp64_coarsest(prec, tol, rp):
+    """Instances with different level counts (their coarsest levels at different
+    depths, each in FP64) against single-instance solvers with the same levels
+    (and, with rp="f64", FP64 arithmetic in both level-0 residual sweeps)."""
+    import xlb_biot_b200.api as G
+    from xlb_biot_b200.batched import BatchedElasticity, auto_levels
+    from xlb_biot_b200.workloads import batch_instances
+    sizes, lams, mus, forces = batch_instances(count=6, sizes=(24, 32, 48, 64), seed=5)
+    b = BatchedElasticity(sizes, lams, mus, forces, levels="auto", precision=prec, coarsest_precision="f64",
+                          residual_precision=rp)
+    assert b.instance_levels == [auto_levels(nx, ny) for nx, ny in sizes]
+    assert len(set(b.instance_levels)) > 1
+    b.reset()
+    norms = []
+    for c in range(3):
+        b.vcycle()
+        norms.append(torch.sqrt(b.norm2).cpu().numpy().copy())
+    for i, (nx, ny) in enumerate(sizes):
+        f, ns = _single(G, nx, lams[i], mus[i], forces[i], prec, b.instance_levels[i], 3, coarsest_precision="f64",
+                        residual_precision=rp)
+        got = b.populations(i).double().cpu().numpy()
+        assert np.abs(got - f).max() <= tol * np.abs(f).max(), i
+        for c in range(3):
+            assert abs(norms[c][i] - ns[c]) <= 10 * tol * ns[c], (i, c)
+
+
+def test_error_criterion_reaches_fp64_accuracy():
+    """FP32 batch with the FP64-arithmetic level-0 residual, stopped by the
+    estimated-error criterion at 1e-6: every instance's displacement is within
+    a few 1e-6 of an all-FP64 batch solved to 1e-11."""
+    from xlb_biot_b200.batched import BatchedElasticity
+    from xlb_biot_b200.workloads import batch_instances
+    sizes, lams, mus, forces = batch_instances(count=12, sizes=(32, 48, 64, 96), seed=2)
+    b = BatchedElasticity(sizes, lams, mus, forces, levels="auto", precision="f32/f32", coarsest_precision="f64",
+                          residual_precision="f64")
+    cycles, est = b.solve(tol=1e-6, max_cycles=200, criterion="error")
+    assert cycles < 200 and np.all(b.converged_at > 0)
+    b64 = BatchedElasticity(sizes, lams, mus, forces, levels="auto", precision="f64/f64")
+    c64, rel64 = b64.solve(tol=1e-11, max_cycles=400)
+    assert np.all(rel64 < 1e-11)
+    for i in range(len(sizes)):
+        u, u64 = b.displacement(i), b64.displacement(i)
+        err = float(torch.linalg.vector_norm(u - u64) / torch.linalg.vector_norm(u64))
+        assert err < 3e-6, (i, err)

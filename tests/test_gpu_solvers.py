@@ -79,3 +79,53 @@ def test_biot_mixed_precision(G):
         eo, do, to = oo[0], oo[1], oo[4]
     assert rel(og[0], oo[0]) < 1e-5          # elasticity populations (FP32)
     assert rel(og[5], oo[5]) < 1e-5          # pressure
+
+
+@pytest.mark.parametrize("prec,dprec,coarse", [("f64/f64", None, None), ("f32/f32", "f64/f64", "f64")])
+def test_biot_step_graph_matches_eager_steps(G, prec, dprec, coarse):
+    """The coupled step captured as one CUDA graph replays exactly the eager
+    step's kernels: all seven outputs bit-identical after several steps, and
+    ``run`` gives the same populations with and without the graph."""
+    from xlb_biot_b200.workloads import periodic_biot_1024
+    sim = periodic_biot_1024(G, n=64, levels=3, precision=prec, darcy_precision=dprec, coarsest_precision=coarse,
+                             max_cycles=2)
+    assert sim.graph_capturable()
+    graph = sim.capture_step(*sim.init_state())
+    graph.load(*sim.init_state())
+    e, d, t = sim.init_state()
+    for step in range(4):
+        eager = sim.step(e, d, t, step)
+        e, d, t = eager[0], eager[1], eager[4]
+        got = graph.replay()
+    for k, (a, b) in enumerate(zip(got, eager)):
+        assert torch.equal(a.double(), b.double()), k
+    sim.cudaGraph = False
+    fe, fd = sim.run(3)
+    sim.cudaGraph = True
+    ge, gd = sim.run(3)
+    assert torch.equal(fe, ge) and torch.equal(fd, gd)
+
+
+@pytest.mark.parametrize("kind", ["dirichlet", "neumann"])
+def test_fp64_arithmetic_residual_sweep_on_fp32_fields(G, kind):
+    """``residual_precision="f64"``: the level-0 residual sweep reads FP32
+    populations, collides, streams and applies the boundary rules in FP64 and
+    rounds only its result.  Near the fixed point (residual << populations) it
+    must equal the FP64 sweep of the same (upcast) populations to FP32 rounding
+    of the residual itself, which the FP32-arithmetic sweep cannot."""
+    kw = dict(**{"lambda": LAM}, mu=MU, nx=34, ny=34, nz=0, MG_levels=2,
+              MG_BCs={"top": True, "bottom": True, "left": True, "right": True})
+    s64 = make_walled_elasticity(G, kind)(lattice=G.LatticeD2Q8("f64/f64"), precision="f64/f64", **kw)
+    s32 = make_walled_elasticity(G, kind)(lattice=G.LatticeD2Q8("f32/f32"), precision="f32/f32",
+                                          residual_precision="f64", **kw)
+    f, _, _ = s64.solve(tol=1e-9, max_sweeps=300)
+    f32 = s32._f(f.float())
+    ref = s64._sweep(s64._f(f32.double()), 0, 1.0, -1.0).double().cpu().numpy()
+    acc = s32._sweep(f32, 0, 1.0, -1.0, acc64=True).double().cpu().numpy()
+    low = s32._sweep(f32, 0, 1.0, -1.0).double().cpu().numpy()
+    scale = np.abs(ref).max()
+    assert scale > 0
+    e_acc = np.abs(acc - ref).max() / scale
+    e_low = np.abs(low - ref).max() / scale
+    assert e_acc < 1e-5, e_acc
+    assert e_low > 100 * e_acc, (e_low, e_acc)     # the test can tell the two apart

@@ -37,7 +37,7 @@ def test_noalloc_matches_regular_entry_point_twice():
     L = solver._layout
     grid = L.grid()
     stream = _lib.stream_ptr()
-    n = lib.xlbb_darcy_sweep_ctas(grid)
+    n = lib.xlbb_darcy_sweep_ctas(_lib.XLBB_F64, grid)
     assert 0 < n <= 16384
     partials = torch.empty(n, dtype=torch.float64, device="cuda")
     f = solver.assign_fields_sharded()

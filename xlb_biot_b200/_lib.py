@@ -11,7 +11,8 @@ import torch
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libxlbb.so")
 
-XLBB_F32, XLBB_F64 = 0, 1
+XLBB_F32, XLBB_F64, XLBB_F32_ACC64 = 0, 1, 2
+XLBB_PROLONG_BLOCKS = 32
 ERRORS = {-1: "XLBB_EBADARG", -2: "XLBB_ELAUNCH", -3: "XLBB_ETIMEOUT", -4: "XLBB_ENONFINITE",
           -5: "XLBB_EUNSUPPORTED"}
 
@@ -55,15 +56,27 @@ class DarcySweep(ctypes.Structure):
                 ("pc", Rules), ("ps", Rules), ("sumsq", ctypes.c_void_p)]
 
 
+class BatchInstance(ctypes.Structure):
+    _fields_ = [("f_in", ctypes.c_void_p), ("f_out", ctypes.c_void_p), ("force", ctypes.c_void_p),
+                ("resid", ctypes.c_void_p), ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("pitch", ctypes.c_int),
+                ("plane", ctypes.c_longlong), ("lam", ctypes.c_double), ("mu", ctypes.c_double)]
+
+
+class BatchTransfer(ctypes.Structure):
+    _fields_ = [("fine", ctypes.c_void_p), ("coarse", ctypes.c_void_p), ("nx_f", ctypes.c_int),
+                ("ny_f", ctypes.c_int), ("pitch_f", ctypes.c_int), ("pitch_c", ctypes.c_int),
+                ("plane_f", ctypes.c_longlong), ("plane_c", ctypes.c_longlong)]
+
+
 P = ctypes.c_void_p
 I = ctypes.c_int
 D = ctypes.c_double
 PG = ctypes.POINTER(Grid)
 SIGNATURES = {
     "xlbb_elast_sweep": (I, [I, PG, ctypes.POINTER(ElastMaterial), ctypes.POINTER(ElastSweep), P]),
-    "xlbb_elast_sweep_ctas": (I, [PG]),
+    "xlbb_elast_sweep_ctas": (I, [I, PG]),
     "xlbb_darcy_sweep": (I, [I, PG, ctypes.POINTER(DarcySweep), P]),
-    "xlbb_darcy_sweep_ctas": (I, [PG]),
+    "xlbb_darcy_sweep_ctas": (I, [I, PG]),
     "xlbb_darcy_sweep_residual_noalloc": (I, [I, PG, ctypes.POINTER(DarcySweep), P, P]),
     "xlbb_darcy_gradient": (I, [I, PG, P, D, ctypes.POINTER(Rules), P, P, P]),
     "xlbb_elast_moments": (I, [I, PG, ctypes.POINTER(ElastMaterial), P, P, P, P, P, P, D, P]),
@@ -78,6 +91,13 @@ SIGNATURES = {
     "xlbb_sweep_set_config": (I, [I, ctypes.POINTER(SweepConfig)]),
     "xlbb_sweep_get_config": (I, [I, ctypes.POINTER(SweepConfig)]),
     "xlbb_device_status": (I, [ctypes.POINTER(ctypes.c_int), I]),
+    "xlbb_batch_desc_bytes": (I, [I]),
+    "xlbb_batch_upload": (I, [I, ctypes.POINTER(BatchInstance), I, P, P]),
+    "xlbb_batched_elast_sweep": (I, [I, P, P, I, I, D, D, I, I, I, P, P]),
+    "xlbb_batched_restrict": (I, [I, I, P, I, P]),
+    "xlbb_batched_prolong_add": (I, [I, I, P, I, P]),
+    "xlbb_batched_prolong_add_norms": (I, [I, I, P, I, P, P, P]),
+    "xlbb_segment_sum": (I, [P, P, I, P, P]),
     "xlbb_last_error": (ctypes.c_char_p, []),
     "xlbb_version": (I, []),
 }

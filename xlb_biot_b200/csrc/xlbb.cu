@@ -8,6 +8,7 @@
 #include <mutex>
 #include <string>
 #include <type_traits>
+#include <vector>
 
 #include "xlbb.h"
 #include "xlbb_common.cuh"
@@ -81,11 +82,13 @@ static bool cfg_ok(const XlbbSweepConfig& c) {
 // D2Q8 elasticity (src/elasticity.py:805-848 transfer matrices, :959-1000
 // collision, :1002-1058 moments).
 // ---------------------------------------------------------------------------
-template <typename T>
+// T: arithmetic type; S: storage type of the fields (S = float with T = double
+// is FP32 storage with FP64 arithmetic).
+template <typename T, typename S = T>
 struct ElastMat {
     T cs, cd, h, n;   // uniform relaxation rates and m_to_f coefficients
-    const T* lam_f;   // optional per-cell Lame fields
-    const T* mu_f;
+    const S* lam_f;   // optional per-cell Lame fields
+    const S* mu_f;
 };
 
 template <typename T>
@@ -125,30 +128,35 @@ __device__ __forceinline__ void elast_collide(const T (&f)[8], bool hasF, T F0, 
     o[7] = n * M2 - T(0.25) * M4 + T(0.25) * M5 - T(0.25) * M6;
 }
 
-template <typename T_, bool RESID>
+// T_: arithmetic type (registers, the post-collision ring, boundary-rule
+// constants); S_: storage type of the fields in HBM.  S_ = float with
+// T_ = double is the FP32-storage / FP64-arithmetic sweep (register-prefetch
+// pipeline only).
+template <typename T_, bool RESID, typename S_ = T_>
 struct ElastPhys {
     using T = T_;
+    using Storage = S_;
     static constexpr int Q = 8;
     __host__ __device__ static constexpr int cx(int i) { return cx8(i); }
     __host__ __device__ static constexpr int cy(int i) { return cy8(i); }
     struct Args {
         SweepGeom geom;
-        const T* f_in;
-        T* f_out;
-        const T* force;
-        const T* fext;
-        const T* resid;
+        const S_* f_in;
+        S_* f_out;
+        const S_* force;
+        const S_* fext;
+        const S_* resid;
         T a, b;
-        ElastMat<T> mat;
+        ElastMat<T, S_> mat;
         RulesView<T, 8> pc, ps;
         double* sumsq;
         int bx0, bx1, by0, by1;
-        T* div_out;
+        S_* div_out;
         T div_scale;
         int mix;   // 0: out = S; 1: out = a f + b S
         int sumsq_diff;   // sumsq of (out - f_in) instead of out
         static constexpr int PMAX = 20;
-        const T* planes[PMAX];   // input planes in from_smem order (bulk-copy kernel)
+        const S_* planes[PMAX];   // input planes in from_smem order (bulk-copy kernel)
         int np;
     };
     struct In {
@@ -188,15 +196,15 @@ struct ElastPhys {
         const size_t o = (size_t)y * p.geom.pitch + x;
         const long long P = p.geom.plane;
 #pragma unroll
-        for (int i = 0; i < 8; ++i) in.f[i] = __ldg(p.f_in + o + i * P);
+        for (int i = 0; i < 8; ++i) in.f[i] = T(__ldg(p.f_in + o + i * P));
         if (RESID) {
 #pragma unroll
-            for (int i = 0; i < 8; ++i) in.r[i] = __ldg(p.resid + o + i * P);
+            for (int i = 0; i < 8; ++i) in.r[i] = T(__ldg(p.resid + o + i * P));
         }
         T F0 = T(0), F1 = T(0);
-        if (p.force) { F0 = __ldg(p.force + o); F1 = __ldg(p.force + o + P); }
+        if (p.force) { F0 = T(__ldg(p.force + o)); F1 = T(__ldg(p.force + o + P)); }
         if (p.fext) {
-            const T e0 = __ldg(p.fext + o), e1 = __ldg(p.fext + o + P);
+            const T e0 = T(__ldg(p.fext + o)), e1 = T(__ldg(p.fext + o + P));
             if (p.force) { F0 = F0 + e0; F1 = F1 + e1; } else { F0 = e0; F1 = e1; }
         }
         in.F0 = F0;
@@ -213,7 +221,7 @@ struct ElastPhys {
         T cs = p.mat.cs, cd = p.mat.cd, h = p.mat.h, n = p.mat.n;
         if (p.mat.mu_f) {
             const size_t c = (size_t)y * p.geom.pitch + x;
-            elast_rates<T>(__ldg(p.mat.lam_f + c), __ldg(p.mat.mu_f + c), cs, cd, h, n);
+            elast_rates<T>(T(__ldg(p.mat.lam_f + c)), T(__ldg(p.mat.mu_f + c)), cs, cd, h, n);
         }
         elast_collide<T>(g, p.force != nullptr || p.fext != nullptr, in.F0, in.F1, cs, cd, h, n, o);
     }
@@ -229,15 +237,16 @@ struct ElastPhys {
             if constexpr (PREV) {
                 if (p.mix) v = p.a * fprev[i] + p.b * S[i];
             }
-            p.f_out[o + i * P] = v;
-            double d = (double)v;
+            const S_ sv = S_(v);
+            p.f_out[o + i * P] = sv;
+            double d = (double)sv;
             if constexpr (PREV) {
-                if (p.sumsq_diff) d -= (double)fprev[i];
+                if (p.sumsq_diff) d -= (double)S_(fprev[i]);
             }
             acc += d * d;
             m2 += (i < 4 ? T(1) : T(2)) * v;
         }
-        if (p.div_out) p.div_out[o] = p.div_scale * m2;
+        if (p.div_out) p.div_out[o] = S_(p.div_scale * m2);
         const bool in_box = x >= p.bx0 && x < p.bx1 && y >= p.by0 && y < p.by1;
         return in_box ? acc : 0.0;
     }
@@ -438,10 +447,25 @@ static void launch_sweep(XlbbSweepConfig c, const XlbbGrid* g, cudaStream_t st, 
     sweep_kernel<Ph, 128, 1, PREV><<<grid, 128 + 32, 0, st>>>(a);
 }
 
-// The configuration a launch actually uses (FP64 caps tx at 128).
+// FP32 storage / FP64 arithmetic: the register-prefetch kernel at tx = 128.
+template <class Ph, bool PREV>
+static void launch_sweep_regs(const XlbbSweepConfig& c, const XlbbGrid* g, cudaStream_t st,
+                              const typename Ph::Args& a) {
+    const dim3 grid = sweep_grid(g, c);
+    if (c.depth == 2) sweep_kernel<Ph, 128, 2, PREV><<<grid, 128 + 32, 0, st>>>(a);
+    else sweep_kernel<Ph, 128, 1, PREV><<<grid, 128 + 32, 0, st>>>(a);
+}
+
+// The configuration a launch actually uses (FP64 arithmetic caps tx at 128;
+// the FP32-storage / FP64-arithmetic sweep has only the register-prefetch
+// pipeline, depth <= 2).
 static XlbbSweepConfig effective_cfg(int kernel, int dtype) {
     XlbbSweepConfig c = g_cfg[kernel];
-    if (dtype == XLBB_F64 && c.tx > 128) c.tx = 128;
+    if ((dtype == XLBB_F64 || dtype == XLBB_F32_ACC64) && c.tx > 128) c.tx = 128;
+    if (dtype == XLBB_F32_ACC64 && c.pipeline != 0) {
+        c.pipeline = 0;
+        if (c.depth > 2) c.depth = 2;
+    }
     return c;
 }
 
@@ -657,47 +681,52 @@ __global__ void axpby_kernel(long long n, T a, const T* x, T b, const T* y, T* o
 
 static SweepGeom geom(const XlbbGrid* g) { return SweepGeom{g->nx, g->ny, g->pitch, g->plane}; }
 
-template <typename T>
-static ElastMat<T> make_mat(const XlbbElastMaterial* m) {
-    ElastMat<T> e;
+template <typename T, typename S = T>
+static ElastMat<T, S> make_mat(const XlbbElastMaterial* m) {
+    ElastMat<T, S> e;
     elast_rates<T>(T(m->lam), T(m->mu), e.cs, e.cd, e.h, e.n);
-    e.lam_f = static_cast<const T*>(m->lam_field);
-    e.mu_f = static_cast<const T*>(m->mu_field);
+    e.lam_f = static_cast<const S*>(m->lam_field);
+    e.mu_f = static_cast<const S*>(m->mu_field);
     return e;
 }
 
-template <typename T, bool RESID, bool PREV>
+template <typename T, bool RESID, bool PREV, typename S = T>
 static int launch_elast(const XlbbGrid* g, const XlbbElastMaterial* mat, const XlbbElastSweep* s, cudaStream_t st) {
-    using Ph = ElastPhys<T, RESID>;
+    using Ph = ElastPhys<T, RESID, S>;
     typename Ph::Args a;
     a.geom = geom(g);
-    a.f_in = static_cast<const T*>(s->f_in);
-    a.f_out = static_cast<T*>(s->f_out);
-    a.force = s->use_force ? static_cast<const T*>(s->force) : nullptr;
-    a.fext = static_cast<const T*>(s->fext);
-    a.resid = static_cast<const T*>(s->resid);
+    a.f_in = static_cast<const S*>(s->f_in);
+    a.f_out = static_cast<S*>(s->f_out);
+    a.force = s->use_force ? static_cast<const S*>(s->force) : nullptr;
+    a.fext = static_cast<const S*>(s->fext);
+    a.resid = static_cast<const S*>(s->resid);
     a.a = T(s->a);
     a.b = T(s->b);
     a.mix = (s->a == 0.0 && s->b == 1.0) ? 0 : 1;
     a.sumsq_diff = (s->sumsq != nullptr && s->sumsq_diff) ? 1 : 0;
-    a.mat = make_mat<T>(mat);
+    a.mat = make_mat<T, S>(mat);
     a.pc = rules_view<T, 8>(s->pc);
     a.ps = rules_view<T, 8>(s->ps);
     a.sumsq = s->sumsq;
     a.bx0 = s->bx0; a.bx1 = s->bx1; a.by0 = s->by0; a.by1 = s->by1;
-    a.div_out = static_cast<T*>(s->div_out);
+    a.div_out = static_cast<S*>(s->div_out);
     a.div_scale = T(-1.5 / (3.0 * (mat->lam + mat->mu) + 1.0));
-    const XlbbSweepConfig c = effective_cfg(0, sizeof(T) == 4 ? XLBB_F32 : XLBB_F64);
-    launch_sweep<Ph, PREV>(c, g, st, a);
+    if constexpr (sizeof(T) != sizeof(S)) {
+        launch_sweep_regs<Ph, PREV>(effective_cfg(0, XLBB_F32_ACC64), g, st, a);
+    } else {
+        const XlbbSweepConfig c = effective_cfg(0, sizeof(T) == 4 ? XLBB_F32 : XLBB_F64);
+        launch_sweep<Ph, PREV>(c, g, st, a);
+    }
     return check_launch("xlbb_elast_sweep");
 }
 
-template <typename T>
+template <typename T, typename S = T>
 static int elast_sweep_t(const XlbbGrid* g, const XlbbElastMaterial* mat, const XlbbElastSweep* s, cudaStream_t st) {
     // the previous populations are kept when mixed or differenced
     const bool mix = !(s->a == 0.0 && s->b == 1.0) || (s->sumsq != nullptr && s->sumsq_diff);
-    if (s->resid) return mix ? launch_elast<T, true, true>(g, mat, s, st) : launch_elast<T, true, false>(g, mat, s, st);
-    return mix ? launch_elast<T, false, true>(g, mat, s, st) : launch_elast<T, false, false>(g, mat, s, st);
+    if (s->resid)
+        return mix ? launch_elast<T, true, true, S>(g, mat, s, st) : launch_elast<T, true, false, S>(g, mat, s, st);
+    return mix ? launch_elast<T, false, true, S>(g, mat, s, st) : launch_elast<T, false, false, S>(g, mat, s, st);
 }
 
 template <typename T>
@@ -722,6 +751,155 @@ static int darcy_sweep_t(const XlbbGrid* g, const XlbbDarcySweep* s, cudaStream_
 
 static inline dim3 row_grid(int nx, int ny, int bs) { return dim3((nx + bs - 1) / bs, ny); }
 
+// ---------------------------------------------------------------------------
+// Batched elasticity multigrid: many independent periodic instances of
+// different sizes and materials in one launch per sweep.  CTAs loop over a
+// work list of tiles (instance, owned columns, strip of rows); every tile is a
+// sweep_strip of that instance's grid.
+// ---------------------------------------------------------------------------
+template <typename T, typename S = T>
+struct BatchInst {
+    const S* f_in;
+    S* f_out;
+    const S* force;
+    const S* resid;
+    SweepGeom geom;
+    T cs, cd, h, n;
+};
+
+template <typename T, typename S = T>
+static BatchInst<T, S> to_batch_inst(const XlbbBatchInstance& s) {
+    BatchInst<T, S> b;
+    b.f_in = static_cast<const S*>(s.f_in);
+    b.f_out = static_cast<S*>(s.f_out);
+    b.force = static_cast<const S*>(s.force);
+    b.resid = static_cast<const S*>(s.resid);
+    b.geom = SweepGeom{s.nx, s.ny, s.pitch, s.plane};
+    elast_rates<T>(T(s.lam), T(s.mu), b.cs, b.cd, b.h, b.n);
+    return b;
+}
+
+template <typename T, int TX, bool RESID, bool PREV, typename S = T>
+__global__ void __launch_bounds__(TX + 32)
+batched_elast_kernel(const BatchInst<T, S>* __restrict__ inst, const XlbbBatchTile* __restrict__ tiles, int ntiles,
+                     T a, T b, int mix, int use_force, int sumsq_diff, double* tile_sumsq) {
+    using Ph = ElastPhys<T, RESID, S>;
+    __shared__ T post[4][8][TX + 2];
+    __shared__ double red[(TX + 32) / 32];
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        __syncthreads();   // the ring of the previous tile is no longer read
+        const XlbbBatchTile tl = tiles[t];
+        const BatchInst<T, S> I = inst[tl.inst];
+        typename Ph::Args p;
+        p.geom = I.geom;
+        p.f_in = I.f_in;
+        p.f_out = I.f_out;
+        p.force = use_force ? I.force : nullptr;
+        p.fext = nullptr;
+        p.resid = I.resid;
+        p.a = a;
+        p.b = b;
+        p.mat = ElastMat<T, S>{I.cs, I.cd, I.h, I.n, nullptr, nullptr};
+        p.pc = RulesView<T, 8>{0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0};
+        p.ps = p.pc;
+        p.sumsq = tile_sumsq;
+        p.bx0 = 0; p.bx1 = I.geom.nx; p.by0 = 0; p.by1 = I.geom.ny;
+        p.div_out = nullptr;
+        p.div_scale = T(0);
+        p.mix = mix;
+        p.sumsq_diff = sumsq_diff;
+        p.np = 0;
+        const double acc = sweep_strip<Ph, TX, 1, PREV>(p, tl.x0, tl.ys, tl.ye, post);
+        if (tile_sumsq != nullptr) {
+            const double s = block_sum(acc, red);
+            if (threadIdx.x == 0) tile_sumsq[t] = s;
+        }
+    }
+}
+
+// Restriction (2x2 block sums) and prolongation (injection, added) of every
+// instance of a periodic batch; blockIdx.y = instance.
+template <typename Tf, typename Tc>
+__global__ void batched_restrict_kernel(const XlbbBatchTransfer* __restrict__ tr) {
+    const XlbbBatchTransfer T_ = tr[blockIdx.y];
+    const Tf* res = static_cast<const Tf*>(T_.fine);
+    Tc* rc = static_cast<Tc*>(T_.coarse);
+    using Ts = typename std::conditional<(sizeof(Tf) > sizeof(Tc)), Tf, Tc>::type;
+    const int ncx = T_.nx_f / 2, ncy = T_.ny_f / 2;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < ncx * ncy; e += gridDim.x * blockDim.x) {
+        const int X = e % ncx, Y = e / ncx;
+        const size_t of = (size_t)(2 * Y) * T_.pitch_f + 2 * X, oc = (size_t)Y * T_.pitch_c + X;
+        for (int i = 0; i < 8; ++i) {
+            const Tf* s = res + of + (size_t)i * T_.plane_f;
+            const Ts v = Ts(s[0]) + Ts(s[T_.pitch_f]) + Ts(s[1]) + Ts(s[T_.pitch_f + 1]);
+            rc[oc + (size_t)i * T_.plane_c] = Tc(v);
+        }
+    }
+}
+
+// With ``parts`` != NULL every block also writes its FP64 sums of the
+// correction^2 and of the corrected populations^2 to parts[2 * block + {0, 1}]
+// (block = blockIdx.y * gridDim.x + blockIdx.x).
+template <typename Tf, typename Tc>
+__global__ void batched_prolong_add_kernel(const XlbbBatchTransfer* __restrict__ tr, double* parts) {
+    __shared__ double red[8];
+    const XlbbBatchTransfer T_ = tr[blockIdx.y];
+    Tf* ff = static_cast<Tf*>(const_cast<void*>(T_.fine));
+    const Tc* fc = static_cast<const Tc*>(T_.coarse);
+    double cc = 0.0, nn = 0.0;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < T_.nx_f * T_.ny_f; e += gridDim.x * blockDim.x) {
+        const int x = e % T_.nx_f, y = e / T_.nx_f;
+        const size_t of = (size_t)y * T_.pitch_f + x, oc = (size_t)(y / 2) * T_.pitch_c + x / 2;
+        for (int i = 0; i < 8; ++i) {
+            const Tc c = fc[oc + (size_t)i * T_.plane_c];
+            const Tf v = Tf(ff[of + (size_t)i * T_.plane_f] + c);
+            ff[of + (size_t)i * T_.plane_f] = v;
+            cc += (double)c * (double)c;
+            nn += (double)v * (double)v;
+        }
+    }
+    if (parts != nullptr) {
+        const double a = block_sum(cc, red);
+        const double b = block_sum(nn, red);
+        if (threadIdx.x == 0) {
+            const size_t blk = (size_t)blockIdx.y * gridDim.x + blockIdx.x;
+            parts[2 * blk] = a;
+            parts[2 * blk + 1] = b;
+        }
+    }
+}
+
+// norms[2 i + k] = sum over the XLBB_PROLONG_BLOCKS blocks of instance i of
+// parts[2 block + k]; one warp per instance, fixed order.
+__global__ void prolong_norms_kernel(const double* parts, int ninst, double* norms) {
+    const int i = blockIdx.x;
+    if (i >= ninst) return;
+    static_assert(XLBB_PROLONG_BLOCKS == 32, "one lane per block");
+    const size_t base = (size_t)i * XLBB_PROLONG_BLOCKS + threadIdx.x;
+    double a = parts[2 * base], b = parts[2 * base + 1];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, o);
+        b += __shfl_xor_sync(0xffffffffu, b, o);
+    }
+    if (threadIdx.x == 0) {
+        norms[2 * i] = a;
+        norms[2 * i + 1] = b;
+    }
+}
+
+// Per-instance FP64 sums of tile partials (tiles of one instance are contiguous).
+__global__ void segment_sum_kernel(const double* parts, const int* begin, int ninst, double* out) {
+    __shared__ double red[8];
+    const int i = blockIdx.x;
+    if (i >= ninst) return;
+    double acc = 0.0;
+    for (int t = begin[i] + threadIdx.x; t < begin[i + 1]; t += blockDim.x) acc += parts[t];
+    const double s = block_sum(acc, red);
+    if (threadIdx.x == 0) out[i] = s;
+}
+
+
 }  // namespace xlbb
 
 using namespace xlbb;
@@ -734,16 +912,20 @@ int xlbb_version(void) { return 100; }
 
 const char* xlbb_last_error(void) { return g_last_error.c_str(); }
 
-int xlbb_elast_sweep_ctas(const XlbbGrid* g) {
-    if (!grid_ok(g)) return fail(XLBB_EBADARG, "xlbb_elast_sweep_ctas: bad grid");
-    const dim3 a = sweep_grid(g, effective_cfg(0, XLBB_F32)), b = sweep_grid(g, effective_cfg(0, XLBB_F64));
-    return (int)max(a.x * a.y, b.x * b.y);
+// Exactly the CTAs (= FP64 partials) of the next sweep launch of this dtype:
+// the reductions read exactly that many partials.
+int xlbb_elast_sweep_ctas(int dtype, const XlbbGrid* g) {
+    if (!grid_ok(g) || (dtype != XLBB_F32 && dtype != XLBB_F64 && dtype != XLBB_F32_ACC64))
+        return fail(XLBB_EBADARG, "xlbb_elast_sweep_ctas: bad argument");
+    const dim3 a = sweep_grid(g, effective_cfg(0, dtype));
+    return (int)(a.x * a.y);
 }
 
-int xlbb_darcy_sweep_ctas(const XlbbGrid* g) {
-    if (!grid_ok(g)) return fail(XLBB_EBADARG, "xlbb_darcy_sweep_ctas: bad grid");
-    const dim3 a = sweep_grid(g, effective_cfg(1, XLBB_F32)), b = sweep_grid(g, effective_cfg(1, XLBB_F64));
-    return (int)max(a.x * a.y, b.x * b.y);
+int xlbb_darcy_sweep_ctas(int dtype, const XlbbGrid* g) {
+    if (!grid_ok(g) || (dtype != XLBB_F32 && dtype != XLBB_F64))
+        return fail(XLBB_EBADARG, "xlbb_darcy_sweep_ctas: bad argument");
+    const dim3 a = sweep_grid(g, effective_cfg(1, dtype));
+    return (int)(a.x * a.y);
 }
 
 int xlbb_sweep_set_config(int kernel, const XlbbSweepConfig* cfg) {
@@ -779,6 +961,7 @@ int xlbb_elast_sweep(int dtype, const XlbbGrid* g, const XlbbElastMaterial* mat,
         return fail(XLBB_EBADARG, "xlbb_elast_sweep: lam_field and mu_field go together");
     if (dtype == XLBB_F32) return elast_sweep_t<float>(g, mat, s, XLBB_STREAM(stream));
     if (dtype == XLBB_F64) return elast_sweep_t<double>(g, mat, s, XLBB_STREAM(stream));
+    if (dtype == XLBB_F32_ACC64) return elast_sweep_t<double, float>(g, mat, s, XLBB_STREAM(stream));
     return fail(XLBB_EUNSUPPORTED, "xlbb_elast_sweep: dtype");
 }
 
@@ -962,7 +1145,7 @@ extern "C" {
 int xlbb_darcy_sweep_residual_noalloc(int dtype, const XlbbGrid* g, const XlbbDarcySweep* s, double* sumsq_out,
                                       void* stream) {
     if (!grid_ok(g) || !s || !sumsq_out) return fail(XLBB_EBADARG, "xlbb_darcy_sweep_residual_noalloc: bad argument");
-    const int n = xlbb_darcy_sweep_ctas(g);
+    const int n = xlbb_darcy_sweep_ctas(dtype, g);
     if (n < 0) return n;
     if (n > XLBB_NOALLOC_MAX_PARTIALS)
         return fail(XLBB_EBADARG, "xlbb_darcy_sweep_residual_noalloc: the launch shape needs more CTA partials than "
@@ -996,6 +1179,117 @@ int xlbb_axpby(int dtype, long long n, double a, const void* x, double b, const 
                                                                        (double*)out);
     else return fail(XLBB_EUNSUPPORTED, "xlbb_axpby: dtype");
     return check_launch("xlbb_axpby");
+}
+
+
+// ---------------------------------------------------------------------------
+// Batched multigrid entry points.
+// ---------------------------------------------------------------------------
+int xlbb_batch_upload(int dtype, const XlbbBatchInstance* host, int ninst, void* dev, void* stream) {
+    if (!host || !dev || ninst <= 0) return fail(XLBB_EBADARG, "xlbb_batch_upload: bad argument");
+    if (dtype == XLBB_F32) {
+        std::vector<BatchInst<float>> v(ninst);
+        for (int i = 0; i < ninst; ++i) v[i] = to_batch_inst<float>(host[i]);
+        cudaMemcpyAsync(dev, v.data(), sizeof(BatchInst<float>) * ninst, cudaMemcpyHostToDevice, XLBB_STREAM(stream));
+        return cudaStreamSynchronize(XLBB_STREAM(stream)) == cudaSuccess ? XLBB_OK : fail(XLBB_ELAUNCH, "xlbb_batch_upload");
+    }
+    if (dtype == XLBB_F64) {
+        std::vector<BatchInst<double>> v(ninst);
+        for (int i = 0; i < ninst; ++i) v[i] = to_batch_inst<double>(host[i]);
+        cudaMemcpyAsync(dev, v.data(), sizeof(BatchInst<double>) * ninst, cudaMemcpyHostToDevice, XLBB_STREAM(stream));
+        return cudaStreamSynchronize(XLBB_STREAM(stream)) == cudaSuccess ? XLBB_OK : fail(XLBB_ELAUNCH, "xlbb_batch_upload");
+    }
+    if (dtype == XLBB_F32_ACC64) {
+        std::vector<BatchInst<double, float>> v(ninst);
+        for (int i = 0; i < ninst; ++i) v[i] = to_batch_inst<double, float>(host[i]);
+        cudaMemcpyAsync(dev, v.data(), sizeof(BatchInst<double, float>) * ninst, cudaMemcpyHostToDevice,
+                        XLBB_STREAM(stream));
+        return cudaStreamSynchronize(XLBB_STREAM(stream)) == cudaSuccess ? XLBB_OK : fail(XLBB_ELAUNCH, "xlbb_batch_upload");
+    }
+    return fail(XLBB_EUNSUPPORTED, "xlbb_batch_upload: dtype");
+}
+
+int xlbb_batch_desc_bytes(int dtype) {
+    if (dtype == XLBB_F64) return (int)sizeof(BatchInst<double>);
+    if (dtype == XLBB_F32_ACC64) return (int)sizeof(BatchInst<double, float>);
+    return (int)sizeof(BatchInst<float>);
+}
+
+}  // extern "C"
+
+template <typename T, typename S = T>
+static int batched_sweep_t(const void* inst, const XlbbBatchTile* tiles, int ntiles, int ctas, double a, double b,
+                           int use_force, int has_resid, int sumsq_diff, double* tile_sumsq, cudaStream_t st) {
+    const int mix = (a == 0.0 && b == 1.0) ? 0 : 1;
+    const bool prev = mix || (tile_sumsq && sumsq_diff);
+    const BatchInst<T, S>* I = static_cast<const BatchInst<T, S>*>(inst);
+#define XLBB_B(R, P) \
+    batched_elast_kernel<T, 128, R, P, S><<<ctas, 160, 0, st>>>(I, tiles, ntiles, T(a), T(b), mix, use_force, \
+                                                                 sumsq_diff, tile_sumsq)
+    if (has_resid) { if (prev) XLBB_B(true, true); else XLBB_B(true, false); }
+    else { if (prev) XLBB_B(false, true); else XLBB_B(false, false); }
+#undef XLBB_B
+    return check_launch("xlbb_batched_elast_sweep");
+}
+
+extern "C" {
+
+int xlbb_batched_elast_sweep(int dtype, const void* inst_dev, const XlbbBatchTile* tiles_dev, int ntiles, int ctas,
+                             double a, double b, int use_force, int has_resid, int sumsq_diff, double* tile_sumsq,
+                             void* stream) {
+    if (!inst_dev || !tiles_dev || ntiles <= 0 || ctas <= 0) return fail(XLBB_EBADARG, "xlbb_batched_elast_sweep: bad argument");
+    if (dtype == XLBB_F32)
+        return batched_sweep_t<float>(inst_dev, tiles_dev, ntiles, ctas, a, b, use_force, has_resid, sumsq_diff,
+                                      tile_sumsq, XLBB_STREAM(stream));
+    if (dtype == XLBB_F64)
+        return batched_sweep_t<double>(inst_dev, tiles_dev, ntiles, ctas, a, b, use_force, has_resid, sumsq_diff,
+                                       tile_sumsq, XLBB_STREAM(stream));
+    if (dtype == XLBB_F32_ACC64)
+        return batched_sweep_t<double, float>(inst_dev, tiles_dev, ntiles, ctas, a, b, use_force, has_resid,
+                                              sumsq_diff, tile_sumsq, XLBB_STREAM(stream));
+    return fail(XLBB_EUNSUPPORTED, "xlbb_batched_elast_sweep: dtype");
+}
+
+int xlbb_batched_restrict(int dtype_fine, int dtype_coarse, const XlbbBatchTransfer* tr_dev, int ninst, void* stream) {
+    if (!tr_dev || ninst <= 0) return fail(XLBB_EBADARG, "xlbb_batched_restrict: bad argument");
+    const dim3 grid(16, ninst);
+    cudaStream_t st = XLBB_STREAM(stream);
+    if (dtype_fine == XLBB_F32 && dtype_coarse == XLBB_F32) batched_restrict_kernel<float, float><<<grid, 256, 0, st>>>(tr_dev);
+    else if (dtype_fine == XLBB_F32 && dtype_coarse == XLBB_F64) batched_restrict_kernel<float, double><<<grid, 256, 0, st>>>(tr_dev);
+    else if (dtype_fine == XLBB_F64 && dtype_coarse == XLBB_F64) batched_restrict_kernel<double, double><<<grid, 256, 0, st>>>(tr_dev);
+    else return fail(XLBB_EUNSUPPORTED, "xlbb_batched_restrict: dtype pair");
+    return check_launch("xlbb_batched_restrict");
+}
+
+static int prolong_t(int dtype_fine, int dtype_coarse, const XlbbBatchTransfer* tr_dev, int ninst, double* parts,
+                     cudaStream_t st) {
+    const dim3 grid(XLBB_PROLONG_BLOCKS, ninst);
+    if (dtype_fine == XLBB_F32 && dtype_coarse == XLBB_F32) batched_prolong_add_kernel<float, float><<<grid, 256, 0, st>>>(tr_dev, parts);
+    else if (dtype_fine == XLBB_F32 && dtype_coarse == XLBB_F64) batched_prolong_add_kernel<float, double><<<grid, 256, 0, st>>>(tr_dev, parts);
+    else if (dtype_fine == XLBB_F64 && dtype_coarse == XLBB_F64) batched_prolong_add_kernel<double, double><<<grid, 256, 0, st>>>(tr_dev, parts);
+    else return fail(XLBB_EUNSUPPORTED, "xlbb_batched_prolong_add: dtype pair");
+    return check_launch("xlbb_batched_prolong_add");
+}
+
+int xlbb_batched_prolong_add(int dtype_fine, int dtype_coarse, const XlbbBatchTransfer* tr_dev, int ninst, void* stream) {
+    if (!tr_dev || ninst <= 0) return fail(XLBB_EBADARG, "xlbb_batched_prolong_add: bad argument");
+    return prolong_t(dtype_fine, dtype_coarse, tr_dev, ninst, nullptr, XLBB_STREAM(stream));
+}
+
+int xlbb_batched_prolong_add_norms(int dtype_fine, int dtype_coarse, const XlbbBatchTransfer* tr_dev, int ninst,
+                                   double* parts, double* norms, void* stream) {
+    if (!tr_dev || ninst <= 0 || !parts || !norms)
+        return fail(XLBB_EBADARG, "xlbb_batched_prolong_add_norms: bad argument");
+    const int st_ = prolong_t(dtype_fine, dtype_coarse, tr_dev, ninst, parts, XLBB_STREAM(stream));
+    if (st_ != XLBB_OK) return st_;
+    prolong_norms_kernel<<<ninst, 32, 0, XLBB_STREAM(stream)>>>(parts, ninst, norms);
+    return check_launch("xlbb_batched_prolong_add_norms");
+}
+
+int xlbb_segment_sum(const double* parts, const int* begin_dev, int nseg, double* out, void* stream) {
+    if (!parts || !begin_dev || !out || nseg <= 0) return fail(XLBB_EBADARG, "xlbb_segment_sum: bad argument");
+    segment_sum_kernel<<<nseg, 256, 0, XLBB_STREAM(stream)>>>(parts, begin_dev, nseg, out);
+    return check_launch("xlbb_segment_sum");
 }
 
 }  // extern "C"

@@ -50,17 +50,16 @@ __device__ __forceinline__ int probe_rule(const RuleProbe& p, int x) {
 // collide(p, y, x, const In&, T (&fs)[Q]), fin(const In&, T (&g)[Q]) (the
 // pre-collision input seen by post-collision rules), f_in(const In&, i) (the
 // sweep input used by the mixing / difference terms) and store<PREV>(...).
+// One CTA's strip: owned columns [x0, x0+TX) of rows [ys, ye) of the grid in
+// ``p``.  Returns this thread's contribution to the FP64 sum of the strip.
+// ``post`` is the CTA's 4-slot ring; callers synchronise before reusing it.
 template <class Phys, int TX, int D, bool PREV>
-__global__ void __launch_bounds__(TX + 32) sweep_kernel(const typename Phys::Args p) {
+__device__ __forceinline__ double sweep_strip(const typename Phys::Args& p, int x0, int ys, int ye,
+                                              typename Phys::T (*post)[Phys::Q][TX + 2]) {
     using T = typename Phys::T;
     constexpr int Q = Phys::Q;
-    constexpr int NT = TX + 2;  // owned columns + 2 halo columns
-    __shared__ T post[4][Q][NT];
-    __shared__ double red[(TX + 32) / 32];
-
     const SweepGeom& G = p.geom;
     const int tid = threadIdx.x;
-    const int x0 = blockIdx.x * TX;
     const int w = min(TX, G.nx - x0);
     // Thread -> ring column.  Threads [0, TX) own columns x0+tid (ring col tid+1);
     // the extra warp's lanes 0/1 collide the left/right halo columns.
@@ -77,8 +76,6 @@ __global__ void __launch_bounds__(TX + 32) sweep_kernel(const typename Phys::Arg
     }
     const bool owner = tid < w;
     const int xw = wrap(xg, G.nx);
-    const int ys = (int)(((long long)blockIdx.y * G.ny) / gridDim.y);
-    const int ye = (int)(((long long)(blockIdx.y + 1) * G.ny) / gridDim.y);
 
     typename Phys::In pf[D];      // register ring of prefetched rows
     RuleProbe pcp[D], psp[D];
@@ -133,7 +130,6 @@ __global__ void __launch_bounds__(TX + 32) sweep_kernel(const typename Phys::Arg
                     const int so = (yo + 4) & 3;
                     T S[Q];
 #pragma unroll
-#pragma unroll
                     for (int i = 0; i < Q; ++i) S[i] = post[(yo - Phys::cy(i) + 4) & 3][i][rc - Phys::cx(i)];
                     const int r = probe_rule(ps_prev, xg);
                     if (r >= 0) {
@@ -154,9 +150,21 @@ __global__ void __launch_bounds__(TX + 32) sweep_kernel(const typename Phys::Arg
             }
         }
     }
+    return acc;
+}
+
+template <class Phys, int TX, int D, bool PREV>
+__global__ void __launch_bounds__(TX + 32) sweep_kernel(const typename Phys::Args p) {
+    using T = typename Phys::T;
+    constexpr int Q = Phys::Q;
+    __shared__ T post[4][Q][TX + 2];
+    __shared__ double red[(TX + 32) / 32];
+    const int ys = (int)(((long long)blockIdx.y * p.geom.ny) / gridDim.y);
+    const int ye = (int)(((long long)(blockIdx.y + 1) * p.geom.ny) / gridDim.y);
+    const double acc = sweep_strip<Phys, TX, D, PREV>(p, blockIdx.x * TX, ys, ye, post);
     if (p.sumsq != nullptr) {
         const double s = block_sum(acc, red);
-        if (tid == 0) p.sumsq[blockIdx.y * gridDim.x + blockIdx.x] = s;
+        if (threadIdx.x == 0) p.sumsq[blockIdx.y * gridDim.x + blockIdx.x] = s;
     }
 }
 

@@ -48,14 +48,21 @@ class AdvectionDiffusionReactionBGK(LBMBase):
         self._ps = compile_rules(self.BCs, L.nx, L.ny, 9, self._dtype, L.device, step="PostStreaming")
         self._grad_rules = compile_rules(self.BCs, L.nx, L.ny, 9, self._dtype, L.device, names=GRADIENT_BC_NAMES)
 
-    def gradient_rules(self, nx, ny):
-        """Gradient rules on an ``nx x ny`` grid (a coarse multigrid level uses the
-        fine-level index sets, clamped/dropped like JAX does)."""
-        if (nx, ny) == (self.nx, self.ny):
+    def gradient_rules(self, nx, ny, dtype=None):
+        """Gradient rules on an ``nx x ny`` grid in ``dtype`` (default: this
+        solver's); a coarse multigrid level uses the fine-level index sets,
+        clamped/dropped like JAX does."""
+        dtype = self._dtype if dtype is None else dtype
+        if (nx, ny) == (self.nx, self.ny) and dtype == self._dtype:
             return self._grad_rules
-        key = (nx, ny)
+        key = (nx, ny, dtype)
         if key not in self._grad_rules_by_shape:
-            self._grad_rules_by_shape[key] = self._grad_rules.restricted(nx, ny, self._dtype, self._layout.device)
+            L = self._layout
+            if (nx, ny) == (self.nx, self.ny):
+                r = compile_rules(self.BCs, L.nx, L.ny, 9, dtype, L.device, names=GRADIENT_BC_NAMES)
+            else:
+                r = self._grad_rules.restricted(nx, ny, dtype, L.device)
+            self._grad_rules_by_shape[key] = r
         return self._grad_rules_by_shape[key]
 
     # ------------------------------------------------------------------ kernels
@@ -72,19 +79,22 @@ class AdvectionDiffusionReactionBGK(LBMBase):
             _lib.stream_ptr()), "xlbb_darcy_moments")
         return (rho, grad) if gradient else rho
 
-    def gradient(self, q, scale=1.0, out=None, base=None):
+    def gradient(self, q, scale=1.0, out=None, base=None, dtype=None):
         """``src/darcy.py:75-104`` (kernel ``xlbb_darcy_gradient``); works on any
-        multigrid level's grid.  ``base`` (optional) is added to the result."""
+        multigrid level's grid.  ``base`` (optional) is added to the result.
+        ``dtype`` (default: this solver's precision) is the precision of the
+        computation and of the result."""
         from .fields import Layout
         nx, ny = int(q.shape[0]), int(q.shape[1])
-        L = self._layout if (nx, ny) == (self.nx, self.ny) else Layout(nx, ny, self._dtype)
+        dtype = self._dtype if dtype is None else dtype
+        L = self._layout if (nx, ny, dtype) == (self.nx, self.ny, self._dtype) else Layout(nx, ny, dtype)
         qf = L.field(q, 1)
         base = L.field(base, 2)     # other precision / layout -> this grid (kept alive over the launch)
         out = L.empty(2) if out is None else out
-        rules = self.gradient_rules(nx, ny)
+        rules = self.gradient_rules(nx, ny, dtype)
         _lib.check(_lib.lib().xlbb_darcy_gradient(
-            self._dcode, L.grid(), _lib.ptr(qf), float(scale), rules.struct(), _lib.ptr(base), _lib.ptr(out),
-            _lib.stream_ptr()), "xlbb_darcy_gradient")
+            _lib.dtype_code(dtype), L.grid(), _lib.ptr(qf), float(scale), rules.struct(), _lib.ptr(base),
+            _lib.ptr(out), _lib.stream_ptr()), "xlbb_darcy_gradient")
         return out
 
     def collision(self, f, external_source=None):
@@ -122,7 +132,7 @@ class AdvectionDiffusionReactionBGK(LBMBase):
         out = L.empty(9) if out is None else out
         if sumsq:
             # one FP64 partial per CTA of the current launch shape
-            self._n_partials = _lib.check(_lib.lib().xlbb_darcy_sweep_ctas(L.grid()), "xlbb_darcy_sweep_ctas")
+            self._n_partials = _lib.check(_lib.lib().xlbb_darcy_sweep_ctas(self._dcode, L.grid()), "xlbb_darcy_sweep_ctas")
             if self._partials.numel() < self._n_partials:
                 self._partials = torch.empty(self._n_partials, dtype=torch.float64, device=L.device)
         s = _lib.DarcySweep(f.data_ptr(), out.data_ptr(), float(self.omega),

@@ -62,6 +62,12 @@ class LBMElasticity:
         if kwargs.get("coarsest_precision") == "f64" and self.levels > 1:
             self._level_dtypes[-1] = torch.float64
         self._layouts = [Layout(*self.grid_size(l), self._level_dtypes[l]) for l in range(self.levels)]
+        # Extension: ``residual_precision="f64"`` computes the level-0 residual sweep
+        # of an FP32 multigrid solve in FP64 arithmetic (FP32 storage): the coarse
+        # corrections then see the residual of the stored state without FP32
+        # rounding noise, which otherwise limits the solution's accuracy.
+        self._res64 = (kwargs.get("residual_precision") == "f64" and self.levels > 1
+                       and self._level_dtypes[0] == torch.float32)
         self.boundingBoxIndices = self.bounding_box_indices()
         self._create_boundary_data()
         force = self.get_force()
@@ -299,6 +305,10 @@ class LBMElasticity:
             pc = compile_rules(bcs, L.nx, L.ny, 8, L.dtype, L.device, step="PostCollision")
             ps = compile_rules(bcs, L.nx, L.ny, 8, L.dtype, L.device, step="PostStreaming")
             self._rules.append((pc, ps))
+        if self._res64:      # FP64 rule constants of the FP64-arithmetic residual sweep
+            L = self._layouts[0]
+            self._rules_acc64 = (compile_rules(self.BCs, L.nx, L.ny, 8, torch.float64, L.device, step="PostCollision"),
+                                 compile_rules(self.BCs, L.nx, L.ny, 8, torch.float64, L.device, step="PostStreaming"))
 
     def distributed_array_init(self, shape, type, init_val=0, sharding=None):
         """A device field of ``shape`` filled with ``init_val`` (``:438-458``)."""
@@ -453,17 +463,20 @@ class LBMElasticity:
 
     # ------------------------------------------------------------------ kernels
     def _sweep(self, f, level, a=0.0, b=1.0, resid=None, fext=None, out=None, sumsq=False, div_out=None,
-               sumsq_diff=False):
+               sumsq_diff=False, acc64=False):
+        """One fused sweep on ``level``; ``acc64``: FP64 arithmetic on the FP32
+        level-0 fields (``residual_precision="f64"``)."""
         L = self._L(level)
         out = L.empty(8) if out is None else out
         if fext is not None and not L.conforms(fext, 2):
             fext = L.field(fext, 2)      # e.g. a coupling force computed in another precision
+        code = _lib.XLBB_F32_ACC64 if acc64 else _lib.dtype_code(L.dtype)
         if sumsq:
             # one FP64 partial per CTA of the current launch shape
-            self._n_partials = _lib.check(_lib.lib().xlbb_elast_sweep_ctas(L.grid()), "xlbb_elast_sweep_ctas")
+            self._n_partials = _lib.check(_lib.lib().xlbb_elast_sweep_ctas(code, L.grid()), "xlbb_elast_sweep_ctas")
             if self._partials.numel() < self._n_partials:
                 self._partials = torch.empty(self._n_partials, dtype=torch.float64, device=L.device)
-        pc, ps = self._rules[level]
+        pc, ps = self._rules_acc64 if acc64 else self._rules[level]
         bx0, bx1, by0, by1 = self._box(level)
         s = _lib.ElastSweep(f.data_ptr(), out.data_ptr(), self.force.data_ptr() if self.force is not None else None,
                             1 if level == 0 else 0, fext.data_ptr() if fext is not None else None,
@@ -471,8 +484,7 @@ class LBMElasticity:
                             pc.struct(), ps.struct(), self._partials.data_ptr() if sumsq else None,
                             bx0, bx1, by0, by1, div_out.data_ptr() if div_out is not None else None,
                             1 if sumsq_diff else 0)
-        _lib.check(_lib.lib().xlbb_elast_sweep(_lib.dtype_code(L.dtype), L.grid(), self._mat, s, _lib.stream_ptr()),
-                   "xlbb_elast_sweep")
+        _lib.check(_lib.lib().xlbb_elast_sweep(code, L.grid(), self._mat, s, _lib.stream_ptr()), "xlbb_elast_sweep")
         return out
 
     def _reduce_partials(self, out_scalar):
@@ -584,7 +596,8 @@ class LBMElasticity:
         res_norm = None
         if level < self.levels - 1:
             ext = self._ext_force(fe, nonlinear_force, f, level)
-            res = self._sweep(f, level, 1.0, -1.0, resid=residual, fext=ext, sumsq=(level == 0))
+            res = self._sweep(f, level, 1.0, -1.0, resid=residual, fext=ext, sumsq=(level == 0),
+                              acc64=(level == 0 and self._res64))
             if level == 0:
                 _lib.check(_lib.lib().xlbb_reduce_sum(self._partials.data_ptr(), self._n_partials,
                                                       self._scalar.data_ptr(),

@@ -26,9 +26,52 @@ class DivGradForce:
         return self.darcy.gradient(self.elasticity.update_divergence(f_el), self.scale)
 
     def evaluate(self, el, f, level, external_force):
-        """external_force + N(f) on multigrid level ``level``."""
+        """external_force + N(f) on multigrid level ``level``, computed in that
+        level's precision (the precision of the sweep that consumes it)."""
         div = el.update_divergence(f, level)
-        return self.darcy.gradient(div, self.scale, base=external_force)
+        return self.darcy.gradient(div, self.scale, base=external_force, dtype=div.dtype)
+
+
+class BiotStepGraph:
+    """One coupled Biot step captured as a CUDA graph.
+
+    The graph reads the state from three static buffers (elasticity and Darcy
+    populations, dt_div_eta), runs ``LBMPoroelasticity.step`` (every kernel of
+    the V-cycles, the coupling gradients and the Darcy sweep) and copies the new
+    state back into the same buffers, so each ``replay`` advances one time step
+    with one graph launch.  Valid while the step takes no host decisions: no
+    dynamic force or source hooks and a fixed inner cycle count.  The other
+    outputs (eta, sigma, pressure, pressure_grad) live in the graph's memory and
+    are overwritten by the next replay."""
+
+    def __init__(self, sim, f_el, f_darcy, dt_div_eta):
+        el, da = sim.elasticity, sim.darcy
+        self.f_el = el._L().empty(8)
+        self.f_darcy = da._layout.empty(9)
+        self.dt_div_eta = da._layout.empty(1)
+        self.load(f_el, f_darcy, dt_div_eta)
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):
+            sim.step(self.f_el, self.f_darcy, self.dt_div_eta, 0)    # warm-up: scratch buffers, module loading
+        torch.cuda.current_stream().wait_stream(side)
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            out = sim.step(self.f_el, self.f_darcy, self.dt_div_eta, 0)
+            self.f_el.copy_(out[0])
+            self.f_darcy.copy_(out[1])
+            self.dt_div_eta.copy_(out[4])
+        self.outputs = (self.f_el, self.f_darcy) + tuple(out[2:4]) + (self.dt_div_eta,) + tuple(out[5:7])
+
+    def load(self, f_el, f_darcy, dt_div_eta):
+        self.f_el.copy_(f_el)
+        self.f_darcy.copy_(f_darcy)
+        self.dt_div_eta.copy_(dt_div_eta)
+
+    def replay(self):
+        """One time step; returns the 7-tuple of ``step`` (static tensors)."""
+        self.graph.replay()
+        return self.outputs
 
 
 class LBMPoroelasticity:
@@ -63,6 +106,9 @@ class LBMPoroelasticity:
             self.printInfoRate = 0
         self.useDynamicForce = self.get_elastic_force(0) is not None
         self.useDynamicSource = self.get_darcy_source(0) is not None
+        # Extension: ``cuda_graph`` (default True) lets ``run`` replay the coupled
+        # step as one CUDA graph when the step takes no host decisions.
+        self.cudaGraph = kwargs.get("cuda_graph", True)
         self.show_simulation_parameters()
 
     # validation (src/poroelasticity.py:72-176)
@@ -204,15 +250,31 @@ class LBMPoroelasticity:
             f_el = el.equilibrium(eta, sigma, external_force=force)
         return f_el, f_darcy, dt_div_eta
 
+    def graph_capturable(self):
+        """True when one coupled step takes no host decisions (no dynamic force or
+        source hooks, a fixed inner cycle count), so it can be a CUDA graph."""
+        return not (self.useDynamicForce or self.useDynamicSource) and self.elasticityTol is None
+
+    def capture_step(self, f_el, f_darcy, dt_div_eta):
+        """A ``BiotStepGraph`` starting from the given state."""
+        if not self.graph_capturable():
+            raise ValueError("the coupled step takes host decisions (dynamic hooks or elasticity_tol)")
+        return BiotStepGraph(self, f_el, f_darcy, dt_div_eta)
+
     def run(self, t_max):
-        """``:208-301`` (t_max + 1 coupled steps)."""
+        """``:208-301`` (t_max + 1 coupled steps; one CUDA graph replay per step
+        when ``graph_capturable``)."""
         f_el, f_darcy, dt_div_eta = self.init_state()
+        graph = self.capture_step(f_el, f_darcy, dt_div_eta) if self.cudaGraph and self.graph_capturable() else None
         start = time.time()
         for timestep in range(0, t_max + 1):
             io_flag = self.ioRate > 0 and (timestep % self.ioRate == 0 or timestep == t_max)
             print_iter_flag = self.printInfoRate > 0 and timestep % self.printInfoRate == 0
-            f_el, f_darcy, eta, sigma, dt_div_eta, pressure, pressure_grad = \
-                self.step(f_el, f_darcy, dt_div_eta, timestep)
+            if graph is not None:
+                f_el, f_darcy, eta, sigma, dt_div_eta, pressure, pressure_grad = graph.replay()
+            else:
+                f_el, f_darcy, eta, sigma, dt_div_eta, pressure, pressure_grad = \
+                    self.step(f_el, f_darcy, dt_div_eta, timestep)
             if print_iter_flag:
                 print(f"Timestep {timestep} of {t_max} completed")
             if io_flag:

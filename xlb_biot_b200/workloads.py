@@ -130,6 +130,40 @@ def periodic_biot_1024(m, n=1024, levels=5, lam=None, mu=None, alpha=1.0, K=0.1,
     return PB(**kw)
 
 
+def fourier_force(n, rng, modes=4):
+    """Sum of ``modes`` periodic Fourier modes with N(0, 1) amplitudes (random
+    wave numbers 1..3, phases), scaled by 1/n^2 like the examples' forces."""
+    x = (np.arange(n) + 0.5) / n
+    X, Y = np.meshgrid(x, x, indexing="ij")
+    f = np.zeros((n, n, 2))
+    for _ in range(modes):
+        kx, ky = rng.integers(1, 4, size=2)
+        ph = rng.uniform(0, 2 * np.pi, size=2)
+        a = rng.standard_normal(2)
+        arg = 2 * np.pi * (kx * X + ky * Y)
+        f[..., 0] += a[0] * np.sin(arg + ph[0])
+        f[..., 1] += a[1] * np.cos(arg + ph[1])
+    return f / n ** 2
+
+
+def batch_instances(count=512, sizes=(64, 96, 128, 192, 256, 384), mu_range=(0.5, 2.0), nu_range=(0.1, 0.4),
+                    stress_unit=16.0, seed=0):
+    """Seeded heterogeneous batch: square sizes drawn uniformly from ``sizes``,
+    shear modulus uniform in ``mu_range`` and Poisson ratio uniform in
+    ``nu_range`` (plane stress, lam = 2 mu nu / (1 - nu)), random smooth
+    forces.  Moduli are expressed in units of ``stress_unit``: the D2Q8
+    model's equilibrium is singular at lattice lambda + mu = 1/3 and the
+    reference's V-cycle diverges for lattice moduli of order one, so the
+    default keeps lambda + mu <= 0.29."""
+    rng = np.random.default_rng(seed)
+    ns = rng.choice(np.asarray(sizes), size=count)
+    mus = rng.uniform(*mu_range, size=count) / stress_unit
+    nus = rng.uniform(*nu_range, size=count)
+    lams = 2 * mus * nus / (1 - nus)
+    forces = [fourier_force(int(n), rng) for n in ns]
+    return [(int(n), int(n)) for n in ns], lams, mus, forces
+
+
 def darcy_lognormal(m, n=1024, ell=16.0, sigma=1.0, seed=0, precision="f32/f32"):
     """Construct the workload's solver in namespace ``m``.  Returns
     ``(solver, k_field)``; the solver carries the per-cell omega field
