@@ -12,8 +12,31 @@ from .boundary_conditions import (BoundaryCondition, create_grid_mask, solid_vox
 from .lattice import Policy
 
 
+def coarsen_field(a, mg_bcs):
+    """Extension without a reference counterpart (the reference's Lame
+    parameters are uniform): the material field of the next coarser level.
+    Interior: mean of each 2 x 2 fine block (the block the restriction sums);
+    rows / columns kept by ``MG_BCs``: mean of the fine pair along them;
+    corners: copied."""
+    l, r, b, t = (int(mg_bcs[k]) for k in ("left", "right", "bottom", "top"))
+    nx, ny = a.shape
+    nxc, nyc = (nx - l - r) // 2 + l + r, (ny - b - t) // 2 + b + t
+    out = np.empty((nxc, nyc), dtype=a.dtype)
+    for X in range(nxc):
+        for Y in range(nyc):
+            xin, yin = l <= X < nxc - r, b <= Y < nyc - t
+            xs = [l + 2 * (X - l), l + 2 * (X - l) + 1] if xin else [0 if X < l else nx - 1]
+            ys = [b + 2 * (Y - b), b + 2 * (Y - b) + 1] if yin else [0 if Y < b else ny - 1]
+            out[X, Y] = np.mean([a[x, y] for x in xs for y in ys])
+    return out
+
+
 class LBMElasticity:
-    """``src/elasticity.py:30-1501``."""
+    """``src/elasticity.py:30-1501``.
+
+    Extension: ``lambda_field`` / ``mu_field`` (shape (nx, ny)) give per-cell
+    Lame parameters; coarse levels use ``coarsen_field``.  With uniform fields
+    every formula reduces to the reference's."""
 
     def __init__(self, **kwargs):
         self.lamda = kwargs.get("lambda")
@@ -43,6 +66,39 @@ class LBMElasticity:
         self.force = self.get_force()
         if self.force is not None:
             self.force = np.asarray(self.force, dtype=self.precisionPolicy.compute_dtype)
+        self._fields = None
+        lf, mf = kwargs.get("lambda_field"), kwargs.get("mu_field")
+        if lf is not None:
+            lam = np.asarray(lf, dtype=np.float64).reshape(self.nx, self.ny)
+            mu = np.asarray(mf, dtype=np.float64).reshape(self.nx, self.ny)
+            self._fields = [(lam, mu)]
+            for _ in range(1, self.levels):
+                lam, mu = coarsen_field(lam, self.mg_BCs), coarsen_field(mu, self.mg_BCs)
+                self._fields.append((lam, mu))
+
+    def _material(self, shape):
+        """(lambda, mu) for an array of ``shape``: scalars, or (nx, ny, 1) fields
+        of the level whose grid has that shape."""
+        if self._fields is None:
+            return self.lamda, self.mu
+        for level in range(self.levels):
+            if tuple(shape[:2]) == self.grid_size(level):
+                lam, mu = self._fields[level]
+                dt = self.precisionPolicy.compute_dtype
+                return lam[..., None].astype(dt), mu[..., None].astype(dt)
+        raise ValueError("no level has this shape")
+
+    def _m_to_f_apply(self, m, lam, mu):
+        """m (..., 7) @ m_to_f with a per-cell ms row when the fields vary."""
+        if self._fields is None:
+            return np.matmul(m, self.m_to_f)
+        g = 1.0 / (12.0 * (lam + mu) - 4.0)
+        g = np.where(np.abs(g) > 100, 0.0, g)
+        base = self.m_to_f.copy()
+        base[2, :] = 0
+        hn = np.concatenate([np.broadcast_to(0.25 + 0.5 * g, g.shape[:2] + (4,)),
+                             np.broadcast_to(-0.25 * g, g.shape[:2] + (4,))], axis=-1)
+        return np.matmul(m, base) + m[..., 2:3] * hn
 
     # -- setup -------------------------------------------------------------
     def _create_boundary_data(self):
@@ -134,13 +190,14 @@ class LBMElasticity:
             eta = eta - 0.5 * self.force
         if external_force is not None:
             eta = eta - 0.5 * external_force
-        cs = -1.0 - 1 / (3 * (self.lamda + self.mu))
+        lam, mu = self._material(np.shape(sigma))
+        cs = -1.0 - 1 / (3 * (lam + mu))
         ms = (sigma[..., 0:1] + sigma[..., 2:3]) * cs
-        cd = -1.0 - 1 / (6 * self.mu)
+        cd = -1.0 - 1 / (6 * mu)
         md = (sigma[..., 0:1] - sigma[..., 2:3]) * cd
         m11 = sigma[..., 1:2] * cd
         m = np.concatenate((eta, ms, md, m11, eta / 3.0), axis=-1)
-        feq = np.matmul(m, self.m_to_f)
+        feq = self._m_to_f_apply(m, lam, mu)
         return self.precisionPolicy.cast_to_output(feq) if cast_output else feq
 
     def collision(self, f, external_force, use_force=True):
@@ -148,8 +205,9 @@ class LBMElasticity:
         f = self.precisionPolicy.cast_to_compute(f)
         external_force = self.precisionPolicy.cast_to_compute(external_force)
         m = np.matmul(f, self.f_to_m)
-        cs = (3 * (self.lamda + self.mu) - 1) / (3 * (self.lamda + self.mu) + 1)
-        cd = (6 * self.mu - 1) / (6 * self.mu + 1)
+        lam, mu = self._material(f.shape)
+        cs = (3 * (lam + mu) - 1) / (3 * (lam + mu) + 1)
+        cd = (6 * mu - 1) / (6 * mu + 1)
         if use_force and self.force is not None and external_force is not None:
             force = self.force + external_force
         elif external_force is not None:
@@ -164,7 +222,7 @@ class LBMElasticity:
         else:
             m = np.concatenate([m[..., 0:2], m[..., 2:3] * cs, m[..., 3:5] * cd,
                                 m[..., 0:2] / 3.0], axis=-1)
-        return self.precisionPolicy.cast_to_output(np.matmul(m, self.m_to_f))
+        return self.precisionPolicy.cast_to_output(self._m_to_f_apply(m, lam, mu))
 
     def update_macroscopic(self, f, external_force=None):
         """``:1002-1038``."""
@@ -174,16 +232,20 @@ class LBMElasticity:
             eta = eta + 0.5 * self.force
         if external_force is not None:
             eta = eta + 0.5 * external_force
-        cs = -1.5 * (self.lamda + self.mu) / (3 * (self.lamda + self.mu) + 1)
+        lam, mu = self._material(f.shape)
+        if self._fields is not None:
+            lam, mu = lam[..., 0], mu[..., 0]
+        cs = -1.5 * (lam + mu) / (3 * (lam + mu) + 1)
         ms = m[..., 2] * cs
-        cd = -3 * self.mu / (6 * self.mu + 1)
+        cd = -3 * mu / (6 * mu + 1)
         md = m[..., 3] * cd
         sigma = np.stack((ms + md, (2 * cd) * m[..., 4], ms - md), axis=-1)
         return eta, sigma
 
     def update_divergence(self, f):
         """``:1040-1058``."""
-        return (-1.5 / (3 * (self.lamda + self.mu) + 1)) * np.matmul(f, self.f_to_m[:, 2:3])
+        lam, mu = self._material(f.shape)
+        return (-1.5 / (3 * (lam + mu) + 1)) * np.matmul(f, self.f_to_m[:, 2:3])
 
     def streaming(self, f):
         return stream(f, self.c)

@@ -21,6 +21,43 @@ from .boundary_conditions import (BoundaryCondition, _at_add, _at_set, _take, gr
 from .fields import Layout, torch_dtype
 
 
+def coarsen_material(a, mg_bcs):
+    """Material field of the next coarser multigrid level (torch, differentiable).
+
+    Extension without a reference counterpart (the reference has uniform
+    Lame parameters).  Interior cells: mean of the 2 x 2 fine block (the
+    block the restriction sums); boundary rows / columns kept by ``MG_BCs``:
+    mean of the fine pair along the boundary; corners: copied."""
+    l, r, b, t = (int(mg_bcs[k]) for k in ("left", "right", "bottom", "top"))
+    nx, ny = a.shape
+    inner = a[l:nx - r, b:ny - t]
+    c = 0.25 * (inner[0::2, 0::2] + inner[1::2, 0::2] + inner[0::2, 1::2] + inner[1::2, 1::2])
+    if b:
+        c = torch.cat([(0.5 * (a[l:nx - r, 0][0::2] + a[l:nx - r, 0][1::2]))[:, None], c], 1)
+    if t:
+        c = torch.cat([c, (0.5 * (a[l:nx - r, ny - 1][0::2] + a[l:nx - r, ny - 1][1::2]))[:, None]], 1)
+
+    def column(x):
+        mid = 0.5 * (a[x, b:ny - t][0::2] + a[x, b:ny - t][1::2])
+        parts = ([a[x, 0:1]] if b else []) + [mid] + ([a[x, ny - 1:ny]] if t else [])
+        return torch.cat(parts)[None, :]
+    if l:
+        c = torch.cat([column(0), c], 0)
+    if r:
+        c = torch.cat([c, column(nx - 1)], 0)
+    return c
+
+
+def material_hierarchy(lam, mu, mg_bcs, levels):
+    """Per-level (lambda, mu) fields: level 0 as given, each coarser level by
+    ``coarsen_material``."""
+    out = [(lam, mu)]
+    for _ in range(1, levels):
+        lam, mu = coarsen_material(lam, mg_bcs), coarsen_material(mu, mg_bcs)
+        out.append((lam, mu))
+    return out
+
+
 class LBMElasticity:
     """``src/elasticity.py:30-1501``."""
 
@@ -73,7 +110,15 @@ class LBMElasticity:
         force = self.get_force()
         self.force = self._layouts[0].field(force, 2) if force is not None else None
         self._mat = _lib.ElastMaterial(float(self.lamda), float(self.mu), None, None)
-        self._lam_field = self._mu_field = None
+        self._mats = [self._mat] * self.levels
+        # Extension: per-cell Lame fields (``lambda_field``, ``mu_field``, shape
+        # (nx, ny) or (nx, ny, 1)); coarse levels use ``coarsen_material``.
+        self._lam_fields = self._mu_fields = None
+        lf, mf = kwargs.get("lambda_field"), kwargs.get("mu_field")
+        if (lf is None) != (mf is None):
+            raise ValueError("lambda_field and mu_field go together")
+        if lf is not None:
+            self.set_material_fields(lf, mf)
         self._div_scale = -1.5 / (3 * (self.lamda + self.mu) + 1)
         self._partials = torch.empty(0, dtype=torch.float64, device=self._layouts[0].device)
         self._n_partials = 0
@@ -333,6 +378,32 @@ class LBMElasticity:
     def get_force(self):
         pass
 
+    # ------------------------------------------------------------------ material fields
+    def set_material_fields(self, lam_field, mu_field):
+        """Per-cell Lame fields on every level (written in place, so CUDA graphs
+        captured earlier see the new values)."""
+        dev = self._layouts[0].device
+
+        def as2d(x):
+            t = torch.as_tensor(x.detach() if isinstance(x, torch.Tensor) else np.asarray(x),
+                                dtype=torch.float64, device=dev)
+            return t.reshape(self.nx, self.ny)
+        hier = material_hierarchy(as2d(lam_field), as2d(mu_field), self.mg_BCs, self.levels)
+        if self._lam_fields is None:
+            self._lam_fields = [self._L(l).empty(1) for l in range(self.levels)]
+            self._mu_fields = [self._L(l).empty(1) for l in range(self.levels)]
+        for l, (lam, mu) in enumerate(hier):
+            self._lam_fields[l].copy_(lam[..., None])
+            self._mu_fields[l].copy_(mu[..., None])
+        self._mats = [_lib.ElastMaterial(float(self.lamda), float(self.mu), self._lam_fields[l].data_ptr(),
+                                         self._mu_fields[l].data_ptr()) for l in range(self.levels)]
+
+    def material_fields(self, level=0):
+        """(lambda, mu) fields of ``level`` (None if uniform)."""
+        if self._lam_fields is None:
+            return None, None
+        return self._lam_fields[level], self._mu_fields[level]
+
     # ------------------------------------------------------------------ fields
     def _L(self, level=0):
         return self._layouts[level]
@@ -359,7 +430,7 @@ class LBMElasticity:
         # a freed temporary's block is handed to the next allocation on the stream
         eta_d, sigma_d = L.field(eta, 2), L.field(sigma, 3)
         _lib.check(_lib.lib().xlbb_elast_equilibrium(
-            self._dcode, L.grid(), self._mat, _lib.ptr(eta_d), _lib.ptr(sigma_d),
+            self._dcode, L.grid(), self._mats[0], _lib.ptr(eta_d), _lib.ptr(sigma_d),
             _lib.ptr(self.force), _lib.ptr(fe), _lib.ptr(out), _lib.stream_ptr()), "xlbb_elast_equilibrium")
         return out
 
@@ -370,7 +441,7 @@ class LBMElasticity:
         eta, sigma = L.empty(2), L.empty(3)
         fe = L.field(external_force, 2)
         _lib.check(_lib.lib().xlbb_elast_moments(
-            self._dcode, L.grid(), self._mat, _lib.ptr(f), _lib.ptr(self.force), _lib.ptr(fe),
+            self._dcode, L.grid(), self._mats[0], _lib.ptr(f), _lib.ptr(self.force), _lib.ptr(fe),
             _lib.ptr(eta), _lib.ptr(sigma), None, 0.0, _lib.stream_ptr()), "xlbb_elast_moments")
         return eta, sigma
 
@@ -382,7 +453,7 @@ class LBMElasticity:
         f = self._f(f, level)
         div = L.empty(1)
         _lib.check(_lib.lib().xlbb_elast_moments(
-            _lib.dtype_code(L.dtype), L.grid(), self._mat, _lib.ptr(f), None, None, None, None, _lib.ptr(div),
+            _lib.dtype_code(L.dtype), L.grid(), self._mats[level], _lib.ptr(f), None, None, None, None, _lib.ptr(div),
             self._div_scale, _lib.stream_ptr()), "xlbb_elast_moments")
         return div
 
@@ -409,13 +480,26 @@ class LBMElasticity:
         f2m = torch.as_tensor(self.f_to_m, device=fd.device, dtype=fd.dtype)
         m2f = torch.as_tensor(self.m_to_f, device=fd.device, dtype=fd.dtype)
         m = fd @ f2m
-        cs = (3 * (self.lamda + self.mu) - 1) / (3 * (self.lamda + self.mu) + 1)
-        cd = (6 * self.mu - 1) / (6 * self.mu + 1)
+        lam_f, mu_f = self.material_fields(level)
+        if lam_f is None:
+            lam, mu = self.lamda, self.mu
+        else:
+            lam, mu = lam_f.to(fd.dtype), mu_f.to(fd.dtype)
+        cs = (3 * (lam + mu) - 1) / (3 * (lam + mu) + 1)
+        cd = (6 * mu - 1) / (6 * mu + 1)
         if F is not None:
             m = torch.cat([m[..., 0:2] + F, m[..., 2:3] * cs, m[..., 3:5] * cd, m[..., 0:2] / 3.0 + F / 6.0], -1)
         else:
             m = torch.cat([m[..., 0:2], m[..., 2:3] * cs, m[..., 3:5] * cd, m[..., 0:2] / 3.0], -1)
-        return self._L(level).field(m @ m2f, 8)
+        if lam_f is None:
+            return self._L(level).field(m @ m2f, 8)
+        # per-cell m_to_f: only the ms row (h for the axis, n for the diagonal directions) varies
+        g = 1.0 / (12.0 * (lam + mu) - 4.0)
+        g = torch.where(g.abs() > 100, torch.zeros_like(g), g)
+        hn = torch.cat([(0.25 + 0.5 * g).expand(*g.shape[:2], 4), (-0.25 * g).expand(*g.shape[:2], 4)], -1)
+        m2f0 = m2f.clone()
+        m2f0[2, :] = 0
+        return self._L(level).field(m @ m2f0 + m[..., 2:3] * hn, 8)
 
     def streaming(self, f):
         """Periodic pull streaming (``:738-803``; API compatibility)."""
@@ -484,7 +568,8 @@ class LBMElasticity:
                             pc.struct(), ps.struct(), self._partials.data_ptr() if sumsq else None,
                             bx0, bx1, by0, by1, div_out.data_ptr() if div_out is not None else None,
                             1 if sumsq_diff else 0)
-        _lib.check(_lib.lib().xlbb_elast_sweep(code, L.grid(), self._mat, s, _lib.stream_ptr()), "xlbb_elast_sweep")
+        _lib.check(_lib.lib().xlbb_elast_sweep(code, L.grid(), self._mats[level], s, _lib.stream_ptr()),
+                   "xlbb_elast_sweep")
         return out
 
     def _reduce_partials(self, out_scalar):

@@ -191,3 +191,80 @@ def darcy_lognormal(m, n=1024, ell=16.0, sigma=1.0, seed=0, precision="f32/f32")
     if getattr(solver, "omega_field", None) is None:
         solver.omega = omega.astype(solver.precisionPolicy.compute_dtype)
     return solver, k
+
+
+def terzaghi_heterogeneous(m, nx=512, ny=258, levels=5, mu0=0.04, nu=0.25, K0=0.1, sigma=0.5, ell=24.0,
+                           load=1e-3, cycles=4, k_smooth=4, seed=0, precision="f32/f32", darcy_precision=None,
+                           coarsest_precision=None, residual_precision=None, log_mu=None, log_k=None):
+    """2D Terzaghi-type consolidation with heterogeneous material.
+
+    A layer of ``ny - 2`` cell rows (plus one boundary row at the bottom and at
+    the top), periodic in x (laterally infinite: no net flux through the
+    sides).  Elasticity: fixed bottom (full-way bounce-back), top loaded by the
+    traction (0, -load * (1 - cos(2 pi (x + 1/2) / nx)) / 2) (anti-bounce-back);
+    Darcy: no flux at the bottom (bounce-back), drained top p = 0
+    (anti-bounce-back); zero initial displacement and pressure.  Per-cell
+    shear modulus mu = mu0 exp(g_mu), lambda = 2 mu nu / (1 - nu) (fixed
+    Poisson ratio), permeability K = K0 exp(g_K), omega = 1 / (3 K + 1/2);
+    g_mu, g_K seeded Gaussian random fields (correlation length ``ell``,
+    standard deviation ``sigma``) unless given (``log_mu``, ``log_k``: the
+    fields g).  ``levels``-level V-cycles (MG_BCs bottom/top, ``k_smooth``
+    smoothing sweeps), ``cycles`` V-cycles per time step, centred coupling.
+    Returns (sim, material) with material = dict(log_mu, log_k, mu, lam, K, omega)."""
+    g_mu = gaussian_random_field(nx, ny, ell, sigma, seed) if log_mu is None else np.asarray(log_mu, np.float64)
+    g_k = gaussian_random_field(nx, ny, ell, sigma, seed + 1) if log_k is None else np.asarray(log_k, np.float64)
+    mu = mu0 * np.exp(g_mu)
+    lam = mu * (2 * nu / (1 - nu))
+    K = K0 * np.exp(g_k)
+    omega = 1.0 / (3.0 * K + 0.5)
+    x = np.arange(nx)
+    traction = np.zeros((nx, 2))
+    traction[:, 1] = -load * 0.5 * (1 - np.cos(2 * np.pi * (x + 0.5) / nx))
+
+    class Darcy(m.AdvectionDiffusionReactionBGK):
+        def initialize_macroscopic_fields(self):
+            return (self.distributed_array_init((self.nx, self.ny, 1), self.precisionPolicy.output_dtype, init_val=0.0),
+                    self.distributed_array_init((self.nx, self.ny, 2), self.precisionPolicy.output_dtype, init_val=0.0))
+
+        def set_boundary_conditions(self):
+            bb = self.boundingBoxIndices
+            self.BCs.append(m.ADR_Neumann_BounceBack(tuple(bb["bottom"].T), self.gridInfo, self.precisionPolicy))
+            self.BCs.append(m.ADR_AntiBounceBack(tuple(bb["top"].T), self.gridInfo, self.precisionPolicy,
+                                                 rho=np.zeros((len(bb["top"]), 1))))
+
+    class Elasticity(m.LBMElasticity):
+        def initialize_macroscopic_fields(self):
+            return (self.distributed_array_init((self.nx, self.ny, 2), self.precisionPolicy.output_dtype, init_val=0.0),
+                    self.distributed_array_init((self.nx, self.ny, 3), self.precisionPolicy.output_dtype, init_val=0.0))
+
+        def set_boundary_conditions(self):
+            bb = self.boundingBoxIndices
+            self.BCs.append(m.ElasticityBounceBackFullway(tuple(bb["bottom"].T), self.gridInfo, self.precisionPolicy))
+            self.BCs.append(m.ElasticityAntiBounceBack(tuple(bb["top"].T), self.gridInfo, self.precisionPolicy,
+                                                       traction))
+            for level in range(1, self.levels):
+                gi, bbl = self.grid_info(level), self.bounding_box_indices(level)
+                self.BCs_MG[level] = [
+                    m.ElasticityBounceBackFullway(tuple(bbl["bottom"].T), gi, self.precisionPolicy),
+                    m.ElasticityAntiBounceBack(tuple(bbl["top"].T), gi, self.precisionPolicy)]
+
+    class Consolidation(m.LBMPoroelasticity):
+        def __init__(self, **kw):
+            super().__init__(Elasticity, Darcy, **kw)
+
+    kw = dict(lattice_elasticity=m.LatticeD2Q8(precision), lattice_darcy=m.LatticeD2Q9(darcy_precision or precision),
+              **{"lambda": float(np.mean(lam))}, mu=float(np.mean(mu)), lambda_field=lam, mu_field=mu,
+              omega=float(np.mean(omega)), omega_field=omega[..., None], alpha=1.0, nx=nx, ny=ny, nz=0,
+              precision=precision, elasticity_MG_levels=levels, elasticity_steps=cycles,
+              MG_BCs={"bottom": True, "top": True}, MG_n_smoothing=k_smooth, coupling_method="centered",
+              print_info_rate=0)
+    if darcy_precision:
+        kw["darcy_precision"] = darcy_precision
+    if coarsest_precision:
+        kw["coarsest_precision"] = coarsest_precision
+    if residual_precision:
+        kw["residual_precision"] = residual_precision
+    sim = Consolidation(**kw)
+    if getattr(sim.darcy, "omega_field", None) is None:
+        sim.darcy.omega = omega[..., None].astype(sim.darcy.precisionPolicy.compute_dtype)
+    return sim, dict(log_mu=g_mu, log_k=g_k, mu=mu, lam=lam, K=K, omega=omega)
