@@ -266,6 +266,72 @@ int xlbb_batched_prolong_add_norms(int dtype_fine, int dtype_coarse, const XlbbB
                                    double* parts, double* norms, void* stream);
 int xlbb_segment_sum(const double* parts, const int* begin_dev, int nseg, double* out, void* stream);
 
+/*
+ * Adjoints (transposed linear maps) for gradients of a misfit with respect to
+ * per-cell material fields.  No counterpart in the reference (which has no
+ * adjoint).  Each call takes the adjoint of a forward kernel's output and
+ * produces the adjoints of its inputs; parameter gradients accumulate per cell
+ * in FP64 and need the forward call's inputs.
+ *
+ * xlbb_elast_sweep_adjoint: transpose of xlbb_elast_sweep with the same a, b,
+ * rules and material: lam_f = a lam_out + lam_g (written), lam_resid -= lam_g
+ * (if not NULL), lam_force = adjoint of the total force force + fext
+ * (2 planes, written, if not NULL), g_lam / g_mu += d/d lambda, d/d mu of the
+ * collision at every cell (if not NULL; need f_in, resid, force, fext of the
+ * forward call).
+ */
+typedef struct {
+    const void* lam_out;     /* adjoint of the sweep's output (8 planes) */
+    void* lam_f;             /* adjoint of f_in (8 planes, written) */
+    void* lam_resid;         /* adjoint of resid (8 planes, accumulated) or NULL */
+    void* lam_force;         /* adjoint of the total force (2 planes, written) or NULL */
+    double* g_lam;           /* per-cell gradient accumulators (FP64) or NULL */
+    double* g_mu;
+    const void* f_in;        /* forward inputs (parameter gradients only) */
+    const void* resid;
+    const void* force;
+    int use_force;
+    const void* fext;
+    double a, b;
+    XlbbRules pc, ps;
+} XlbbElastSweepAdjoint;
+
+int xlbb_elast_sweep_adjoint(int dtype, const XlbbGrid* g, const XlbbElastMaterial* mat,
+                             const XlbbElastSweepAdjoint* s, void* stream);
+
+/* Transpose of xlbb_darcy_sweep: lam_f (written), lam_source = adjoint of the
+ * total source (1 plane, written, or NULL), g_omega += d/d omega per cell. */
+typedef struct {
+    const void* lam_out;
+    void* lam_f;
+    void* lam_source;
+    double* g_omega;
+    const void* f_in;
+    double omega;
+    const void* omega_field;
+    const void* source;
+    const void* ext_source;
+    XlbbRules pc, ps;
+} XlbbDarcySweepAdjoint;
+
+int xlbb_darcy_sweep_adjoint(int dtype, const XlbbGrid* g, const XlbbDarcySweepAdjoint* s, void* stream);
+
+/* lam_q += G^T lam_grad, G = xlbb_darcy_gradient with the same scale and rules. */
+int xlbb_darcy_gradient_adjoint(int dtype, const XlbbGrid* g, const void* lam_grad, double scale,
+                                const XlbbRules* rules, void* lam_q, void* stream);
+
+/* lam_f += adjoint of eta (without forces) and of the divergence moment;
+ * g_lam / g_mu += derivative of the divergence scale (need f). */
+int xlbb_elast_moments_adjoint(int dtype, const XlbbGrid* g, const XlbbElastMaterial* mat, const void* f,
+                               const void* lam_eta, const void* lam_div, double div_scale, void* lam_f,
+                               double* g_lam, double* g_mu, void* stream);
+
+/* lam_f += adjoint of rho (without sources) and of grad = -3 omega sum c f;
+ * g_omega += d/d omega (needs f). */
+int xlbb_darcy_moments_adjoint(int dtype, const XlbbGrid* g, const void* f, double omega,
+                               const void* omega_field, const void* lam_rho, const void* lam_grad, void* lam_f,
+                               double* g_omega, void* stream);
+
 /* Deterministic FP64 sum of n partials (fixed order) into *out. */
 int xlbb_reduce_sum(const double* partials, int n, double* out, void* stream);
 

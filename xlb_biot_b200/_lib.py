@@ -68,6 +68,21 @@ class BatchTransfer(ctypes.Structure):
                 ("plane_f", ctypes.c_longlong), ("plane_c", ctypes.c_longlong)]
 
 
+class ElastSweepAdjoint(ctypes.Structure):
+    _fields_ = [("lam_out", ctypes.c_void_p), ("lam_f", ctypes.c_void_p), ("lam_resid", ctypes.c_void_p),
+                ("lam_force", ctypes.c_void_p), ("g_lam", ctypes.c_void_p), ("g_mu", ctypes.c_void_p),
+                ("f_in", ctypes.c_void_p), ("resid", ctypes.c_void_p), ("force", ctypes.c_void_p),
+                ("use_force", ctypes.c_int), ("fext", ctypes.c_void_p), ("a", ctypes.c_double),
+                ("b", ctypes.c_double), ("pc", Rules), ("ps", Rules)]
+
+
+class DarcySweepAdjoint(ctypes.Structure):
+    _fields_ = [("lam_out", ctypes.c_void_p), ("lam_f", ctypes.c_void_p), ("lam_source", ctypes.c_void_p),
+                ("g_omega", ctypes.c_void_p), ("f_in", ctypes.c_void_p), ("omega", ctypes.c_double),
+                ("omega_field", ctypes.c_void_p), ("source", ctypes.c_void_p), ("ext_source", ctypes.c_void_p),
+                ("pc", Rules), ("ps", Rules)]
+
+
 P = ctypes.c_void_p
 I = ctypes.c_int
 D = ctypes.c_double
@@ -98,6 +113,11 @@ SIGNATURES = {
     "xlbb_batched_prolong_add": (I, [I, I, P, I, P]),
     "xlbb_batched_prolong_add_norms": (I, [I, I, P, I, P, P, P]),
     "xlbb_segment_sum": (I, [P, P, I, P, P]),
+    "xlbb_elast_sweep_adjoint": (I, [I, PG, ctypes.POINTER(ElastMaterial), ctypes.POINTER(ElastSweepAdjoint), P]),
+    "xlbb_darcy_sweep_adjoint": (I, [I, PG, ctypes.POINTER(DarcySweepAdjoint), P]),
+    "xlbb_darcy_gradient_adjoint": (I, [I, PG, P, D, ctypes.POINTER(Rules), P, P]),
+    "xlbb_elast_moments_adjoint": (I, [I, PG, ctypes.POINTER(ElastMaterial), P, P, P, D, P, P, P, P]),
+    "xlbb_darcy_moments_adjoint": (I, [I, PG, P, D, P, P, P, P, P, P]),
     "xlbb_last_error": (ctypes.c_char_p, []),
     "xlbb_version": (I, []),
 }

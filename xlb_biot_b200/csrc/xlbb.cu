@@ -1293,3 +1293,5 @@ int xlbb_segment_sum(const double* parts, const int* begin_dev, int nseg, double
 }
 
 }  // extern "C"
+
+#include "xlbb_adjoint.cuh"
