@@ -137,10 +137,11 @@ __global__ void elast_sweep_adjoint_kernel(const ElastAdjArgs<T> p) {
 #pragma unroll
         for (int i = 0; i < 8; ++i) p.lam_resid[o + i * P] = p.lam_resid[o + i * P] - lg[i];
     }
-    const bool hasF = p.force != nullptr || p.fext != nullptr;
+    // the collision with F absent is the same map as with F = 0: the adjoint
+    // of the force is defined either way
     if (p.lam_force) {
-        p.lam_force[o] = hasF ? lM0 + lM5 / T(6) : T(0);
-        p.lam_force[o + P] = hasF ? lM1 + lM6 / T(6) : T(0);
+        p.lam_force[o] = lM0 + lM5 / T(6);
+        p.lam_force[o + P] = lM1 + lM6 / T(6);
     }
     if (p.g_mu) {
         // moments of the forward sweep's pre-collision input g = f - resid
@@ -219,8 +220,7 @@ __global__ void darcy_sweep_adjoint_kernel(const DarcyAdjArgs<T> p) {
     for (int i = 0; i < 9; ++i) W += w9<T>(i) * lp[i];
 #pragma unroll
     for (int i = 0; i < 9; ++i) p.lam_f[o + i * P] = (T(1) - om) * lp[i] + om * W + lge[i];
-    const bool hasS = p.source != nullptr || p.ext != nullptr;
-    if (p.lam_source) p.lam_source[o] = hasS ? W : T(0);
+    if (p.lam_source) p.lam_source[o] = W;   // d o_i / d S = w_i (also at S = 0)
     if (p.g_omega) {
         double sf = 0.0, lf = 0.0;
 #pragma unroll
