@@ -470,6 +470,99 @@ def run_c4(args):
     return 0
 
 
+def run_c5(args):
+    """Adjoint of heterogeneous Terzaghi-type consolidation: 512 x 256 cells
+    (arrays 512 x 258 with the boundary rows), 200 Biot steps, each with 4
+    five-level V-cycles (4 smoothing sweeps per level), checkpoints every 16
+    steps; per-cell log-shear-modulus and log-permeability fields (seeded
+    Gaussian random fields, correlation length 24 cells, sigma 0.5); misfit of
+    the last step's displacement and pressure against a forward run with
+    perturbed fields.  Gradients through ``ConsolidationMisfit`` (hand-written
+    adjoint kernels, CUDA graphs for the forward step, the taping step and
+    the adjoint step).  Reports backward / forward time, central finite
+    differences along random directions (FP64), FP32 vs FP64 gradients."""
+    import numpy as np
+    import torch
+    import xlb_biot_b200.api as G
+    from xlb_biot_b200.biot_adjoint import BiotAdjointModel, ConsolidationMisfit, consolidation_parameters
+    from xlb_biot_b200.workloads import gaussian_random_field, terzaghi_heterogeneous
+    steps, ndir = args.adjoint_steps, args.fd_directions
+    dev = torch.device("cuda")
+    nx, ny = 512, 258
+
+    def build(prec, log_mu=None, log_k=None):
+        sim, mat = terzaghi_heterogeneous(G, precision=prec, log_mu=log_mu, log_k=log_k)
+        return BiotAdjointModel(sim, steps, checkpoint_every=16, graphs=True), mat
+
+    # observations: the same problem with perturbed material fields
+    base_mu = gaussian_random_field(nx, ny, 24.0, 0.5, 0)
+    base_k = gaussian_random_field(nx, ny, 24.0, 0.5, 1)
+    pert_mu = base_mu + gaussian_random_field(nx, ny, 24.0, 0.1, 11)
+    pert_k = base_k + gaussian_random_field(nx, ny, 24.0, 0.1, 12)
+    mobs, _ = build("f64/f64", pert_mu, pert_k)
+    mobs.forward()
+    obs = (mobs.eta.double().clone(), mobs.p.double().clone())
+    del mobs
+
+    def grad(model):
+        model.set_observations(*obs)
+        lm = torch.as_tensor(base_mu, dtype=torch.float64, device=dev).requires_grad_()
+        lk = torch.as_tensor(base_k, dtype=torch.float64, device=dev).requires_grad_()
+        (J, t_f) = _timed(lambda: ConsolidationMisfit.apply(*consolidation_parameters(lm, lk), model))
+        (_, t_b) = _timed(lambda: J.backward())
+        return float(J.detach()), lm.grad.double(), lk.grad.double(), t_f, t_b
+
+    out = {}
+    for prec in ("f64/f64", "f32/f32"):
+        model, _ = build(prec)
+        grad(model)                                   # graph capture + warm-up
+        J, gm, gk, t_f, t_b = grad(model)
+        out[prec] = dict(J=J, gm=gm, gk=gk, forward_s=t_f, backward_s=t_b, model=model)
+    # central differences along random directions (FP64, the same graphs)
+    m64 = out["f64/f64"]["model"]
+    rng = np.random.default_rng(3)
+    errs = []
+    lm0 = torch.as_tensor(base_mu, dtype=torch.float64, device=dev)
+    lk0 = torch.as_tensor(base_k, dtype=torch.float64, device=dev)
+    t0 = time.time()
+    for _ in range(ndir):
+        dm = torch.as_tensor(rng.standard_normal((nx, ny)), device=dev)
+        dk = torch.as_tensor(rng.standard_normal((nx, ny)), device=dev)
+        eps = 1e-5
+        vals = []
+        for sgn in (1.0, -1.0):
+            m64.set_parameters(*consolidation_parameters(lm0 + sgn * eps * dm, lk0 + sgn * eps * dk))
+            vals.append(m64.forward())
+        fd = (vals[0] - vals[1]) / (2 * eps)
+        ad = float((out["f64/f64"]["gm"] * dm).sum() + (out["f64/f64"]["gk"] * dk).sum())
+        errs.append(abs(fd - ad) / abs(fd))
+    t_fd = time.time() - t0
+    errs = np.asarray(errs)
+
+    def rel(a, b):
+        return float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b))
+    r32, r64 = out["f32/f32"], out["f64/f64"]
+    levels, k, cyc = 5, 4, 4
+    lus = steps * cyc * sum((2 * k + (1 if l < levels - 1 else 0)) * (nx >> l) * ((ny - 2) // 2 ** l + 2)
+                            for l in range(levels))
+    line = {"workload": "c5_adjoint_consolidation_512x256_200steps", "metric": "adjoint/forward time",
+            "value": r32["backward_s"] / r32["forward_s"], "unit": "x", "higher_is_better": False,
+            "fp32": {"forward_s": r32["forward_s"], "backward_s": r32["backward_s"],
+                     "forward_glups": lus / r32["forward_s"] / 1e9},
+            "fp64": {"forward_s": r64["forward_s"], "backward_s": r64["backward_s"],
+                     "ratio": r64["backward_s"] / r64["forward_s"]},
+            "backward_includes": "recomputation of every 16-step segment with tapes (checkpoints every 16 steps)",
+            "fd_check_fp64": {"directions": ndir, "eps": 1e-5, "max_rel_err": float(errs.max()),
+                              "median_rel_err": float(np.median(errs)), "seconds": t_fd},
+            "fp32_vs_fp64_gradient_rel_err": {"log_mu": rel(r32["gm"], r64["gm"]),
+                                              "log_k": rel(r32["gk"], r64["gk"])},
+            "J": {"fp64": r64["J"], "fp32": r32["J"]},
+            "steps": steps, "cycles_per_step": cyc, "levels": levels, "k_smooth": k,
+            "peak_memory_gb": torch.cuda.max_memory_allocated() / 1e9}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -479,8 +572,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--launch-shape", default="",
                     help="tx,depth,ctas_per_sm,min_rows,pipeline of the Darcy sweep (skips the autotuner)")
-    ap.add_argument("--workload", choices=["darcy", "c1", "c3", "c4"], default="darcy",
-                    help="darcy: the headline line; c1/c3/c4: the other configurations (one JSON line each)")
+    ap.add_argument("--adjoint-steps", type=int, default=200)
+    ap.add_argument("--fd-directions", type=int, default=32)
+    ap.add_argument("--workload", choices=["darcy", "c1", "c3", "c4", "c5"], default="darcy",
+                    help="darcy: the headline line; c1/c3/c4/c5: the other configurations (one JSON line each)")
     ap.add_argument("--biot-steps", type=int, default=100)
     ap.add_argument("--instances", type=int, default=512)
     args = ap.parse_args()
@@ -494,6 +589,8 @@ def main():
         return run_c3(args)
     if args.workload == "c4":
         return run_c4(args)
+    if args.workload == "c5":
+        return run_c5(args)
     return run_ours(args)
 
 

@@ -32,7 +32,7 @@ from .elasticity import material_hierarchy
 class BiotAdjointModel:
     """Forward / adjoint driver of ``steps`` coupled Biot steps of ``sim``."""
 
-    def __init__(self, sim, steps, checkpoint_every=16):
+    def __init__(self, sim, steps, checkpoint_every=16, graphs=False):
         if sim.useDynamicForce or sim.useDynamicSource:
             raise ValueError("per-step force / source hooks are not supported by the adjoint")
         if sim.elasticityTol is not None or sim.alternative_gradient:
@@ -49,6 +49,12 @@ class BiotAdjointModel:
         self.g_omega = f64_plane(self.da._layout)
         self.eta_obs = self.p_obs = None
         self.timing = {}
+        # ``graphs``: the plain step, and per checkpoint slot the taping step and
+        # its adjoint, run as CUDA graphs (captured on first use) over static
+        # state buffers; results are identical to the eager path.
+        self.graphs = bool(graphs)
+        self._fwd_graph = None
+        self._bwd_graphs = None
 
     # ------------------------------------------------------------------ parameters
     def set_parameters(self, lam0, mu0, omega):
@@ -121,17 +127,87 @@ class BiotAdjointModel:
             tape.update(fe=fe, fd=fd, force=force, cycles=cycles, f=f, diff=diff, source=source)
         return f, fd_new, dtd_new, eta, pressure
 
+    # ------------------------------------------------------------------ CUDA graphs
+    def _state_buffers(self):
+        return self.el._L().empty(8), self.da._layout.empty(9), self.da._layout.empty(1)
+
+    @staticmethod
+    def _warm(fn):
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):
+            fn()
+        torch.cuda.current_stream().wait_stream(side)
+
+    @staticmethod
+    def _load(bufs, vals):
+        for b, v in zip(bufs, vals):
+            b.copy_(v)
+
+    def _build_forward_graph(self):
+        S = self._state_buffers()
+        self._load(S, self.sim.init_state())
+        self._warm(lambda: self.step(*S))
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            out = self.step(*S)
+            self._load(S, out[:3])
+        self._fwd_graph = (g, S, out[3], out[4])
+
+    def _build_backward_graphs(self):
+        el, da = self.el, self.da
+        n = min(self.every, self.steps)
+        ins = [self._state_buffers() for _ in range(n + 1)]
+        lam = (el._L().zeros(8), da._layout.zeros(9), da._layout.zeros(1))
+        src = (el._L().zeros(2), da._layout.zeros(1))
+        for b in ins:
+            self._load(b, self.sim.init_state())
+
+        def warm():
+            tp = {}
+            self.step(*ins[0], tape=tp)
+            self.step_adjoint(tp, *lam, *src)
+        self._warm(warm)
+        self.grads.zero_()
+        self.g_omega.zero_()
+        tapes, steps_g, adj_g = [], [], []
+        for j in range(n):
+            g = torch.cuda.CUDAGraph()
+            tp = {}
+            with torch.cuda.graph(g):
+                out = self.step(*ins[j], tape=tp)
+                self._load(ins[j + 1], out[:3])
+            tapes.append(tp)
+            steps_g.append(g)
+            a = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(a):
+                out = self.step_adjoint(tp, *lam, *src)
+                self._load(lam, out)
+            adj_g.append(a)
+        self._bwd_graphs = dict(ins=ins, lam=lam, src=src, tapes=tapes, steps=steps_g, adj=adj_g)
+
     def forward(self):
         """Runs the time loop from ``sim.init_state()``; keeps checkpoints;
         returns J (float) when observations are set, else None."""
+        if self.graphs and self._fwd_graph is None:
+            self._build_forward_graph()
         t0 = time.time()
-        fe, fd, dtd = self.sim.init_state()
         self.checkpoints = {}
         eta = p = None
-        for k in range(self.steps):
-            if k % self.every == 0:
-                self.checkpoints[k] = (fe.clone(), fd.clone(), dtd.clone())
-            fe, fd, dtd, eta, p = self.step(fe, fd, dtd)
+        if self.graphs:
+            g, S, eta_s, p_s = self._fwd_graph
+            self._load(S, self.sim.init_state())
+            for k in range(self.steps):
+                if k % self.every == 0:
+                    self.checkpoints[k] = tuple(t.clone() for t in S)
+                g.replay()
+            eta, p = eta_s, p_s
+        else:
+            fe, fd, dtd = self.sim.init_state()
+            for k in range(self.steps):
+                if k % self.every == 0:
+                    self.checkpoints[k] = (fe.clone(), fd.clone(), dtd.clone())
+                fe, fd, dtd, eta, p = self.step(fe, fd, dtd)
         self.eta, self.p = eta, p
         J = None
         if self.eta_obs is not None:
@@ -217,6 +293,10 @@ class BiotAdjointModel:
     def backward(self):
         """Adjoint of the last ``forward``: returns (per-level d/d lambda,
         per-level d/d mu, d/d omega) as FP64 (nx_l, ny_l) tensors."""
+        if self.graphs:
+            if self._bwd_graphs is None:
+                self._build_backward_graphs()
+            return self._backward_graphs()
         t0 = time.time()
         el, da = self.el, self.da
         self.grads.zero_()
@@ -239,6 +319,34 @@ class BiotAdjointModel:
                 lam_fe, lam_fd, lam_dtd = self.step_adjoint(tapes[k - s], lam_fe, lam_fd, lam_dtd,
                                                             lam_eta if last else None, lam_p if last else None)
                 tapes[k - s] = None
+        torch.cuda.synchronize()
+        self.timing["backward_s"] = time.time() - t0
+        g_lam = [t[..., 0].clone() for t in self.grads.lam]
+        g_mu = [t[..., 0].clone() for t in self.grads.mu]
+        return g_lam, g_mu, self.g_omega[..., 0].clone()
+
+
+    def _backward_graphs(self):
+        t0 = time.time()
+        B = self._bwd_graphs
+        self.grads.zero_()
+        self.g_omega.zero_()
+        for t in B["lam"] + B["src"]:
+            t.zero_()
+        for s in reversed(sorted(self.checkpoints)):
+            n = min(s + self.every, self.steps) - s
+            self._load(B["ins"][0], self.checkpoints[s])
+            for j in range(n):
+                B["steps"][j].replay()
+            for j in range(n - 1, -1, -1):
+                last = s + j == self.steps - 1
+                if last:
+                    B["src"][0].copy_(self.eta.double() - self.eta_obs.double())
+                    B["src"][1].copy_(self.p.double() - self.p_obs.double())
+                B["adj"][j].replay()
+                if last:
+                    for t in B["src"]:
+                        t.zero_()
         torch.cuda.synchronize()
         self.timing["backward_s"] = time.time() - t0
         g_lam = [t[..., 0].clone() for t in self.grads.lam]
@@ -272,11 +380,16 @@ class ConsolidationMisfit(torch.autograd.Function):
         return (gJ * dl).to(lam0.dtype), (gJ * dm).to(mu0.dtype), (gJ * g_om).to(omega.dtype), None
 
 
-def consolidation_parameters(log_mu, log_k, mu0=0.04, nu=0.25, K0=0.1):
+def consolidation_parameters(log_mu, log_k, mu0=None, lam0=None, K0=None, nu=None):
     """Level-0 (lambda, mu, omega) of ``workloads.terzaghi_heterogeneous`` from
     the log-shear-modulus and log-permeability fields (torch, differentiable):
-    mu = mu0 exp(log_mu), lambda = 2 mu nu / (1 - nu), omega = 1 / (3 K0 exp(log_k) + 1/2)."""
+    mu = mu0 exp(log_mu), lambda = lam0 (or 2 mu nu / (1 - nu) if ``nu`` is
+    given), omega = 1 / (3 K0 exp(log_k) + 1/2).  Defaults as the workload's."""
+    from .workloads import TERZAGHI_K, TERZAGHI_LAM, TERZAGHI_MU
+    mu0 = TERZAGHI_MU if mu0 is None else mu0
+    lam0 = TERZAGHI_LAM if lam0 is None else lam0
+    K0 = TERZAGHI_K if K0 is None else K0
     mu = mu0 * torch.exp(log_mu)
-    lam = mu * (2.0 * nu / (1.0 - nu))
+    lam = mu * (2.0 * nu / (1.0 - nu)) if nu is not None else torch.full_like(mu, lam0)
     omega = 1.0 / (3.0 * K0 * torch.exp(log_k) + 0.5)
     return lam, mu, omega

@@ -193,9 +193,19 @@ def darcy_lognormal(m, n=1024, ell=16.0, sigma=1.0, seed=0, precision="f32/f32")
     return solver, k
 
 
-def terzaghi_heterogeneous(m, nx=512, ny=258, levels=5, mu0=0.04, nu=0.25, K0=0.1, sigma=0.5, ell=24.0,
-                           load=1e-3, cycles=4, k_smooth=4, seed=0, precision="f32/f32", darcy_precision=None,
-                           coarsest_precision=None, residual_precision=None, log_mu=None, log_k=None):
+# Non-dimensional material of the reference's 2D consolidation example
+# (examples/poroelasticity/2D.py: E = 1e5, nu = 0.9 plane-stress Lame
+# parameters, c0 = 1e-6, kappa = 1e-9, L = 100, T = 2e6, load 1e4), which in
+# lattice units does not depend on nx except through epsilon and the load.
+TERZAGHI_LAM = 0.1 * 0.9 / (1 - 0.9 ** 2)
+TERZAGHI_MU = 0.5 * 0.1 / (1 + 0.9)
+TERZAGHI_K = 0.2
+
+
+def terzaghi_heterogeneous(m, nx=512, ny=258, levels=5, mu0=TERZAGHI_MU, lam0=TERZAGHI_LAM, nu=None,
+                           K0=TERZAGHI_K, sigma=0.5, ell=24.0, load=None, epsilon=None, cycles=4, k_smooth=4,
+                           seed=0, precision="f32/f32", darcy_precision=None, coarsest_precision=None,
+                           residual_precision=None, log_mu=None, log_k=None):
     """2D Terzaghi-type consolidation with heterogeneous material.
 
     A layer of ``ny - 2`` cell rows (plus one boundary row at the bottom and at
@@ -204,17 +214,21 @@ def terzaghi_heterogeneous(m, nx=512, ny=258, levels=5, mu0=0.04, nu=0.25, K0=0.
     traction (0, -load * (1 - cos(2 pi (x + 1/2) / nx)) / 2) (anti-bounce-back);
     Darcy: no flux at the bottom (bounce-back), drained top p = 0
     (anti-bounce-back); zero initial displacement and pressure.  Per-cell
-    shear modulus mu = mu0 exp(g_mu), lambda = 2 mu nu / (1 - nu) (fixed
-    Poisson ratio), permeability K = K0 exp(g_K), omega = 1 / (3 K + 1/2);
-    g_mu, g_K seeded Gaussian random fields (correlation length ``ell``,
-    standard deviation ``sigma``) unless given (``log_mu``, ``log_k``: the
-    fields g).  ``levels``-level V-cycles (MG_BCs bottom/top, ``k_smooth``
-    smoothing sweeps), ``cycles`` V-cycles per time step, centred coupling.
+    shear modulus mu = mu0 exp(g_mu) with lambda = lam0 (or, if ``nu`` is
+    given, lambda = 2 mu nu / (1 - nu) per cell), permeability
+    K = K0 exp(g_K), omega = 1 / (3 K + 1/2); g_mu, g_K seeded Gaussian random
+    fields (correlation length ``ell``, standard deviation ``sigma``) unless
+    given (``log_mu``, ``log_k``: the fields g).  Defaults: the reference's 2D
+    example in lattice units (epsilon = 100 / nx, load = 1 / nx).
+    ``levels``-level V-cycles (MG_BCs bottom/top, ``k_smooth`` smoothing
+    sweeps), ``cycles`` V-cycles per time step, centred coupling.
     Returns (sim, material) with material = dict(log_mu, log_k, mu, lam, K, omega)."""
+    load = 1.0 / nx if load is None else load
+    epsilon = 100.0 / nx if epsilon is None else epsilon
     g_mu = gaussian_random_field(nx, ny, ell, sigma, seed) if log_mu is None else np.asarray(log_mu, np.float64)
     g_k = gaussian_random_field(nx, ny, ell, sigma, seed + 1) if log_k is None else np.asarray(log_k, np.float64)
     mu = mu0 * np.exp(g_mu)
-    lam = mu * (2 * nu / (1 - nu))
+    lam = mu * (2 * nu / (1 - nu)) if nu is not None else np.full_like(mu, lam0)
     K = K0 * np.exp(g_k)
     omega = 1.0 / (3.0 * K + 0.5)
     x = np.arange(nx)
@@ -254,7 +268,8 @@ def terzaghi_heterogeneous(m, nx=512, ny=258, levels=5, mu0=0.04, nu=0.25, K0=0.
 
     kw = dict(lattice_elasticity=m.LatticeD2Q8(precision), lattice_darcy=m.LatticeD2Q9(darcy_precision or precision),
               **{"lambda": float(np.mean(lam))}, mu=float(np.mean(mu)), lambda_field=lam, mu_field=mu,
-              omega=float(np.mean(omega)), omega_field=omega[..., None], alpha=1.0, nx=nx, ny=ny, nz=0,
+              omega=float(np.mean(omega)), omega_field=omega[..., None], alpha=1.0, epsilon=float(epsilon),
+              nx=nx, ny=ny, nz=0,
               precision=precision, elasticity_MG_levels=levels, elasticity_steps=cycles,
               MG_BCs={"bottom": True, "top": True}, MG_n_smoothing=k_smooth, coupling_method="centered",
               print_info_rate=0)
