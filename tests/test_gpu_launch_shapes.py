@@ -1,6 +1,7 @@
-"""Every launch shape of the fused sweeps (register-prefetch and bulk-copy
-pipelines, 128/256 columns, each prefetch depth) gives bitwise the same
-populations, and those match the oracle; the bounded waits report no timeout."""
+"""Every launch shape of the fused sweeps (register-prefetch, bulk-copy,
+warp and collide-and-push pipelines, 128/256 columns, each prefetch depth)
+gives bitwise the same populations, and those match the oracle; the bounded
+waits report no timeout."""
 import numpy as np
 import pytest
 import torch
@@ -64,8 +65,9 @@ def test_darcy_all_shapes_identical(G, shapes, prec):
         autotune.set_config(autotune.DARCY, **saved)
 
 
+@pytest.mark.parametrize("kind", ["dirichlet", "neumann"])
 @pytest.mark.parametrize("prec", ["f32/f32", "f64/f64"])
-def test_elasticity_multigrid_all_shapes_identical(G, shapes, prec):
+def test_elasticity_multigrid_all_shapes_identical(G, shapes, prec, kind):
     """V-cycles exercise the plain, damped (a, b) and residual (resid) sweeps."""
     from xlb_biot_b200 import autotune
     saved = autotune.get_config(autotune.ELASTICITY)
@@ -79,7 +81,7 @@ def test_elasticity_multigrid_all_shapes_identical(G, shapes, prec):
             if prec == "f64/f64" and (c["tx"] > 128 or c["depth"] > 4):
                 continue
             autotune.set_config(autotune.ELASTICITY, **c)
-            s = make_walled_elasticity(G, "dirichlet")(lattice=G.LatticeD2Q8(prec), **kw)
+            s = make_walled_elasticity(G, kind)(lattice=G.LatticeD2Q8(prec), **kw)
             f, r = s.step(f0, 0)
             f, r = s.step(f, 1)
             results.append((c, f.cpu().numpy(), float(r)))
@@ -87,7 +89,7 @@ def test_elasticity_multigrid_all_shapes_identical(G, shapes, prec):
             assert np.array_equal(f, results[0][1]), c
             # the FP64 norm sums one partial per CTA: the order depends on the grid
             assert abs(r - results[0][2]) <= 1e-13 * abs(results[0][2]), c
-        so = make_walled_elasticity(O, "dirichlet")(lattice=O.LatticeD2Q8(prec), **kw)
+        so = make_walled_elasticity(O, kind)(lattice=O.LatticeD2Q8(prec), **kw)
         fo, ro = so.step(f0.astype(so.precisionPolicy.compute_dtype), 0)
         fo, ro = so.step(fo, 1)
         tol = 1e-12 if prec == "f64/f64" else 1e-5

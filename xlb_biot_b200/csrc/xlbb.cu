@@ -32,8 +32,10 @@ static int check_launch(const char* what) {
     return XLBB_OK;
 }
 
+// Offsets inside one plane are 32-bit in the kernels: a plane holds < 2^31 elements.
 static bool grid_ok(const XlbbGrid* g) {
-    return g && g->nx > 0 && g->ny > 0 && g->pitch >= g->nx && g->plane >= (long long)g->pitch * g->ny;
+    return g && g->nx > 0 && g->ny > 0 && g->pitch >= g->nx && g->plane >= (long long)g->pitch * g->ny &&
+           g->plane < (1LL << 31);
 }
 
 static int g_num_sms = 0;
@@ -75,8 +77,12 @@ static constexpr int WARP_COLS = 30;   // output columns of one warp of sweep_wa
 static bool cfg_ok(const XlbbSweepConfig& c) {
     const bool depth_ok = c.pipeline == 1 ? (c.depth == 2 || c.depth == 4 || c.depth == 6) : (c.depth == 1 || c.depth == 2);
     return (c.tx == 128 || c.tx == 256) && depth_ok && c.ctas_per_sm >= 1 && c.ctas_per_sm <= 32 &&
-           c.min_rows >= 1 && c.pipeline >= 0 && c.pipeline <= 2;
+           c.min_rows >= 1 && c.pipeline >= 0 && c.pipeline <= 3;
 }
+
+// Pipeline 3 (collide-and-push) runs sweeps without fused reductions; the
+// others run on this row-marching shape.
+static XlbbSweepConfig push_fallback(bool f32) { return XlbbSweepConfig{f32 ? 256 : 128, 1, 3, 8, 0}; }
 
 // ---------------------------------------------------------------------------
 // D2Q8 elasticity (src/elasticity.py:805-848 transfer matrices, :959-1000
@@ -158,7 +164,24 @@ struct ElastPhys {
         static constexpr int PMAX = 20;
         const S_* planes[PMAX];   // input planes in from_smem order (bulk-copy kernel)
         int np;
+        // Plane pointers in fixed slots (f 0-7, resid 8-15, force 16-17, fext
+        // 18-19; NULL when absent), so a kernel addresses plane i of a cell as
+        // ip[i] + (32-bit cell offset) instead of base + i * plane.
+        const S_* ip[20];
+        S_* op[8];
     };
+    __host__ __device__ static void fill_ptrs(Args& a) {
+        const long long P = a.geom.plane;
+        for (int i = 0; i < 8; ++i) {
+            a.ip[i] = a.f_in + i * P;
+            a.ip[8 + i] = a.resid ? a.resid + i * P : nullptr;
+            a.op[i] = a.f_out + i * P;
+        }
+        a.ip[16] = a.force;
+        a.ip[17] = a.force ? a.force + P : nullptr;
+        a.ip[18] = a.fext;
+        a.ip[19] = a.fext ? a.fext + P : nullptr;
+    }
     struct In {
         T f[8];
         T r[RESID ? 8 : 1];
@@ -193,18 +216,17 @@ struct ElastPhys {
         in.F1 = F1;
     }
     __device__ static void load(const Args& p, int y, int x, In& in) {
-        const size_t o = (size_t)y * p.geom.pitch + x;
-        const long long P = p.geom.plane;
+        const int o = y * p.geom.pitch + x;
 #pragma unroll
-        for (int i = 0; i < 8; ++i) in.f[i] = T(__ldg(p.f_in + o + i * P));
+        for (int i = 0; i < 8; ++i) in.f[i] = T(__ldg(p.ip[i] + o));
         if (RESID) {
 #pragma unroll
-            for (int i = 0; i < 8; ++i) in.r[i] = T(__ldg(p.resid + o + i * P));
+            for (int i = 0; i < 8; ++i) in.r[i] = T(__ldg(p.ip[8 + i] + o));
         }
         T F0 = T(0), F1 = T(0);
-        if (p.force) { F0 = T(__ldg(p.force + o)); F1 = T(__ldg(p.force + o + P)); }
+        if (p.force) { F0 = T(__ldg(p.ip[16] + o)); F1 = T(__ldg(p.ip[17] + o)); }
         if (p.fext) {
-            const T e0 = T(__ldg(p.fext + o)), e1 = T(__ldg(p.fext + o + P));
+            const T e0 = T(__ldg(p.ip[18] + o)), e1 = T(__ldg(p.ip[19] + o));
             if (p.force) { F0 = F0 + e0; F1 = F1 + e1; } else { F0 = e0; F1 = e1; }
         }
         in.F0 = F0;
@@ -214,21 +236,28 @@ struct ElastPhys {
 #pragma unroll
         for (int i = 0; i < 8; ++i) g[i] = RESID ? in.f[i] - in.r[i] : in.f[i];
     }
+    // Output population i of the cell at offset o from its streamed-in value s
+    // (the store stage's algebra, for the collide-and-push sweep).
+    __device__ static void put(const Args& p, int i, int o, T s) {
+        T v = s;
+        if (p.mix) v = p.a * T(__ldg(p.ip[i] + o)) + p.b * s;
+        p.op[i][o] = S_(v);
+    }
+    static bool push_ok(const Args& a) { return a.sumsq == nullptr && a.div_out == nullptr; }
     __device__ static T f_in(const In& in, int i) { return in.f[i]; }
     __device__ static void collide(const Args& p, int y, int x, const In& in, T (&o)[8]) {
         T g[8];
         fin(in, g);
         T cs = p.mat.cs, cd = p.mat.cd, h = p.mat.h, n = p.mat.n;
         if (p.mat.mu_f) {
-            const size_t c = (size_t)y * p.geom.pitch + x;
+            const int c = y * p.geom.pitch + x;
             elast_rates<T>(T(__ldg(p.mat.lam_f + c)), T(__ldg(p.mat.mu_f + c)), cs, cd, h, n);
         }
         elast_collide<T>(g, p.force != nullptr || p.fext != nullptr, in.F0, in.F1, cs, cd, h, n, o);
     }
     template <bool PREV>
     __device__ static double store(const Args& p, int y, int x, T (&S)[8], const T* fprev) {
-        const size_t o = (size_t)y * p.geom.pitch + x;
-        const long long P = p.geom.plane;
+        const int o = y * p.geom.pitch + x;
         double acc = 0.0;
         T m2 = T(0);
 #pragma unroll
@@ -238,7 +267,7 @@ struct ElastPhys {
                 if (p.mix) v = p.a * fprev[i] + p.b * S[i];
             }
             const S_ sv = S_(v);
-            p.f_out[o + i * P] = sv;
+            p.op[i][o] = sv;
             double d = (double)sv;
             if constexpr (PREV) {
                 if (p.sumsq_diff) d -= (double)S_(fprev[i]);
@@ -274,7 +303,19 @@ struct DarcyPhys {
         static constexpr int PMAX = 12;
         const T* planes[PMAX];   // input planes in from_smem order (bulk-copy kernel)
         int np;
+        // Plane pointers in fixed slots (f 0-8, omega 9, source 10, ext 11)
+        const T* ip[12];
+        T* op[9];
     };
+    __host__ __device__ static void fill_ptrs(Args& a) {
+        for (int i = 0; i < 9; ++i) {
+            a.ip[i] = a.f_in + i * a.geom.plane;
+            a.op[i] = a.f_out + i * a.geom.plane;
+        }
+        a.ip[9] = a.omega_f;
+        a.ip[10] = a.source;
+        a.ip[11] = a.ext;
+    }
     struct In {
         T f[9];
         T S;
@@ -301,20 +342,21 @@ struct DarcyPhys {
         in.S = S;
     }
     __device__ static void load(const Args& p, int y, int x, In& in) {
-        const size_t o = (size_t)y * p.geom.pitch + x;
-        const long long P = p.geom.plane;
+        const int o = y * p.geom.pitch + x;
 #pragma unroll
-        for (int i = 0; i < 9; ++i) in.f[i] = __ldg(p.f_in + o + i * P);
+        for (int i = 0; i < 9; ++i) in.f[i] = __ldg(p.ip[i] + o);
         T S = T(0);
-        if (p.source) S = __ldg(p.source + o);
-        if (p.ext) S = p.source ? S + __ldg(p.ext + o) : __ldg(p.ext + o);
+        if (p.source) S = __ldg(p.ip[10] + o);
+        if (p.ext) S = p.source ? S + __ldg(p.ip[11] + o) : __ldg(p.ip[11] + o);
         in.S = S;
-        in.om = p.omega_f ? __ldg(p.omega_f + o) : p.omega;
+        in.om = p.omega_f ? __ldg(p.ip[9] + o) : p.omega;
     }
     __device__ static void fin(const In& in, T (&g)[9]) {
 #pragma unroll
         for (int i = 0; i < 9; ++i) g[i] = in.f[i];
     }
+    __device__ static void put(const Args& p, int i, int o, T s) { p.op[i][o] = s; }
+    static bool push_ok(const Args& a) { return a.sumsq == nullptr; }
     __device__ static T f_in(const In& in, int i) { return in.f[i]; }
     __device__ static void collide(const Args& p, int, int, const In& in, T (&o)[9]) {
         const bool hasS = p.source != nullptr || p.ext != nullptr;
@@ -334,12 +376,11 @@ struct DarcyPhys {
     }
     template <bool PREV>
     __device__ static double store(const Args& p, int y, int x, T (&S)[9], const T* fprev) {
-        const size_t o = (size_t)y * p.geom.pitch + x;
-        const long long P = p.geom.plane;
+        const int o = y * p.geom.pitch + x;
         double acc = 0.0;
 #pragma unroll
         for (int i = 0; i < 9; ++i) {
-            p.f_out[o + i * P] = S[i];
+            p.op[i][o] = S[i];
             if constexpr (PREV) {
                 const double d = (double)S[i] - (double)fprev[i];
                 acc += d * d;
@@ -348,6 +389,8 @@ struct DarcyPhys {
         return acc;
     }
 };
+
+#include "xlbb_push.cuh"
 
 // Launch geometry of the sweeps: tx owned columns per CTA, strips of rows
 // chosen so that the grid holds about ctas_per_sm CTAs per SM (one wave),
@@ -412,6 +455,16 @@ static bool bulk_aligned(const typename Ph::Args& a) {
 template <class Ph, bool PREV>
 static void launch_sweep(XlbbSweepConfig c, const XlbbGrid* g, cudaStream_t st, typename Ph::Args& a) {
     constexpr bool F32 = sizeof(typename Ph::T) == 4;
+    Ph::fill_ptrs(a);
+    if (c.pipeline == 3) {
+        if (Ph::push_ok(a)) {
+            const int bs = c.tx;
+            push_kernel<Ph><<<dim3((g->nx + bs - 1) / bs, g->ny), bs, 0, st>>>(a);
+            if (a.ps.count > 0) push_fixup_kernel<Ph><<<(a.ps.count + 127) / 128, 128, 0, st>>>(a);
+            return;
+        }
+        c = push_fallback(F32);
+    }
     const dim3 grid = sweep_grid(g, c);
     if (c.pipeline == 2) {
         const WarpGrid wg = warp_grid(g, c);
@@ -450,7 +503,8 @@ static void launch_sweep(XlbbSweepConfig c, const XlbbGrid* g, cudaStream_t st, 
 // FP32 storage / FP64 arithmetic: the register-prefetch kernel at tx = 128.
 template <class Ph, bool PREV>
 static void launch_sweep_regs(const XlbbSweepConfig& c, const XlbbGrid* g, cudaStream_t st,
-                              const typename Ph::Args& a) {
+                              typename Ph::Args& a) {
+    Ph::fill_ptrs(a);
     const dim3 grid = sweep_grid(g, c);
     if (c.depth == 2) sweep_kernel<Ph, 128, 2, PREV><<<grid, 128 + 32, 0, st>>>(a);
     else sweep_kernel<Ph, 128, 1, PREV><<<grid, 128 + 32, 0, st>>>(a);
@@ -809,6 +863,7 @@ batched_elast_kernel(const BatchInst<T, S>* __restrict__ inst, const XlbbBatchTi
         p.mix = mix;
         p.sumsq_diff = sumsq_diff;
         p.np = 0;
+        Ph::fill_ptrs(p);
         const double acc = sweep_strip<Ph, TX, 1, PREV>(p, tl.x0, tl.ys, tl.ye, post);
         if (tile_sumsq != nullptr) {
             const double s = block_sum(acc, red);
@@ -917,14 +972,18 @@ const char* xlbb_last_error(void) { return g_last_error.c_str(); }
 int xlbb_elast_sweep_ctas(int dtype, const XlbbGrid* g) {
     if (!grid_ok(g) || (dtype != XLBB_F32 && dtype != XLBB_F64 && dtype != XLBB_F32_ACC64))
         return fail(XLBB_EBADARG, "xlbb_elast_sweep_ctas: bad argument");
-    const dim3 a = sweep_grid(g, effective_cfg(0, dtype));
+    XlbbSweepConfig c = effective_cfg(0, dtype);
+    if (c.pipeline == 3) c = push_fallback(dtype == XLBB_F32);
+    const dim3 a = sweep_grid(g, c);
     return (int)(a.x * a.y);
 }
 
 int xlbb_darcy_sweep_ctas(int dtype, const XlbbGrid* g) {
     if (!grid_ok(g) || (dtype != XLBB_F32 && dtype != XLBB_F64))
         return fail(XLBB_EBADARG, "xlbb_darcy_sweep_ctas: bad argument");
-    const dim3 a = sweep_grid(g, effective_cfg(1, dtype));
+    XlbbSweepConfig c = effective_cfg(1, dtype);
+    if (c.pipeline == 3) c = push_fallback(dtype == XLBB_F32);
+    const dim3 a = sweep_grid(g, c);
     return (int)(a.x * a.y);
 }
 

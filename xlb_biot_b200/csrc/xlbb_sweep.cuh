@@ -34,7 +34,7 @@ template <typename T, int Q>
 __device__ __forceinline__ RuleProbe load_probe(const RulesView<T, Q>& r, int y, int x) {
     RuleProbe p{0u, 0};
     if (r.count > 0) {
-        const size_t w = (size_t)y * r.words_per_row + (x >> 5);
+        const int w = y * r.words_per_row + (x >> 5);
         p.mask = __ldg(r.mask + w);
         p.base = __ldg(r.word_base + w);
     }
