@@ -324,7 +324,9 @@ def run_ours(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": traffic, "algorithmic_bytes_per_launch": N * N * BYTES_PER_LU_F32,
-                         "kernel": "xlbb::sweep_kernel<DarcyPhys<float>>", "kernel_ms": per_sweep_ms},
+                         "kernel": ("xlbb::push_kernel<DarcyPhys<float>>"
+                                    if tuned.get("pipeline") == 3 else "xlbb::sweep_kernel<DarcyPhys<float>>"),
+                         "kernel_ms": per_sweep_ms},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": "GLUPS", "h2d_bytes_per_step": host_f.numel() * host_f.element_size(),
                     "d2h_bytes_per_step": 8},

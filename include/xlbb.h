@@ -61,6 +61,12 @@ typedef struct {
     const uint32_t* mask;    /* ny*words_per_row words: bit (x%32) of word x/32 set on rule cells */
     const int* word_base;    /* rule index of the first rule cell of each mask word */
     int words_per_row;       /* >= ceil(nx/32) */
+    /* Post-streaming rules, for the collide-and-push sweep (may be NULL: that
+     * sweep then uses the row-marching kernel): one word per cell (index
+     * y*nx + x), bit d set when direction d pushed from this cell lands where a
+     * rule rebuilds it, bit 16 set on rule cells.  Only built when every
+     * "current value" code is +current with constant 0. */
+    const uint32_t* push;
 } XlbbRules;
 
 /*

@@ -143,3 +143,51 @@ def test_non_local_bc_is_rejected():
     bc.create_local_mask_and_normal_arrays(GB.grid_mask(6, 6, lat, None))
     with pytest.raises(NotImplementedError):
         compile_rules([bc], 6, 6, 8, torch.float64, "cpu", step="PostStreaming")
+
+
+@pytest.mark.parametrize("name,q,nx,ny,builder", _scenarios(), ids=[s[0] for s in _scenarios()])
+def test_push_words_reproduce_stream_then_rules(name, q, nx, ny, builder):
+    """The collide-and-push sweep's per-cell push words: pushing every
+    post-collision population except the flagged directions, then letting each
+    rule cell write the directions its post-streaming rules rebuild, writes every
+    output exactly once and equals streaming followed by the rules."""
+    glat = GL.LatticeD2Q8("f64/f64") if q == 8 else GL.LatticeD2Q9("f64/f64")
+    gpp = GB.PrecisionPolicy(np.float64, np.float64)
+    gbcs = _prep(builder(G, glat, {"nx": nx, "ny": ny, "nz": 0, "dim": 2, "lattice": glat}, gpp, nx, ny),
+                 nx, ny, glat, GB.grid_mask)
+    rules = compile_rules(gbcs, nx, ny, q, torch.float64, "cpu", step="PostStreaming")
+    if rules.count == 0:
+        return
+    keep = 2 * q + 1
+    if rules.push is None:       # a "current value" code transforms the streamed value: row-marching sweep
+        assert np.any(rules.code_np == keep + 1) or np.any((rules.code_np == keep) & (rules.cst_np != 0))
+        return
+    c = np.asarray(glat.c, dtype=np.int64)
+    rng = np.random.default_rng(5)
+    post = rng.standard_normal((nx, ny, q))
+    stream = np.stack([np.roll(post[..., i], (c[0, i], c[1, i]), axis=(0, 1)) for i in range(q)], -1)
+    cx, cy = rules.cells[:, 0], rules.cells[:, 1]
+    ref = stream.copy()
+    ref[cx, cy] = evaluate_rules(rules, stream[cx, cy], post[cx, cy])
+    words = rules.push.numpy().view(np.uint32).reshape(ny, nx).T
+    out = np.zeros_like(post)
+    count = np.zeros((nx, ny, q), dtype=np.int64)
+    for x in range(nx):
+        for y in range(ny):
+            for i in range(q):
+                if not (words[x, y] >> i) & 1:
+                    z = ((x + c[0, i]) % nx, (y + c[1, i]) % ny)
+                    out[z + (i,)] = post[x, y, i]
+                    count[z + (i,)] += 1
+    assert np.array_equal(((words >> 16) & 1).astype(bool)[cx, cy], np.ones(len(cx), bool))
+    assert int(((words >> 16) & 1).sum()) == rules.count
+    for r, (x, y) in enumerate(zip(cx, cy)):
+        for d in range(q):
+            code = int(rules.code_np[r, d])
+            if code != keep:
+                k = code if code < q else (code - q if code < 2 * q else 0)
+                base = post[x, y, k] if code < q else (-post[x, y, k] if code < 2 * q else 0.0)
+                out[x, y, d] = base + rules.cst_np[r, d]
+                count[x, y, d] += 1
+    assert np.all(count == 1)
+    np.testing.assert_allclose(out, ref, rtol=0, atol=1e-14)

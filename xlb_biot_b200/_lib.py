@@ -28,7 +28,7 @@ class Grid(ctypes.Structure):
 class Rules(ctypes.Structure):
     _fields_ = [("count", ctypes.c_int), ("row_ptr", ctypes.c_void_p), ("cell_x", ctypes.c_void_p),
                 ("code", ctypes.c_void_p), ("cst", ctypes.c_void_p), ("mask", ctypes.c_void_p),
-                ("word_base", ctypes.c_void_p), ("words_per_row", ctypes.c_int)]
+                ("word_base", ctypes.c_void_p), ("words_per_row", ctypes.c_int), ("push", ctypes.c_void_p)]
 
 
 class SweepConfig(ctypes.Structure):

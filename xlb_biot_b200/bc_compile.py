@@ -24,7 +24,7 @@ from .boundary_conditions import apply_in_order
 class CompiledRules:
     """Device-resident rule table of one grid and one phase."""
 
-    def __init__(self, q, ny, cells, code, cst, dtype, device, nx=None):
+    def __init__(self, q, ny, cells, code, cst, dtype, device, nx=None, push=False):
         self.q = q
         self.count = len(cells)
         self.nx = int(nx) if nx is not None else (int(cells[:, 0].max()) + 1 if len(cells) else 1)
@@ -55,13 +55,37 @@ class CompiledRules:
             self.word_base = torch.as_tensor(word_base, device=device)
         else:
             self.row_ptr = self.cell_x = self.code = self.cst = self.mask = self.word_base = None
+        self.push = self._push_words(ny, device) if push and self.count else None
+
+    def _push_words(self, ny, device):
+        """Per-cell word of the collide-and-push sweep for post-streaming rules:
+        bit d of cell x is set when x + c_d is a rule cell whose direction d is
+        rebuilt from that cell's own values (source / zero codes), bit 16 on
+        rule cells.  None when a "current value" code transforms the streamed
+        value (negated, or with a constant): that sweep cannot apply it."""
+        q, nx = self.q, self.nx
+        keep, neg_keep = 2 * q + 1, 2 * q + 2
+        code = self.code_np
+        if np.any(code == neg_keep) or np.any((code == keep) & (self.cst_np != 0)):
+            return None
+        from .lattice import LatticeD2Q8, LatticeD2Q9
+        c = np.asarray((LatticeD2Q8 if q == 8 else LatticeD2Q9)("f64/f64").c, dtype=np.int64)
+        zx, zy = self.cells[:, 0], self.cells[:, 1]
+        words = np.zeros(ny * nx, dtype=np.uint32)
+        np.bitwise_or.at(words, zy * nx + zx, np.uint32(1 << 16))
+        for d in range(q):
+            rebuilt = code[:, d] != keep
+            sx = (zx[rebuilt] - c[0, d]) % nx
+            sy = (zy[rebuilt] - c[1, d]) % ny
+            np.bitwise_or.at(words, sy * nx + sx, np.uint32(1 << d))
+        return torch.as_tensor(words.view(np.int32), device=device)
 
     def struct(self):
         if self.count == 0:
-            return _lib.Rules(0, None, None, None, None, None, None, self.words_per_row)
+            return _lib.Rules(0, None, None, None, None, None, None, self.words_per_row, None)
         return _lib.Rules(self.count, self.row_ptr.data_ptr(), self.cell_x.data_ptr(), self.code.data_ptr(),
                           self.cst.data_ptr(), self.mask.data_ptr(), self.word_base.data_ptr(),
-                          self.words_per_row)
+                          self.words_per_row, self.push.data_ptr() if self.push is not None else None)
 
     def restricted(self, nx, ny, dtype, device):
         """The same rules on a smaller grid: cells outside it are dropped (the
@@ -136,7 +160,7 @@ def compile_rules(bcs, nx, ny, q, dtype, device, step=None, names=None, check=Tr
         if np.any(bad):
             raise NotImplementedError("boundary rule scales a population; not representable")
         code[:, d] = cd
-    rules = CompiledRules(q, ny, cells, code, c0, dtype, device, nx)
+    rules = CompiledRules(q, ny, cells, code, c0, dtype, device, nx, push=(step == "PostStreaming"))
     if check:
         _self_check(bcs, nx, ny, q, step, names, rules)
     return rules

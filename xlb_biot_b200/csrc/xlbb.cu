@@ -60,6 +60,7 @@ static RulesView<T, Q> rules_view(const XlbbRules& r) {
     v.mask = r.mask;
     v.word_base = r.word_base;
     v.words_per_row = r.words_per_row;
+    v.push = r.push;
     if (v.count > 0 && (r.mask == nullptr || r.word_base == nullptr)) v.count = 0;
     return v;
 }
@@ -457,10 +458,9 @@ static void launch_sweep(XlbbSweepConfig c, const XlbbGrid* g, cudaStream_t st, 
     constexpr bool F32 = sizeof(typename Ph::T) == 4;
     Ph::fill_ptrs(a);
     if (c.pipeline == 3) {
-        if (Ph::push_ok(a)) {
+        if (Ph::push_ok(a) && (a.ps.count == 0 || a.ps.push != nullptr)) {
             const int bs = c.tx;
             push_kernel<Ph><<<dim3((g->nx + bs - 1) / bs, g->ny), bs, 0, st>>>(a);
-            if (a.ps.count > 0) push_fixup_kernel<Ph><<<(a.ps.count + 127) / 128, 128, 0, st>>>(a);
             return;
         }
         c = push_fallback(F32);
@@ -854,7 +854,7 @@ batched_elast_kernel(const BatchInst<T, S>* __restrict__ inst, const XlbbBatchTi
         p.a = a;
         p.b = b;
         p.mat = ElastMat<T, S>{I.cs, I.cd, I.h, I.n, nullptr, nullptr};
-        p.pc = RulesView<T, 8>{0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0};
+        p.pc = RulesView<T, 8>{0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0, nullptr};
         p.ps = p.pc;
         p.sumsq = tile_sumsq;
         p.bx0 = 0; p.bx1 = I.geom.nx; p.by0 = 0; p.by1 = I.geom.ny;

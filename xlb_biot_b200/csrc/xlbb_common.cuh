@@ -27,6 +27,7 @@ struct RulesView {
     const uint32_t* mask;    // one bit per cell, words_per_row words per row
     const int* word_base;    // index of the first rule cell of each mask word
     int words_per_row;
+    const uint32_t* push;    // per-cell push word of post-streaming rules (or NULL)
 };
 
 // Index of the rule of cell (x, y), or -1.  Rows are CSR, x sorted.

@@ -4,15 +4,29 @@
 // post-collision rules, and write every post-collision population straight to
 // the cell it streams to (z = x + c_i, periodic wrap), mixed with that cell's
 // input as the sweep's algebra asks.  No shared memory, no barriers, no
-// recomputed rows: every input is read once and every output written once
-// (each destination receives exactly one population per direction).
-// Post-streaming rules need the destination cell's own post-collision values,
-// which another thread computed, so a second, sparse kernel over the rule
-// cells recomputes them (same device functions, same arithmetic) and rewrites
-// the directions the rules replace.  Sweeps that fuse an FP64 residual or a
-// divergence output use the row-marching kernels instead.
+// recomputed rows: every input is read once and every output written once.
+// Post-streaming rules are resolved in the same kernel: a direction d that
+// the destination's rule rebuilds from the destination's own post-collision
+// values (source or zero codes) is written by the destination cell's thread,
+// which has those values, and skipped by the pushing thread (a per-cell push
+// word, built with the rule table, says which); rule tables whose "keep"
+// codes transform the pushed value have no push word and use the row-marching
+// sweep.  Each output is written exactly once, with the arithmetic of the
+// row-marching sweep.
+// Sweeps that fuse an FP64 residual or a divergence output use the
+// row-marching kernels instead.
 // Included inside namespace xlbb, after the physics structs.
 #pragma once
+
+// Rule index of cell (zx, zy) in a bitmask-indexed rule table, or -1.
+template <typename T, int Q>
+__device__ __forceinline__ int rule_at(const RulesView<T, Q>& r, int zy, int zx) {
+    const int w = zy * r.words_per_row + (zx >> 5);
+    const uint32_t m = __ldg(r.mask + w);
+    const uint32_t bit = 1u << (zx & 31);
+    if (!(m & bit)) return -1;
+    return __ldg(r.word_base + w) + __popc(m & (bit - 1u));
+}
 
 // Post-collision populations of cell (y, x): load, collide, post-collision rules
 // (the arithmetic of the row-marching sweep's collide stage).
@@ -49,46 +63,26 @@ __global__ void __launch_bounds__(256) push_kernel(const typename Phys::Args p) 
     if (x >= G.nx) return;
     T fs[Q];
     post_collision<Phys>(p, y, x, fs);
+    const int ym = y == 0 ? G.ny - 1 : y - 1, yp = y == G.ny - 1 ? 0 : y + 1;
     const int xm = x == 0 ? G.nx - 1 : x - 1, xp = x == G.nx - 1 ? 0 : x + 1;
-    const int rm = (y == 0 ? G.ny - 1 : y - 1) * G.pitch, r0 = y * G.pitch;
-    const int rp = (y == G.ny - 1 ? 0 : y + 1) * G.pitch;
+    // the cell's push word: directions rebuilt at their destination, own rules
+    const uint32_t pw = p.ps.count > 0 ? __ldg(p.ps.push + y * G.nx + x) : 0u;
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
         const int zx = Phys::cx(i) > 0 ? xp : (Phys::cx(i) < 0 ? xm : x);
-        const int zr = Phys::cy(i) > 0 ? rp : (Phys::cy(i) < 0 ? rm : r0);
-        Phys::put(p, i, zr + zx, fs[i]);
+        const int zy = Phys::cy(i) > 0 ? yp : (Phys::cy(i) < 0 ? ym : y);
+        if (!(pw & (1u << i))) Phys::put(p, i, zy * G.pitch + zx, fs[i]);
     }
-}
-
-// Post-streaming rules of every rule cell (one thread per rule cell).
-template <class Phys>
-__global__ void push_fixup_kernel(const typename Phys::Args p) {
-    using T = typename Phys::T;
-    constexpr int Q = Phys::Q;
-    const SweepGeom& G = p.geom;
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= p.ps.count) return;
-    int lo = 0, hi = G.ny - 1;              // the row y with row_ptr[y] <= r < row_ptr[y + 1]
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (__ldg(p.ps.row_ptr + mid) <= r) lo = mid; else hi = mid - 1;
-    }
-    const int y = lo, x = __ldg(p.ps.cell_x + r);
-    T post[Q];
-    post_collision<Phys>(p, y, x, post);
-    const int o = y * G.pitch + x;
+    if (pw & (1u << 16)) {       // this cell's post-streaming rules, from its own post-collision values
+        const int r = rule_at(p.ps, y, x);
+        const int o = y * G.pitch + x;
 #pragma unroll
-    for (int d = 0; d < Q; ++d) {
-        const uint8_t code = __ldg(p.ps.code + (size_t)r * Q + d);
-        const T cst = p.ps.cst[(size_t)r * Q + d];
-        if (code == 2 * Q + 1 && cst == T(0)) continue;   // identity: the pushed value stands
-        T cur = T(0);
-        if (code >= 2 * Q + 1) {                           // needs the value streamed in: recompute its source
-            T nb[Q];
-            post_collision<Phys>(p, wrap(y - Phys::cy(d), G.ny), wrap(x - Phys::cx(d), G.nx), nb);
-            cur = pick<T, Q>(nb, d);
+        for (int d = 0; d < Q; ++d) {
+            const uint8_t code = __ldg(p.ps.code + (size_t)r * Q + d);
+            if (code != 2 * Q + 1) {
+                const int k = code < Q ? code : (code < 2 * Q ? code - Q : 0);
+                Phys::put(p, d, o, rule_value<T, Q>(code, T(0), pick<T, Q>(fs, k), p.ps.cst[(size_t)r * Q + d]));
+            }
         }
-        const int k = code < Q ? code : (code < 2 * Q ? code - Q : 0);
-        Phys::put(p, d, o, rule_value<T, Q>(code, cur, pick<T, Q>(post, k), cst));
     }
 }
