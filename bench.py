@@ -362,7 +362,7 @@ def run_c1(args):
     res = {}
     for prec in ("f32/f32", "f64/f64"):
         s, u = plain_elasticity_128(G, precision=prec)
-        s.solve(tol=1e-3, check_every=200)                 # warm-up (module load, capture)
+        s.solve(tol=1e-8, check_every=200)                 # warm-up: module load, graph capture, clocks
         (f, it, rel), t = _timed(lambda: s.solve(tol=1e-8, check_every=200))
         eta, _ = s.update_macroscopic(f)
         res[prec] = (eta.double().cpu().numpy(), it, rel, t, s.stalled)
@@ -607,6 +607,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--launch-shape", default="",
                     help="tx,depth,ctas_per_sm,min_rows,pipeline of the Darcy sweep (skips the autotuner)")
+    ap.add_argument("--elast-shape", default="",
+                    help="tx,depth,ctas_per_sm,min_rows,pipeline of the elasticity sweeps (all workloads)")
     ap.add_argument("--adjoint-steps", type=int, default=200)
     ap.add_argument("--fd-directions", type=int, default=32)
     ap.add_argument("--workload", choices=["darcy", "c1", "c3", "c4", "c5"], default="darcy",
@@ -618,6 +620,9 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.elast_shape:
+        from xlb_biot_b200 import autotune
+        autotune.set_config(autotune.ELASTICITY, *[int(v) for v in args.elast_shape.split(",")])
     if args.workload == "c1":
         return run_c1(args)
     if args.workload == "c3":

@@ -70,8 +70,9 @@ static bool rules_ok(const XlbbRules& r, const XlbbGrid* g) {
     return r.cell_x && r.code && r.cst && r.mask && r.word_base && r.words_per_row * 32 >= g->nx;
 }
 
-// Launch shapes of the sweeps, per kernel family (0: elasticity, 1: Darcy).
-static XlbbSweepConfig g_cfg[2] = {{256, 1, 3, 8, 0}, {256, 1, 3, 8, 0}};
+// Launch shapes of the sweeps, per kernel family (0: elasticity, 1: Darcy):
+// collide-and-push by default (sweeps with fused reductions use push_fallback).
+static XlbbSweepConfig g_cfg[2] = {{128, 1, 1, 8, 3}, {128, 1, 1, 8, 3}};
 
 static constexpr int WARP_COLS = 30;   // output columns of one warp of sweep_warp_kernel
 

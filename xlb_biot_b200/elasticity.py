@@ -596,7 +596,7 @@ class LBMElasticity:
                 if rel < tol:
                     break
             return f, it, rel
-        loop = ElasticLoop(self, check_every, external_force)
+        loop = self._elastic_loop(check_every, external_force)
         r0 = loop.first(f)
         it, rel = 1, 1.0
         best, since_best = np.inf, 0
@@ -616,6 +616,18 @@ class LBMElasticity:
                     self.stalled = True
                     break
         return loop.result, it, rel
+
+    def _elastic_loop(self, n, external_force):
+        """The ``ElasticLoop`` of ``n`` sweeps, captured once per solver and
+        reused (a new external force is copied into its buffer in place)."""
+        cache = self.__dict__.setdefault("_loops", {})
+        key = (int(n), external_force is None)
+        loop = cache.get(key)
+        if loop is None:
+            loop = cache[key] = ElasticLoop(self, n, external_force)
+        elif external_force is not None:
+            loop.ext.copy_(self._L().field(external_force, 2))
+        return loop
 
     def _restrict_full(self, res, level):
         Lf, Lc = self._L(level), self._L(level + 1)
@@ -852,7 +864,10 @@ class ElasticLoop:
         L = solver._L(0)
         self.solver, self.n = solver, int(n) + (int(n) % 2)   # even: the result lands in ``state``
         self.state, self._other = L.empty(8), L.empty(8)
-        self.ext = L.field(external_force, 2)
+        self.ext = None                       # owned buffer: the graph reads it by address
+        if external_force is not None:
+            self.ext = L.empty(2)
+            self.ext.copy_(L.field(external_force, 2))
         self.sumsq = torch.zeros(1, dtype=torch.float64, device=L.device)
         self.launches_per_replay = self.n + 1
         s = torch.cuda.Stream()
