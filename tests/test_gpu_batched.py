@@ -101,3 +101,30 @@ def test_error_criterion_reaches_fp64_accuracy():
         u, u64 = b.displacement(i), b64.displacement(i)
         err = float(torch.linalg.vector_norm(u - u64) / torch.linalg.vector_norm(u64))
         assert err < 3e-6, (i, err)
+
+
+@pytest.mark.parametrize("prec", ["f64/f64", "f32/f32"])
+def test_batched_push_and_row_marching_identical(prec):
+    """The batched sweep's collide-and-push form (the default) and its
+    row-marching form give bit-identical V-cycles (populations and correction
+    norms); the residual norms group their FP64 partials differently."""
+    from xlb_biot_b200 import autotune
+    from xlb_biot_b200.batched import BatchedElasticity
+    from xlb_biot_b200.workloads import batch_instances
+    sizes, lams, mus, forces = batch_instances(count=5, sizes=(24, 32, 48, 64), seed=9)
+    saved = autotune.get_config(autotune.ELASTICITY)
+    out = []
+    try:
+        for shape in ((256, 1, 3, 8, 0), (128, 1, 1, 8, 3)):
+            autotune.set_config(autotune.ELASTICITY, *shape)
+            b = BatchedElasticity(sizes, lams, mus, forces, levels="auto", precision=prec, coarsest_precision="f64",
+                                  residual_precision="f64")
+            b.reset()
+            for _ in range(3):
+                b.vcycle()
+            out.append(([b.populations(i).clone() for i in range(len(sizes))], b.norm2.clone(), b.corr2.clone()))
+    finally:
+        autotune.set_config(autotune.ELASTICITY, **saved)
+    for x, y in zip(out[0][0], out[1][0]):
+        assert torch.equal(x, y)
+    assert torch.allclose(out[0][1], out[1][1], rtol=1e-12, atol=0) and torch.equal(out[0][2], out[1][2])

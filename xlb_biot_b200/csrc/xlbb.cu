@@ -238,14 +238,26 @@ struct ElastPhys {
 #pragma unroll
         for (int i = 0; i < 8; ++i) g[i] = RESID ? in.f[i] - in.r[i] : in.f[i];
     }
-    // Output population i of the cell at offset o from its streamed-in value s
-    // (the store stage's algebra, for the collide-and-push sweep).
-    __device__ static void put(const Args& p, int i, int o, T s) {
+    // Output population i of cell (zx, zy) (offset o) from its streamed-in
+    // value s, with the store stage's algebra (collide-and-push sweep); returns
+    // the value's term of the fused FP64 sum of squares (0 without one).
+    template <bool SUMSQ>
+    __device__ static double put(const Args& p, int i, int o, int zx, int zy, T s) {
         T v = s;
-        if (p.mix) v = p.a * T(__ldg(p.ip[i] + o)) + p.b * s;
-        p.op[i][o] = S_(v);
+        T fz = T(0);
+        if (p.mix || (SUMSQ && p.sumsq_diff)) fz = T(__ldg(p.ip[i] + o));
+        if (p.mix) v = p.a * fz + p.b * s;
+        const S_ sv = S_(v);
+        p.op[i][o] = sv;
+        if constexpr (SUMSQ) {
+            if (zx < p.bx0 || zx >= p.bx1 || zy < p.by0 || zy >= p.by1) return 0.0;
+            double d = (double)sv;
+            if (p.sumsq_diff) d -= (double)S_(fz);
+            return d * d;
+        }
+        return 0.0;
     }
-    static bool push_ok(const Args& a) { return a.sumsq == nullptr && a.div_out == nullptr; }
+    static bool push_ok(const Args& a) { return a.div_out == nullptr; }
     __device__ static T f_in(const In& in, int i) { return in.f[i]; }
     __device__ static void collide(const Args& p, int y, int x, const In& in, T (&o)[8]) {
         T g[8];
@@ -357,8 +369,16 @@ struct DarcyPhys {
 #pragma unroll
         for (int i = 0; i < 9; ++i) g[i] = in.f[i];
     }
-    __device__ static void put(const Args& p, int i, int o, T s) { p.op[i][o] = s; }
-    static bool push_ok(const Args& a) { return a.sumsq == nullptr; }
+    template <bool SUMSQ>
+    __device__ static double put(const Args& p, int i, int o, int, int, T s) {
+        p.op[i][o] = s;
+        if constexpr (SUMSQ) {
+            const double d = (double)s - (double)__ldg(p.ip[i] + o);
+            return d * d;
+        }
+        return 0.0;
+    }
+    static bool push_ok(const Args&) { return true; }
     __device__ static T f_in(const In& in, int i) { return in.f[i]; }
     __device__ static void collide(const Args& p, int, int, const In& in, T (&o)[9]) {
         const bool hasS = p.source != nullptr || p.ext != nullptr;
@@ -451,6 +471,15 @@ static bool bulk_aligned(const typename Ph::Args& a) {
     return true;
 }
 
+// Collide and push: one thread per cell, tx threads per block along x, one row
+// per block row; with fused partials, one FP64 partial per block.
+template <class Ph>
+static void launch_push(const XlbbSweepConfig& c, const XlbbGrid* g, cudaStream_t st, const typename Ph::Args& a) {
+    const dim3 grid((g->nx + c.tx - 1) / c.tx, g->ny);
+    if (a.sumsq) push_kernel<Ph, true><<<grid, c.tx, 0, st>>>(a);
+    else push_kernel<Ph, false><<<grid, c.tx, 0, st>>>(a);
+}
+
 // Runtime (bulk, tx, depth) -> template instance.  The register-prefetch
 // kernel takes depth 1..2, the bulk-copy ring depth 2, 4 or 6; FP64 uses
 // tx = 128 (larger rings exceed the shared memory of one SM).
@@ -460,8 +489,7 @@ static void launch_sweep(XlbbSweepConfig c, const XlbbGrid* g, cudaStream_t st, 
     Ph::fill_ptrs(a);
     if (c.pipeline == 3) {
         if (Ph::push_ok(a) && (a.ps.count == 0 || a.ps.push != nullptr)) {
-            const int bs = c.tx;
-            push_kernel<Ph><<<dim3((g->nx + bs - 1) / bs, g->ny), bs, 0, st>>>(a);
+            launch_push<Ph>(c, g, st, a);
             return;
         }
         c = push_fallback(F32);
@@ -517,7 +545,7 @@ static void launch_sweep_regs(const XlbbSweepConfig& c, const XlbbGrid* g, cudaS
 static XlbbSweepConfig effective_cfg(int kernel, int dtype) {
     XlbbSweepConfig c = g_cfg[kernel];
     if ((dtype == XLBB_F64 || dtype == XLBB_F32_ACC64) && c.tx > 128) c.tx = 128;
-    if (dtype == XLBB_F32_ACC64 && c.pipeline != 0) {
+    if (dtype == XLBB_F32_ACC64 && (c.pipeline == 1 || c.pipeline == 2)) {
         c.pipeline = 0;
         if (c.depth > 2) c.depth = 2;
     }
@@ -767,7 +795,13 @@ static int launch_elast(const XlbbGrid* g, const XlbbElastMaterial* mat, const X
     a.div_out = static_cast<S*>(s->div_out);
     a.div_scale = T(-1.5 / (3.0 * (mat->lam + mat->mu) + 1.0));
     if constexpr (sizeof(T) != sizeof(S)) {
-        launch_sweep_regs<Ph, PREV>(effective_cfg(0, XLBB_F32_ACC64), g, st, a);
+        const XlbbSweepConfig c = effective_cfg(0, XLBB_F32_ACC64);
+        if (c.pipeline == 3 && Ph::push_ok(a) && (a.ps.count == 0 || a.ps.push != nullptr)) {
+            Ph::fill_ptrs(a);
+            launch_push<Ph>(c, g, st, a);
+        } else {
+            launch_sweep_regs<Ph, PREV>(c, g, st, a);
+        }
     } else {
         const XlbbSweepConfig c = effective_cfg(0, sizeof(T) == 4 ? XLBB_F32 : XLBB_F64);
         launch_sweep<Ph, PREV>(c, g, st, a);
@@ -873,6 +907,48 @@ batched_elast_kernel(const BatchInst<T, S>* __restrict__ inst, const XlbbBatchTi
     }
 }
 
+// Collide-and-push form of the batched sweep (no fused reduction): a block of
+// 128 x 8 threads takes a tile, thread (tx, ty) its column x0 + tx and every
+// 8th row from ys + ty (independent cells: no barrier).
+template <typename T, bool RESID, bool SUMSQ, typename S = T>
+__global__ void __launch_bounds__(1024)
+batched_push_kernel(const BatchInst<T, S>* __restrict__ inst, const XlbbBatchTile* __restrict__ tiles, int ntiles,
+                    T a, T b, int mix, int use_force, int sumsq_diff, double* tile_sumsq) {
+    using Ph = ElastPhys<T, RESID, S>;
+    __shared__ double red[32];
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const XlbbBatchTile tl = tiles[t];
+        const BatchInst<T, S> I = inst[tl.inst];
+        const int x = tl.x0 + threadIdx.x;
+        double acc = 0.0;
+        typename Ph::Args p;
+        p.geom = I.geom;
+        p.f_in = I.f_in;
+        p.f_out = I.f_out;
+        p.force = use_force ? I.force : nullptr;
+        p.fext = nullptr;
+        p.resid = I.resid;
+        p.a = a;
+        p.b = b;
+        p.mat = ElastMat<T, S>{I.cs, I.cd, I.h, I.n, nullptr, nullptr};
+        p.pc = RulesView<T, 8>{0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0, nullptr};
+        p.ps = p.pc;
+        p.sumsq = tile_sumsq;
+        p.bx0 = 0; p.bx1 = I.geom.nx; p.by0 = 0; p.by1 = I.geom.ny;
+        p.div_out = nullptr;
+        p.mix = mix;
+        p.sumsq_diff = sumsq_diff;
+        p.np = 0;
+        Ph::fill_ptrs(p);
+        if (x < I.geom.nx)
+            for (int y = tl.ys + threadIdx.y; y < tl.ye; y += blockDim.y) acc += push_cell<Ph, SUMSQ>(p, y, x);
+        if constexpr (SUMSQ) {   // the tile's writes: every output of the instance is written once
+            const double s = block_sum_2d(acc, red);
+            if (threadIdx.x == 0 && threadIdx.y == 0) tile_sumsq[t] = s;
+        }
+    }
+}
+
 // Restriction (2x2 block sums) and prolongation (injection, added) of every
 // instance of a periodic batch; blockIdx.y = instance.
 template <typename Tf, typename Tc>
@@ -973,8 +1049,8 @@ const char* xlbb_last_error(void) { return g_last_error.c_str(); }
 int xlbb_elast_sweep_ctas(int dtype, const XlbbGrid* g) {
     if (!grid_ok(g) || (dtype != XLBB_F32 && dtype != XLBB_F64 && dtype != XLBB_F32_ACC64))
         return fail(XLBB_EBADARG, "xlbb_elast_sweep_ctas: bad argument");
-    XlbbSweepConfig c = effective_cfg(0, dtype);
-    if (c.pipeline == 3) c = push_fallback(dtype == XLBB_F32);
+    const XlbbSweepConfig c = effective_cfg(0, dtype);
+    if (c.pipeline == 3) return ((g->nx + c.tx - 1) / c.tx) * g->ny;   // one partial per push block
     const dim3 a = sweep_grid(g, c);
     return (int)(a.x * a.y);
 }
@@ -982,8 +1058,8 @@ int xlbb_elast_sweep_ctas(int dtype, const XlbbGrid* g) {
 int xlbb_darcy_sweep_ctas(int dtype, const XlbbGrid* g) {
     if (!grid_ok(g) || (dtype != XLBB_F32 && dtype != XLBB_F64))
         return fail(XLBB_EBADARG, "xlbb_darcy_sweep_ctas: bad argument");
-    XlbbSweepConfig c = effective_cfg(1, dtype);
-    if (c.pipeline == 3) c = push_fallback(dtype == XLBB_F32);
+    const XlbbSweepConfig c = effective_cfg(1, dtype);
+    if (c.pipeline == 3) return ((g->nx + c.tx - 1) / c.tx) * g->ny;   // one partial per push block
     const dim3 a = sweep_grid(g, c);
     return (int)(a.x * a.y);
 }
@@ -1019,6 +1095,8 @@ int xlbb_elast_sweep(int dtype, const XlbbGrid* g, const XlbbElastMaterial* mat,
 
     if ((mat->mu_field == nullptr) != (mat->lam_field == nullptr))
         return fail(XLBB_EBADARG, "xlbb_elast_sweep: lam_field and mu_field go together");
+    if (s->div_out && s->sumsq && effective_cfg(0, dtype).pipeline == 3)
+        return fail(XLBB_EUNSUPPORTED, "xlbb_elast_sweep: div_out with sumsq needs a row-marching launch shape");
     if (dtype == XLBB_F32) return elast_sweep_t<float>(g, mat, s, XLBB_STREAM(stream));
     if (dtype == XLBB_F64) return elast_sweep_t<double>(g, mat, s, XLBB_STREAM(stream));
     if (dtype == XLBB_F32_ACC64) return elast_sweep_t<double, float>(g, mat, s, XLBB_STREAM(stream));
@@ -1283,6 +1361,16 @@ static int batched_sweep_t(const void* inst, const XlbbBatchTile* tiles, int nti
     const int mix = (a == 0.0 && b == 1.0) ? 0 : 1;
     const bool prev = mix || (tile_sumsq && sumsq_diff);
     const BatchInst<T, S>* I = static_cast<const BatchInst<T, S>*>(inst);
+    if (g_cfg[0].pipeline == 3) {     // collide and push
+        const dim3 blk(128, 8);
+#define XLBB_BP(R, Q_)                                                                                   \
+    batched_push_kernel<T, R, Q_, S><<<ctas, blk, 0, st>>>(I, tiles, ntiles, T(a), T(b), mix, use_force, sumsq_diff, \
+                                                          tile_sumsq)
+        if (has_resid) { if (tile_sumsq) XLBB_BP(true, true); else XLBB_BP(true, false); }
+        else { if (tile_sumsq) XLBB_BP(false, true); else XLBB_BP(false, false); }
+#undef XLBB_BP
+        return check_launch("xlbb_batched_elast_sweep");
+    }
 #define XLBB_B(R, P) \
     batched_elast_kernel<T, 128, R, P, S><<<ctas, 160, 0, st>>>(I, tiles, ntiles, T(a), T(b), mix, use_force, \
                                                                  sumsq_diff, tile_sumsq)

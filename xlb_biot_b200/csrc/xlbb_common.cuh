@@ -84,4 +84,22 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
     return s;
 }
 
+// Block-wide FP64 sum for 2D blocks (warps follow the linear thread index;
+// sh holds one double per warp): the total is returned in thread (0, 0).
+__device__ __forceinline__ double block_sum_2d(double v, double* sh) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    const int lane = tid & 31, wid = tid >> 5;
+    __syncthreads();
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    double s = 0.0;
+    if (tid == 0) {
+        const int nw = (blockDim.x * blockDim.y + 31) >> 5;
+        for (int i = 0; i < nw; ++i) s += sh[i];   // fixed order: deterministic
+    }
+    return s;
+}
+
 }  // namespace xlbb

@@ -12,9 +12,9 @@
 // word, built with the rule table, says which); rule tables whose "keep"
 // codes transform the pushed value have no push word and use the row-marching
 // sweep.  Each output is written exactly once, with the arithmetic of the
-// row-marching sweep.
-// Sweeps that fuse an FP64 residual or a divergence output use the
-// row-marching kernels instead.
+// row-marching sweep.  The fused FP64 sums of squares are the writers' sums
+// (one partial per block); only the divergence side output needs the
+// row-marching kernels.
 // Included inside namespace xlbb, after the physics structs.
 #pragma once
 
@@ -53,25 +53,26 @@ __device__ __forceinline__ void post_collision(const typename Phys::Args& p, int
     }
 }
 
-template <class Phys>
-__global__ void __launch_bounds__(256) push_kernel(const typename Phys::Args p) {
+// One cell of the collide-and-push sweep; returns the FP64 squares of the
+// values it wrote (the sweep's fused sum: every output is written exactly once,
+// so the writers' sums add up to the sum over all outputs).
+template <class Phys, bool SUMSQ>
+__device__ __forceinline__ double push_cell(const typename Phys::Args& p, int y, int x) {
     using T = typename Phys::T;
     constexpr int Q = Phys::Q;
     const SweepGeom& G = p.geom;
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y;
-    if (x >= G.nx) return;
     T fs[Q];
     post_collision<Phys>(p, y, x, fs);
     const int ym = y == 0 ? G.ny - 1 : y - 1, yp = y == G.ny - 1 ? 0 : y + 1;
     const int xm = x == 0 ? G.nx - 1 : x - 1, xp = x == G.nx - 1 ? 0 : x + 1;
     // the cell's push word: directions rebuilt at their destination, own rules
     const uint32_t pw = p.ps.count > 0 ? __ldg(p.ps.push + y * G.nx + x) : 0u;
+    double acc = 0.0;
 #pragma unroll
     for (int i = 0; i < Q; ++i) {
         const int zx = Phys::cx(i) > 0 ? xp : (Phys::cx(i) < 0 ? xm : x);
         const int zy = Phys::cy(i) > 0 ? yp : (Phys::cy(i) < 0 ? ym : y);
-        if (!(pw & (1u << i))) Phys::put(p, i, zy * G.pitch + zx, fs[i]);
+        if (!(pw & (1u << i))) acc += Phys::template put<SUMSQ>(p, i, zy * G.pitch + zx, zx, zy, fs[i]);
     }
     if (pw & (1u << 16)) {       // this cell's post-streaming rules, from its own post-collision values
         const int r = rule_at(p.ps, y, x);
@@ -81,8 +82,24 @@ __global__ void __launch_bounds__(256) push_kernel(const typename Phys::Args p) 
             const uint8_t code = __ldg(p.ps.code + (size_t)r * Q + d);
             if (code != 2 * Q + 1) {
                 const int k = code < Q ? code : (code < 2 * Q ? code - Q : 0);
-                Phys::put(p, d, o, rule_value<T, Q>(code, T(0), pick<T, Q>(fs, k), p.ps.cst[(size_t)r * Q + d]));
+                acc += Phys::template put<SUMSQ>(p, d, o, x, y,
+                                 rule_value<T, Q>(code, T(0), pick<T, Q>(fs, k), p.ps.cst[(size_t)r * Q + d]));
             }
         }
+    }
+    return acc;
+}
+
+template <class Phys, bool SUMSQ>
+__global__ void __launch_bounds__(256) push_kernel(const typename Phys::Args p) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    if constexpr (SUMSQ) {        // one FP64 partial per block
+        __shared__ double red[8];
+        const double acc = x < p.geom.nx ? push_cell<Phys, true>(p, y, x) : 0.0;
+        const double s = block_sum(acc, red);
+        if (threadIdx.x == 0) p.sumsq[blockIdx.y * gridDim.x + blockIdx.x] = s;
+    } else {
+        if (x < p.geom.nx) push_cell<Phys, false>(p, y, x);
     }
 }
