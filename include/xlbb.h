@@ -338,6 +338,15 @@ int xlbb_darcy_moments_adjoint(int dtype, const XlbbGrid* g, const void* f, doub
                                const void* omega_field, const void* lam_rho, const void* lam_grad, void* lam_f,
                                double* g_omega, void* stream);
 
+/* Transpose of a multigrid level's Biot coupling force
+ * ext = fe + G(div(f), scale) (xlbb_darcy_gradient of xlbb_elast_moments'
+ * divergence, with the gradient's rules): lam_f += div^T G^T lam_ext,
+ * lam_fe += lam_ext (if not NULL), g_lam / g_mu += derivative of the
+ * divergence scale (need the forward f).  One kernel. */
+int xlbb_divgrad_adjoint(int dtype, const XlbbGrid* g, const XlbbElastMaterial* mat, const void* lam_ext,
+                         double scale, const XlbbRules* rules, const void* f, void* lam_f, void* lam_fe,
+                         double* g_lam, double* g_mu, void* stream);
+
 /* Deterministic FP64 sum of n partials (fixed order) into *out. */
 int xlbb_reduce_sum(const double* partials, int n, double* out, void* stream);
 

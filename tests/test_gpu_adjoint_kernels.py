@@ -157,3 +157,27 @@ def test_moment_adjoints_are_the_transposes(G):
     fd = _fd(da.omega_field.copy_, da.omega_field.clone(), d, 1e-7,
              lambda: ip(da.update_macroscopic(f9, gradient=True)[1], yg))
     assert abs(fd - ip(g_om, d)) <= 1e-6 * abs(fd)
+
+
+def test_fused_divgrad_adjoint_equals_composition(G):
+    """xlbb_divgrad_adjoint (one kernel) equals the gradient-stencil transpose
+    followed by the divergence transpose, plus the force accumulation."""
+    from xlb_biot_b200.adjoint import ElastGrads, divgrad_adjoint, elast_moments_adjoint, gradient_adjoint
+    from xlb_biot_b200.workloads import terzaghi_heterogeneous
+    sim, _ = terzaghi_heterogeneous(G, nx=32, ny=18, levels=2, cycles=1, ell=5.0, precision="f64/f64")
+    el, da = sim.elasticity, sim.darcy
+    for level in range(el.levels):
+        L = el._L(level)
+        lam_ext, f = rnd(L, 2, 1), rnd(L, 8, 2)
+        g1, g2 = ElastGrads(el), ElastGrads(el)
+        a_f, a_fe = rnd(L, 8, 3), rnd(L, 2, 4)
+        b_f, b_fe = L.empty(8), L.empty(2)
+        b_f.copy_(a_f)
+        b_fe.copy_(a_fe)
+        divgrad_adjoint(el, da, level, lam_ext, 0.3, a_f, lam_fe=a_fe, f=f, grads=g1)
+        lam_div = L.zeros(1)
+        gradient_adjoint(da, lam_ext, 0.3, lam_div, dtype=L.dtype)
+        elast_moments_adjoint(el, level, b_f, lam_div=lam_div, f=f, grads=g2)
+        b_fe.add_(lam_ext)
+        for x, y in ((a_f, b_f), (a_fe, b_fe), (g1.mu[level], g2.mu[level]), (g1.lam[level], g2.lam[level])):
+            assert torch.allclose(x, y, rtol=1e-13, atol=1e-13 * float(y.abs().max()))

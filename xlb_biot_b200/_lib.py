@@ -118,6 +118,8 @@ SIGNATURES = {
     "xlbb_darcy_gradient_adjoint": (I, [I, PG, P, D, ctypes.POINTER(Rules), P, P]),
     "xlbb_elast_moments_adjoint": (I, [I, PG, ctypes.POINTER(ElastMaterial), P, P, P, D, P, P, P, P]),
     "xlbb_darcy_moments_adjoint": (I, [I, PG, P, D, P, P, P, P, P, P]),
+    "xlbb_divgrad_adjoint": (I, [I, PG, ctypes.POINTER(ElastMaterial), P, D, ctypes.POINTER(Rules), P, P, P, P, P,
+                                 P]),
     "xlbb_last_error": (ctypes.c_char_p, []),
     "xlbb_version": (I, []),
 }

@@ -121,3 +121,27 @@ def darcy_moments_adjoint(da, lam_f, lam_rho=None, lam_grad=None, f=None, g_omeg
         lam_f.data_ptr(), g_omega.data_ptr() if g_omega is not None else None, _lib.stream_ptr()),
         "xlbb_darcy_moments_adjoint")
     return lam_f
+
+
+def divgrad_adjoint(el, da, level, lam_ext, scale, lam_f, lam_fe=None, f=None, grads=None):
+    """Transpose of the coupling force ext = fe + ``da.gradient(el.update_divergence(f,
+    level), scale, dtype=level's)``: lam_f += div^T G^T lam_ext, lam_fe += lam_ext
+    (if given); ``grads`` accumulates the divergence scale's derivative (needs f)."""
+    L = el._L(level)
+    rules = da.gradient_rules(L.nx, L.ny, L.dtype)
+    _lib.check(_lib.lib().xlbb_divgrad_adjoint(
+        _lib.dtype_code(L.dtype), L.grid(), el._mats[level], lam_ext.data_ptr(), float(scale), rules.struct(), _p(f),
+        lam_f.data_ptr(), _p(lam_fe), grads.lam[level].data_ptr() if grads is not None else None,
+        grads.mu[level].data_ptr() if grads is not None else None, _lib.stream_ptr()), "xlbb_divgrad_adjoint")
+    return lam_f
+
+
+def add_(dst, src):
+    """dst += src for two fields of one layout (the library's axpby over the
+    fields' planes, padding included)."""
+    n = dst.shape[2] * dst.stride(2)
+    if src.shape != dst.shape or src.stride() != dst.stride() or src.dtype != dst.dtype:
+        raise ValueError("add_: fields of one layout expected")
+    _lib.check(_lib.lib().xlbb_axpby(_lib.dtype_code(dst.dtype), n, 1.0, dst.data_ptr(), 1.0, src.data_ptr(),
+                                     dst.data_ptr(), _lib.stream_ptr()), "xlbb_axpby")
+    return dst

@@ -24,8 +24,8 @@ import time
 
 import torch
 
-from .adjoint import (ElastGrads, darcy_moments_adjoint, darcy_sweep_adjoint, elast_moments_adjoint,
-                      elast_sweep_adjoint, f64_plane, gradient_adjoint)
+from .adjoint import (ElastGrads, add_, darcy_moments_adjoint, darcy_sweep_adjoint, divgrad_adjoint,
+                      elast_moments_adjoint, elast_sweep_adjoint, f64_plane, gradient_adjoint)
 from .elasticity import material_hierarchy
 
 
@@ -222,12 +222,7 @@ class BiotAdjointModel:
     def _N_adj(self, lam_ext, f, level, lam_f, lam_fe):
         """Transpose of ext = fe + G(div_level(f), sN): lam_fe += lam_ext (if
         given), lam_f += div^T G^T lam_ext, material gradient of div."""
-        L = self.el._L(level)
-        if lam_fe is not None:
-            lam_fe.add_(lam_ext)
-        lam_div = L.zeros(1)
-        gradient_adjoint(self.da, lam_ext, self.sN, lam_div, dtype=L.dtype)
-        elast_moments_adjoint(self.el, level, lam_f, lam_div=lam_div, f=f, grads=self.grads)
+        divgrad_adjoint(self.el, self.da, level, lam_ext, self.sN, lam_f, lam_fe=lam_fe, f=f, grads=self.grads)
 
     def _vcycle_adj(self, lam, rec, lam_resid, lam_fe):
         el, g = self.el, self.el.gamma
@@ -251,7 +246,7 @@ class BiotAdjointModel:
                 lam_f, lam_ext = elast_sweep_adjoint(el, lv, lam_res, 1.0, -1.0, f_in=f, resid=r, fext=ext,
                                                      lam_resid=lam_resid, want_force=True, grads=self.grads)
                 self._N_adj(lam_ext, f, lv, lam_f, lam_fe)
-                lam = el._f(lam + lam_f, lv)
+                lam = add_(lam_f, lam)
         return lam
 
     def step_adjoint(self, tp, lam_fe_new, lam_fd_new, lam_dtd_new, lam_eta=None, lam_p=None):

@@ -328,6 +328,68 @@ __global__ void darcy_moments_adjoint_kernel(SweepGeom G, const T* f, T omega, c
     if (g_omega && lam_grad) g_omega[o] += dom;
 }
 
+// Transpose of the Biot coupling force of a multigrid level,
+// ext = fe + G(c(x) m2(f), scale): one kernel for G^T (the gradient stencil
+// with its rules, gathered at this cell) followed by the divergence's
+// transpose at this cell: lam_f += c w2 (G^T lam_ext), lam_fe += lam_ext, and
+// the divergence scale's material gradient (needs the forward f).
+template <typename T>
+__global__ void divgrad_adjoint_kernel(SweepGeom G, ElastMat<T> mat, T lam_u, T mu_u, T div_scale, T scale,
+                                       RulesView<T, 9> rules, const T* lg, const T* f, T* lam_f, T* lam_fe,
+                                       double* g_lam, double* g_mu) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    if (x >= G.nx) return;
+    const size_t o = (size_t)y * G.pitch + x;
+    const long long P = G.plane;
+    T acc = T(0);                       // (G^T lam_ext)(x), as gradient_adjoint_kernel
+#pragma unroll
+    for (int d = 1; d < 9; ++d) {
+        const int zx = wrap(x + cx9(d), G.nx), zy = wrap(y + cy9(d), G.ny);
+        const size_t oz = (size_t)zy * G.pitch + zx;
+        const T k = T(-3) * scale * w9<T>(d);
+        T v = k * (T(cx9(d)) * __ldg(lg + oz) + T(cy9(d)) * __ldg(lg + oz + P));
+        if (rules.count > 0) v *= rule_keep_factor<T, 9>(rules, zy, zx, d);
+        acc += v;
+    }
+    const T gx = __ldg(lg + o), gy = __ldg(lg + o + P);
+    if (rules.count > 0) {
+        const int r = find_rule(rules, y, x);
+        if (r >= 0) {
+#pragma unroll
+            for (int d = 0; d < 9; ++d) {
+                const uint8_t code = __ldg(rules.code + (size_t)r * 9 + d);
+                if (code < 18) {
+                    const T k = T(-3) * scale * w9<T>(d);
+                    const T v = k * (T(cx9(d)) * gx + T(cy9(d)) * gy);
+                    acc += code < 9 ? v : -v;
+                }
+            }
+        }
+    }
+    if (lam_fe) {
+        lam_fe[o] += gx;
+        lam_fe[o + P] += gy;
+    }
+    T lam = lam_u, mu = mu_u, c = div_scale;
+    if (mat.mu_f) {
+        lam = mat.lam_f[o];
+        mu = mat.mu_f[o];
+        c = T(-1.5) / (T(3) * (lam + mu) + T(1));
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) lam_f[o + i * P] += c * (i < 4 ? T(1) : T(2)) * acc;
+    if (g_mu) {
+        double m2 = 0.0;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) m2 += (i < 4 ? 1.0 : 2.0) * (double)f[o + i * P];
+        const double s = (double)lam + (double)mu;
+        const double v = (double)acc * m2 * (4.5 / ((3.0 * s + 1.0) * (3.0 * s + 1.0)));
+        g_lam[o] += v;
+        g_mu[o] += v;
+    }
+}
+
 }  // namespace xlbb
 
 extern "C" {
@@ -462,6 +524,30 @@ int xlbb_darcy_moments_adjoint(int dtype, const XlbbGrid* g, const void* f, doub
             (const double*)lam_grad, (double*)lam_f, g_omega);
     else return fail(XLBB_EUNSUPPORTED, "xlbb_darcy_moments_adjoint: dtype");
     return check_launch("xlbb_darcy_moments_adjoint");
+}
+
+int xlbb_divgrad_adjoint(int dtype, const XlbbGrid* g, const XlbbElastMaterial* mat, const void* lam_ext,
+                         double scale, const XlbbRules* rules, const void* f, void* lam_f, void* lam_fe,
+                         double* g_lam, double* g_mu, void* stream) {
+    using namespace xlbb;
+    if (!grid_ok(g) || !mat || !lam_ext || !lam_f || !rules) return fail(XLBB_EBADARG, "xlbb_divgrad_adjoint: bad argument");
+    if ((g_lam == nullptr) != (g_mu == nullptr) || (g_mu && !f))
+        return fail(XLBB_EBADARG, "xlbb_divgrad_adjoint: parameter gradients need g_lam, g_mu and f");
+    if (!rules_ok(*rules, g)) return fail(XLBB_EBADARG, "xlbb_divgrad_adjoint: incomplete rules");
+    const dim3 grid((g->nx + 127) / 128, g->ny);
+    cudaStream_t st = XLBB_STREAM(stream);
+    const double div_scale = -1.5 / (3.0 * (mat->lam + mat->mu) + 1.0);
+    if (dtype == XLBB_F32)
+        divgrad_adjoint_kernel<float><<<grid, 128, 0, st>>>(
+            geom(g), make_mat<float>(mat), (float)mat->lam, (float)mat->mu, (float)div_scale, (float)scale,
+            rules_view<float, 9>(*rules), (const float*)lam_ext, (const float*)f, (float*)lam_f, (float*)lam_fe,
+            g_lam, g_mu);
+    else if (dtype == XLBB_F64)
+        divgrad_adjoint_kernel<double><<<grid, 128, 0, st>>>(
+            geom(g), make_mat<double>(mat), mat->lam, mat->mu, div_scale, scale, rules_view<double, 9>(*rules),
+            (const double*)lam_ext, (const double*)f, (double*)lam_f, (double*)lam_fe, g_lam, g_mu);
+    else return fail(XLBB_EUNSUPPORTED, "xlbb_divgrad_adjoint: dtype");
+    return check_launch("xlbb_divgrad_adjoint");
 }
 
 }  // extern "C"
