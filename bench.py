@@ -490,6 +490,13 @@ def run_c4(args):
     b.solve(tol=1e-2, max_cycles=3)                                   # warm-up + graph capture
     (cycles, est), secs = _timed(lambda: b.solve(tol=tol, max_cycles=max_cycles, criterion="error"))
     lu = b.lattice_updates_per_cycle() * cycles
+    # roofline of the batched kernel: level-0 smoothing sweeps of the whole batch
+    # (72 B per cell: 8 populations read and written, 2 force planes, FP32)
+    ln = b.smooth_xy[0][0]
+    (_, t_sw) = _timed(lambda: [b._sweep(0, ln, 1.0 - b.gamma, b.gamma) for _ in range(20)])
+    cells0 = sum(nx * ny for nx, ny in sizes)
+    peak, peak_kind = measured_peak_hbm()
+    sweep_gbs = cells0 * 72 / (t_sw / 20) / 1e9
 
     # FP64 GPU oracle: the same batch in FP64 to a relative residual of 1e-11
     b64 = BatchedElasticity(sizes, lams, mus, forces, levels="auto", precision="f64/f64")
@@ -535,6 +542,10 @@ def run_c4(args):
                                      "mean_vcycles": cyc_single / len(sample)},
             "speedup_vs_single_loop": (args.instances / secs) / single_sps,
             "launches_per_vcycle": b.launches_per_cycle,
+            "batched_sweep_roofline": {"bound": "hbm", "achieved": sweep_gbs, "peak": peak, "unit": "GB/s",
+                                       "frac": sweep_gbs / peak, "peak_kind": peak_kind,
+                                       "kernel": "xlbb::batched_push_kernel<float> (level-0 smoothing sweep, "
+                                                 "all 512 instances, 72 B/LU)", "sweep_ms": t_sw / 20 * 1e3},
             "dtype": "f32 storage and smoothing, f64 level-0 residual arithmetic, f64 coarsest level and norms",
             "levels": "per instance: coarsest side 3-4 cells (5 to 8 levels)",
             "material": "mu in [0.5, 2] / 16, nu in [0.1, 0.4] (lattice lambda + mu <= 0.29: the D2Q8 "
