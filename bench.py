@@ -554,6 +554,30 @@ def run_c4(args):
     return 0
 
 
+def run_c4sweep(args):
+    """The batched kernel alone: level-0 damped smoothing sweeps (a = 1/4,
+    b = 3/4) of the 512-instance batch, timed with CUDA events; prints the
+    sweep's roofline (72 B per cell: 8 populations read and written, 2 force
+    planes, FP32)."""
+    from xlb_biot_b200.batched import BatchedElasticity
+    from xlb_biot_b200.workloads import batch_instances
+    sizes, lams, mus, forces = batch_instances(count=args.instances)
+    b = BatchedElasticity(sizes, lams, mus, forces, levels="auto", precision="f32/f32", coarsest_precision="f64",
+                          residual_precision="f64")
+    ln = b.smooth_xy[0][0]
+    for _ in range(max(3, args.warmup)):
+        b._sweep(0, ln, 0.25, 0.75)
+    (_, t) = _timed(lambda: [b._sweep(0, ln, 0.25, 0.75) for _ in range(args.steps)])
+    cells = sum(nx * ny for nx, ny in sizes)
+    peak, peak_kind = measured_peak_hbm()
+    gbs = cells * 72 / (t / args.steps) / 1e9
+    print(json.dumps({"workload": "c4_batched_level0_sweep", "metric": "GB/s", "value": gbs, "unit": "GB/s",
+                      "cells": cells, "sweeps": args.steps, "ms_per_sweep": t / args.steps * 1e3,
+                      "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
+                                   "frac": gbs / peak, "peak_kind": peak_kind}}), flush=True)
+    return 0
+
+
 def run_c5(args):
     """Adjoint of heterogeneous Terzaghi-type consolidation: 512 x 256 cells
     (arrays 512 x 258 with the boundary rows), 200 Biot steps, each with 4
@@ -660,7 +684,7 @@ def main():
                     help="tx,depth,ctas_per_sm,min_rows,pipeline of the elasticity sweeps (all workloads)")
     ap.add_argument("--adjoint-steps", type=int, default=200)
     ap.add_argument("--fd-directions", type=int, default=32)
-    ap.add_argument("--workload", choices=["darcy", "c1", "c3", "c4", "c5"], default="darcy",
+    ap.add_argument("--workload", choices=["darcy", "c1", "c3", "c4", "c4sweep", "c5"], default="darcy",
                     help="darcy: the headline line; c1/c3/c4/c5: the other configurations (one JSON line each)")
     ap.add_argument("--biot-steps", type=int, default=100)
     ap.add_argument("--instances", type=int, default=512)
@@ -680,6 +704,8 @@ def main():
         return run_c4(args)
     if args.workload == "c5":
         return run_c5(args)
+    if args.workload == "c4sweep":
+        return run_c4sweep(args)
     return run_ours(args)
 
 
