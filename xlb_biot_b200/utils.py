@@ -1,4 +1,8 @@
-"""Unit bookkeeping and field utilities (mirror of ``src/utils.py:17-106``)."""
+"""Unit bookkeeping, field utilities and VTK output (mirror of
+``src/utils.py:17-106,144-196,243-304``)."""
+import os
+import time
+
 import numpy as np
 import torch
 
@@ -96,3 +100,76 @@ def downsample_field(field, factor, method='bicubic'):
     mx = torch.as_tensor(_resize_matrix(nx, nx // factor), dtype=t.dtype, device=t.device)
     my = torch.as_tensor(_resize_matrix(ny, ny // factor), dtype=t.dtype, device=t.device)
     return torch.einsum("ax,xyc,by->abc", mx, t, my)
+
+
+# ---------------------------------------------------------------------------
+# Legacy-VTK output.  The reference writes these files through pyvista
+# (``pv.ImageData(...).save(name, binary=True)``), which is not a dependency
+# here: the same file layout is written directly (legacy VTK, binary,
+# STRUCTURED_POINTS with one more point than cells per axis, one cell-data
+# array per field, x fastest, big-endian).
+# ---------------------------------------------------------------------------
+_VTK_TYPES = {np.dtype(np.float32): "float", np.dtype(np.float64): "double", np.dtype(np.int32): "int",
+              np.dtype(np.int64): "vtktypeint64", np.dtype(np.uint8): "unsigned_char"}
+
+
+def _host(a):
+    if isinstance(a, torch.Tensor):
+        a = a.detach().cpu().numpy()
+    return np.asarray(a)
+
+
+def write_vtk_cells(filename, cell_dims, arrays, title="fields"):
+    """Legacy binary VTK of a uniform grid of ``cell_dims`` cells (2 or 3 ints)
+    with one cell-data array per ``arrays`` entry (name -> array of that shape,
+    or already flat in x-fastest order)."""
+    dims = tuple(int(d) for d in cell_dims) + (1,) * (3 - len(cell_dims))
+    ncell = int(np.prod(dims))
+    with open(filename, "wb") as fh:
+        fh.write(f"# vtk DataFile Version 3.0\n{title}\nBINARY\nDATASET STRUCTURED_POINTS\n".encode())
+        fh.write("DIMENSIONS {} {} {}\n".format(*[d + 1 if d > 1 or i < len(cell_dims) else 1
+                                                  for i, d in enumerate(dims)]).encode())
+        fh.write(b"ORIGIN 0 0 0\nSPACING 1 1 1\n")
+        fh.write(f"CELL_DATA {ncell}\n".encode())
+        for name, a in arrays.items():
+            a = _host(a)
+            if a.dtype == np.bool_:
+                a = a.astype(np.uint8)
+            if a.dtype not in _VTK_TYPES:
+                a = a.astype(np.float64)
+            flat = a.reshape(-1, order="F") if a.ndim > 1 else a.reshape(-1)
+            if flat.size != ncell:
+                raise ValueError(f"field {name!r} has {flat.size} values for {ncell} cells")
+            fh.write(f"SCALARS {name} {_VTK_TYPES[flat.dtype]} 1\nLOOKUP_TABLE default\n".encode())
+            fh.write(flat.astype(flat.dtype.newbyteorder(">")).tobytes())
+            fh.write(b"\n")
+
+
+def save_fields_vtk(timestep, fields, output_dir=".", prefix="fields"):
+    """``src/utils.py:144-196``: every field of ``fields`` (all the same shape,
+    (nx, ny) or (nx, ny, nz)) as cell data of ``<prefix>_<timestep:07d>.vtk``."""
+    shapes = {tuple(np.shape(_host(v))) for v in fields.values()}
+    assert len(shapes) == 1, "All fields must have the same dimensions!"
+    (shape,) = shapes
+    output_filename = os.path.join(output_dir, prefix + "_" + f"{timestep:07d}.vtk")
+    start = time.time()
+    write_vtk_cells(output_filename, shape, fields, title=prefix)
+    print(f"Saved {output_filename} in {time.time() - start:.6f} seconds.")
+
+
+def save_BCs_vtk(timestep, BCs, gridInfo, output_dir="."):
+    """``src/utils.py:243-304``: one boolean cell array per boundary condition
+    (named ``<bc.name>_<k>`` for the k-th BC of that name) in ``BCs_<timestep:07d>.vtk``."""
+    dims = (gridInfo["nx"], gridInfo["ny"]) if gridInfo["nz"] == 0 else \
+        (gridInfo["nx"], gridInfo["ny"], gridInfo["nz"])
+    counts, arrays = {}, {}
+    for bc in BCs:
+        counts[bc.name] = counts.get(bc.name, -1) + 1
+        idx = bc.update_function(timestep)[0] if getattr(bc, "isDynamic", False) else bc.indices
+        mask = np.zeros(dims, dtype=bool)
+        mask[tuple(np.asarray(i) for i in idx)] = True
+        arrays[f"{bc.name}_{counts[bc.name]}"] = mask
+    output_filename = os.path.join(output_dir, "BCs_" + f"{timestep:07d}.vtk")
+    start = time.time()
+    write_vtk_cells(output_filename, dims, arrays, title="BCs")
+    print(f"Saved {output_filename} in {time.time() - start:.6f} seconds.")
