@@ -91,7 +91,8 @@ class CompiledRules:
         """The same rules on a smaller grid: cells outside it are dropped (the
         reference's coarse-level gradient gathers clamp and scatters drop)."""
         keep = (self.cells[:, 0] < nx) & (self.cells[:, 1] < ny) if self.count else np.zeros(0, bool)
-        return CompiledRules(self.q, ny, self.cells[keep], self.code_np[keep], self.cst_np[keep], dtype, device, nx)
+        return CompiledRules(self.q, ny, self.cells[keep], self.code_np[keep], self.cst_np[keep], dtype, device, nx,
+                             push=self.push is not None)
 
 
 def _run(bcs, fout, fin, step, names):
@@ -160,7 +161,9 @@ def compile_rules(bcs, nx, ny, q, dtype, device, step=None, names=None, check=Tr
         if np.any(bad):
             raise NotImplementedError("boundary rule scales a population; not representable")
         code[:, d] = cd
-    rules = CompiledRules(q, ny, cells, code, c0, dtype, device, nx, push=(step == "PostStreaming"))
+    # push words: post-streaming rules (collide-and-push sweep, transposed sweeps)
+    # and the gradient's rules (its transposed stencil gathers the same way)
+    rules = CompiledRules(q, ny, cells, code, c0, dtype, device, nx, push=(step == "PostStreaming" or step is None))
     if check:
         _self_check(bcs, nx, ny, q, step, names, rules)
     return rules

@@ -30,6 +30,26 @@ __device__ __forceinline__ T rule_keep_factor(const RulesView<T, Q>& r, int y, i
     return T(0);
 }
 
+// Factor the adjoint of rule table r passes back through the stream from
+// (zy, zx) for direction d of the cell at (y, x) = (zy, zx) - c_d: with the
+// table's push words (word of the source cell, bit d set when the value was
+// rebuilt at the destination) one coalesced load per cell, else a search.
+template <typename T, int Q>
+__device__ __forceinline__ T gather_factor(const RulesView<T, Q>& r, uint32_t pw, int zy, int zx, int d) {
+    if (r.count == 0) return T(1);
+    if (r.push) return (pw >> d) & 1u ? T(0) : T(1);
+    return rule_keep_factor<T, Q>(r, zy, zx, d);
+}
+
+// Rule index of the cell itself (bitmask probe with push words' bit 16 as a
+// first filter).
+template <typename T, int Q>
+__device__ __forceinline__ int own_rule(const RulesView<T, Q>& r, uint32_t pw, int y, int x) {
+    if (r.count == 0) return -1;
+    if (r.push && !((pw >> 16) & 1u)) return -1;
+    return probe_rule(load_probe(r, y, x), x);
+}
+
 // Adjoint of the rules of one cell applied to v (in place): the adjoint that
 // flows to the rules' source directions is added to src[].
 template <typename T, int Q>
@@ -79,19 +99,19 @@ __global__ void elast_sweep_adjoint_kernel(const ElastAdjArgs<T> p) {
     const size_t o = (size_t)y * G.pitch + x;
     const long long P = G.plane;
     // adjoint of the post-collision populations of this cell
+    const uint32_t pw = p.ps.count > 0 && p.ps.push ? __ldg(p.ps.push + y * G.nx + x) : 0u;
     T lp[8];
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
         const int zx = wrap(x + cx8(i), G.nx), zy = wrap(y + cy8(i), G.ny);
-        T v = __ldg(p.lam_out + (size_t)zy * G.pitch + zx + i * P);
-        if (p.ps.count > 0) v *= rule_keep_factor<T, 8>(p.ps, zy, zx, i);
-        lp[i] = p.b * v;
+        const T v = __ldg(p.lam_out + (size_t)zy * G.pitch + zx + i * P);
+        lp[i] = p.b * (v * gather_factor<T, 8>(p.ps, pw, zy, zx, i));
     }
     T lo[8];
 #pragma unroll
     for (int i = 0; i < 8; ++i) lo[i] = __ldg(p.lam_out + o + i * P);
     if (p.ps.count > 0) {
-        const int r = find_rule(p.ps, y, x);
+        const int r = own_rule<T, 8>(p.ps, pw, y, x);
         if (r >= 0) {   // post-streaming rules of this cell read its own post-collision values
             T v[8], add[8];
 #pragma unroll
@@ -105,7 +125,7 @@ __global__ void elast_sweep_adjoint_kernel(const ElastAdjArgs<T> p) {
     T lge[8];
 #pragma unroll
     for (int i = 0; i < 8; ++i) lge[i] = T(0);
-    if (p.pc.count > 0) rules_transpose<T, 8>(p.pc, find_rule(p.pc, y, x), lp, lge);
+    if (p.pc.count > 0) rules_transpose<T, 8>(p.pc, probe_rule(load_probe(p.pc, y, x), x), lp, lge);
     // rates of this cell
     T lam = p.lam_u, mu = p.mu_u;
     T cs = p.mat.cs, cd = p.mat.cd, h = p.mat.h, n = p.mat.n;
@@ -191,16 +211,16 @@ __global__ void darcy_sweep_adjoint_kernel(const DarcyAdjArgs<T> p) {
     if (x >= G.nx) return;
     const size_t o = (size_t)y * G.pitch + x;
     const long long P = G.plane;
+    const uint32_t pw = p.ps.count > 0 && p.ps.push ? __ldg(p.ps.push + y * G.nx + x) : 0u;
     T lp[9];
 #pragma unroll
     for (int i = 0; i < 9; ++i) {
         const int zx = wrap(x + cx9(i), G.nx), zy = wrap(y + cy9(i), G.ny);
-        T v = __ldg(p.lam_out + (size_t)zy * G.pitch + zx + i * P);
-        if (p.ps.count > 0) v *= rule_keep_factor<T, 9>(p.ps, zy, zx, i);
-        lp[i] = v;
+        const T v = __ldg(p.lam_out + (size_t)zy * G.pitch + zx + i * P);
+        lp[i] = v * gather_factor<T, 9>(p.ps, pw, zy, zx, i);
     }
     if (p.ps.count > 0) {
-        const int r = find_rule(p.ps, y, x);
+        const int r = own_rule<T, 9>(p.ps, pw, y, x);
         if (r >= 0) {
             T v[9], add[9];
 #pragma unroll
@@ -213,7 +233,7 @@ __global__ void darcy_sweep_adjoint_kernel(const DarcyAdjArgs<T> p) {
     T lge[9];
 #pragma unroll
     for (int i = 0; i < 9; ++i) lge[i] = T(0);
-    if (p.pc.count > 0) rules_transpose<T, 9>(p.pc, find_rule(p.pc, y, x), lp, lge);
+    if (p.pc.count > 0) rules_transpose<T, 9>(p.pc, probe_rule(load_probe(p.pc, y, x), x), lp, lge);
     const T om = p.omega_f ? __ldg(p.omega_f + o) : p.omega;
     T W = T(0);
 #pragma unroll
@@ -242,17 +262,17 @@ __global__ void gradient_adjoint_kernel(SweepGeom G, const T* lg, T scale, Rules
     if (x >= G.nx) return;
     const size_t o = (size_t)y * G.pitch + x;
     T acc = T(0);
+    const uint32_t pw = rules.count > 0 && rules.push ? __ldg(rules.push + y * G.nx + x) : 0u;
 #pragma unroll
     for (int d = 1; d < 9; ++d) {
         const int zx = wrap(x + cx9(d), G.nx), zy = wrap(y + cy9(d), G.ny);
         const size_t oz = (size_t)zy * G.pitch + zx;
         const T k = T(-3) * scale * w9<T>(d);
-        T v = k * (T(cx9(d)) * __ldg(lg + oz) + T(cy9(d)) * __ldg(lg + oz + G.plane));
-        if (rules.count > 0) v *= rule_keep_factor<T, 9>(rules, zy, zx, d);
-        acc += v;
+        const T v = k * (T(cx9(d)) * __ldg(lg + oz) + T(cy9(d)) * __ldg(lg + oz + G.plane));
+        acc += v * gather_factor<T, 9>(rules, pw, zy, zx, d);
     }
     if (rules.count > 0) {
-        const int r = find_rule(rules, y, x);
+        const int r = own_rule<T, 9>(rules, pw, y, x);
         if (r >= 0) {   // rules of this cell whose source is q(x) itself
             const T gx = __ldg(lg + o), gy = __ldg(lg + o + G.plane);
 #pragma unroll
@@ -343,18 +363,18 @@ __global__ void divgrad_adjoint_kernel(SweepGeom G, ElastMat<T> mat, T lam_u, T 
     const size_t o = (size_t)y * G.pitch + x;
     const long long P = G.plane;
     T acc = T(0);                       // (G^T lam_ext)(x), as gradient_adjoint_kernel
+    const uint32_t pw = rules.count > 0 && rules.push ? __ldg(rules.push + y * G.nx + x) : 0u;
 #pragma unroll
     for (int d = 1; d < 9; ++d) {
         const int zx = wrap(x + cx9(d), G.nx), zy = wrap(y + cy9(d), G.ny);
         const size_t oz = (size_t)zy * G.pitch + zx;
         const T k = T(-3) * scale * w9<T>(d);
-        T v = k * (T(cx9(d)) * __ldg(lg + oz) + T(cy9(d)) * __ldg(lg + oz + P));
-        if (rules.count > 0) v *= rule_keep_factor<T, 9>(rules, zy, zx, d);
-        acc += v;
+        const T v = k * (T(cx9(d)) * __ldg(lg + oz) + T(cy9(d)) * __ldg(lg + oz + P));
+        acc += v * gather_factor<T, 9>(rules, pw, zy, zx, d);
     }
     const T gx = __ldg(lg + o), gy = __ldg(lg + o + P);
     if (rules.count > 0) {
-        const int r = find_rule(rules, y, x);
+        const int r = own_rule<T, 9>(rules, pw, y, x);
         if (r >= 0) {
 #pragma unroll
             for (int d = 0; d < 9; ++d) {
