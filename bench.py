@@ -454,6 +454,29 @@ def run_c3(args):
     eta = sim.elasticity.update_macroscopic(out[0])[0].double().cpu().numpy()
     eta_r = ref[0].elasticity.update_macroscopic(ref[1][0])[0].cpu().numpy()
     p, p_r = out[5].double().cpu().numpy(), ref[1][5].cpu().numpy()
+    # roofline of the dominant kernel, the level-0 FP32 damped smoothing sweep
+    # (collide and push): 8 populations read and written plus the coupling
+    # force's 2 planes (and 2 for a static body force), 4 B each.  Its operands
+    # (~75 MB) fit in L2, so L2 is flushed before each timed sweep by reading a
+    # 256 MB buffer (clean lines: no write-back inside the timed sweep) and
+    # each sweep is timed alone: the HBM-bound figure
+    el = sim.elasticity
+    L0 = el._L(0)
+    f0, ext, buf = out[0], L0.zeros(2), L0.empty(8)
+    planes = 8 + 8 + 2 + (2 if el.force is not None else 0)
+    flush = torch.ones(64 << 20, dtype=torch.float32, device=f0.device)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(23)]
+    for e0, e1 in evs:
+        flush.sum()
+        e0.record()
+        el._sweep(f0, 0, 1.0 - el.gamma, el.gamma, fext=ext, out=buf)
+        e1.record()
+    torch.cuda.synchronize()
+    t_sw = sum(e0.elapsed_time(e1) for e0, e1 in evs[3:]) * 1e-3      # 3 warm-up sweeps
+    del flush
+    (_, t_warm) = _timed(lambda: [el._sweep(f0, 0, 1.0 - el.gamma, el.gamma, fext=ext, out=buf) for _ in range(20)])
+    peak, peak_kind = measured_peak_hbm()
+    sweep_gbs = n * n * planes * 4 / (t_sw / 20) / 1e9
     line = {"workload": "c3_periodic_biot_1024x1024_mg5", "metric": "GLUPS", "value": lus / secs / 1e9,
             "unit": "GLUPS", "biot_steps": steps, "vcycles": cycles, "lattice_updates": lus,
             "seconds": secs, "dtype": "f32 elasticity, f64 coarsest level, f64 pressure",
@@ -462,7 +485,12 @@ def run_c3(args):
             "launch": "one CUDA graph replay per coupled step",
             "rel_err_u_vs_fp64": float(np.linalg.norm(eta - eta_r) / np.linalg.norm(eta_r)),
             "rel_err_p_vs_fp64": float(np.linalg.norm(p - p_r) / np.linalg.norm(p_r)),
-            "fp64": {"seconds": ref[3], "vcycles": ref[2]}}
+            "fp64": {"seconds": ref[3], "vcycles": ref[2]},
+            "roofline": {"kernel": "level-0 FP32 smoothing sweep (collide and push)", "bound": "hbm",
+                         "achieved": sweep_gbs, "peak": peak, "unit": "GB/s", "frac": sweep_gbs / peak,
+                         "peak_kind": peak_kind, "bytes_per_cell": planes * 4, "ms_per_sweep": t_sw / 20 * 1e3,
+                         "l2": "flushed (read) before each timed sweep",
+                         "ms_per_sweep_back_to_back": t_warm / 20 * 1e3}}
     print(json.dumps(line), flush=True)
     return 0
 

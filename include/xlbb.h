@@ -79,7 +79,9 @@ typedef struct {
  *      pitch, otherwise pipeline 0 is used);
  *   2: independent warps of 30 output columns (tx ignored), post-collision
  *      rows in registers, streaming by warp shuffles, no barrier; register
- *      prefetch of depth (1, 2) rows; ctas_per_sm counts CTAs of 4 warps.
+ *      prefetch of depth (1, 2) rows; ctas_per_sm counts CTAs of 4 warps;
+ *   3: collide and push (the default): one thread per cell, CTAs of tx
+ *      columns of one row; depth, ctas_per_sm and min_rows are not used.
  * FP64 sweeps cap tx at 128.
  */
 typedef struct {
@@ -225,7 +227,8 @@ int xlbb_prolong_add(int dtype_fine, int dtype_coarse, const XlbbGrid* fine, con
  * xlbb_batch_upload converts host instance records into the device
  * descriptor array `dev` (xlbb_batch_desc_bytes(dtype) bytes each; the caller
  * owns it).  A sweep runs every tile of `tiles_dev`: tile = (instance, x0,
- * row range), CTAs of 128 owned columns looping over the list; the algebra is
+ * row range), CTAs of 128 owned columns looping over the list (`ctas` is an
+ * upper bound: at most one wave of resident CTAs is launched); the algebra is
  * the one of xlbb_elast_sweep (out = a f + b STEP(f - resid)); tile_sumsq (one
  * double per tile, or NULL) receives sum(out^2) / sum((out - f_in)^2), reduced
  * per instance by xlbb_segment_sum over tile ranges begin[i]..begin[i+1].
