@@ -520,8 +520,8 @@ def run_c4(args):
     lu = b.lattice_updates_per_cycle() * cycles
     # roofline of the batched kernel: level-0 smoothing sweeps of the whole batch
     # (72 B per cell: 8 populations read and written, 2 force planes, FP32)
-    ln = b.smooth_xy[0][0]
-    (_, t_sw) = _timed(lambda: [b._sweep(0, ln, 1.0 - b.gamma, b.gamma) for _ in range(20)])
+    lns = b.smooth_xy[0]
+    (_, t_sw) = _timed(lambda: [b._sweep(0, ln, 1.0 - b.gamma, b.gamma) for _ in range(20) for ln in lns])
     cells0 = sum(nx * ny for nx, ny in sizes)
     peak, peak_kind = measured_peak_hbm()
     sweep_gbs = cells0 * 72 / (t_sw / 20) / 1e9
@@ -572,14 +572,21 @@ def run_c4(args):
             "launches_per_vcycle": b.launches_per_cycle,
             "batched_sweep_roofline": {"bound": "hbm", "achieved": sweep_gbs, "peak": peak, "unit": "GB/s",
                                        "frac": sweep_gbs / peak, "peak_kind": peak_kind,
-                                       "kernel": "xlbb::batched_push_kernel<float> (level-0 smoothing sweep, "
-                                                 "all 512 instances, 72 B/LU)", "sweep_ms": t_sw / 20 * 1e3},
+                                       "kernel": batched_kernel_name(lns) + " (level-0 smoothing sweep, "
+                                                 "all instances, 72 B/LU)", "sweep_ms": t_sw / 20 * 1e3},
             "dtype": "f32 storage and smoothing, f64 level-0 residual arithmetic, f64 coarsest level and norms",
             "levels": "per instance: coarsest side 3-4 cells (5 to 8 levels)",
             "material": "mu in [0.5, 2] / 16, nu in [0.1, 0.4] (lattice lambda + mu <= 0.29: the D2Q8 "
                         "model is singular at 1/3 and the reference's V-cycle diverges for moduli of order 1)"}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def batched_kernel_name(launches):
+    """Kernel(s) of a list of FP32 batched sweep launches."""
+    names = sorted({"xlbb::batched_push4_kernel<float>" if ln.vec else "xlbb::batched_push_kernel<float>"
+                    for ln in launches})
+    return " + ".join(names)
 
 
 def run_c4sweep(args):
@@ -592,14 +599,16 @@ def run_c4sweep(args):
     sizes, lams, mus, forces = batch_instances(count=args.instances)
     b = BatchedElasticity(sizes, lams, mus, forces, levels="auto", precision="f32/f32", coarsest_precision="f64",
                           residual_precision="f64")
-    ln = b.smooth_xy[0][0]
+    lns = b.smooth_xy[0]
     for _ in range(max(3, args.warmup)):
-        b._sweep(0, ln, 0.25, 0.75)
-    (_, t) = _timed(lambda: [b._sweep(0, ln, 0.25, 0.75) for _ in range(args.steps)])
+        for ln in lns:
+            b._sweep(0, ln, 0.25, 0.75)
+    (_, t) = _timed(lambda: [b._sweep(0, ln, 0.25, 0.75) for _ in range(args.steps) for ln in lns])
     cells = sum(nx * ny for nx, ny in sizes)
     peak, peak_kind = measured_peak_hbm()
     gbs = cells * 72 / (t / args.steps) / 1e9
     print(json.dumps({"workload": "c4_batched_level0_sweep", "metric": "GB/s", "value": gbs, "unit": "GB/s",
+                      "kernel": batched_kernel_name(lns), "launches_per_sweep": len(lns),
                       "cells": cells, "sweeps": args.steps, "ms_per_sweep": t / args.steps * 1e3,
                       "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
                                    "frac": gbs / peak, "peak_kind": peak_kind}}), flush=True)

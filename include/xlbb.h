@@ -92,7 +92,8 @@ int xlbb_sweep_set_config(int kernel, const XlbbSweepConfig* cfg);
 int xlbb_sweep_get_config(int kernel, XlbbSweepConfig* cfg);
 
 /* Device status word of the kernels' bounded waits (0, or XLBB_ETIMEOUT if a
- * wait gave up); synchronous; reset != 0 clears it. */
+ * wait gave up; XLBB_EBADARG if xlbb_batched_elast_sweep4 skipped an instance
+ * that does not qualify); synchronous; reset != 0 clears it. */
 int xlbb_device_status(int* status, int reset);
 
 typedef struct {
@@ -259,6 +260,18 @@ int xlbb_batch_upload(int dtype, const XlbbBatchInstance* host, int ninst, void*
 int xlbb_batched_elast_sweep(int dtype, const void* inst_dev, const XlbbBatchTile* tiles_dev, int ntiles,
                              int ctas, double a, double b, int use_force, int has_resid, int sumsq_diff,
                              double* tile_sumsq, void* stream);
+/*
+ * The same sweep by the four-column kernel (dtype XLBB_F32 only): a warp
+ * takes a tile row, a lane four adjacent columns, with
+ * 16-byte loads and stores and streaming along x by warp shuffles.  Every
+ * instance must store FP32 with nx, pitch and plane multiples of 4 and 16-byte
+ * aligned planes (xlbb_batch_upload records whether it does); the tiles of one
+ * that does not are skipped and the device status word is set to
+ * XLBB_EBADARG.  Results equal xlbb_batched_elast_sweep's.
+ */
+int xlbb_batched_elast_sweep4(int dtype, const void* inst_dev, const XlbbBatchTile* tiles_dev, int ntiles,
+                              int ctas, double a, double b, int use_force, int has_resid, int sumsq_diff,
+                              double* tile_sumsq, void* stream);
 int xlbb_batched_restrict(int dtype_fine, int dtype_coarse, const XlbbBatchTransfer* tr_dev, int ninst,
                           void* stream);
 int xlbb_batched_prolong_add(int dtype_fine, int dtype_coarse, const XlbbBatchTransfer* tr_dev, int ninst,

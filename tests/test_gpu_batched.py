@@ -118,7 +118,7 @@ def test_batched_push_and_row_marching_identical(prec):
         for shape in ((256, 1, 3, 8, 0), (128, 1, 1, 8, 3)):
             autotune.set_config(autotune.ELASTICITY, *shape)
             b = BatchedElasticity(sizes, lams, mus, forces, levels="auto", precision=prec, coarsest_precision="f64",
-                                  residual_precision="f64")
+                                  residual_precision="f64", vectorized=False)
             b.reset()
             for _ in range(3):
                 b.vcycle()
@@ -128,3 +128,60 @@ def test_batched_push_and_row_marching_identical(prec):
     for x, y in zip(out[0][0], out[1][0]):
         assert torch.equal(x, y)
     assert torch.allclose(out[0][1], out[1][1], rtol=1e-12, atol=0) and torch.equal(out[0][2], out[1][2])
+
+
+def _mixed_batch(seed=5):
+    """Widths on one tile (64, 96, 24), on several (192, 256) and with a short
+    last tile (136 = 128 + 8); coarse levels of 24 (6, 3) and of 136 (34, 17)
+    are not multiples of 4 and stay on the one-column kernel."""
+    rng = np.random.default_rng(seed)
+    sizes = [(64, 40), (192, 64), (256, 32), (96, 48), (24, 24), (136, 72)]
+    mus = rng.uniform(0.5, 2.0, len(sizes)) / 16.0
+    nus = rng.uniform(0.1, 0.4, len(sizes))
+    lams = 2 * mus * nus / (1 - nus)
+    forces = [1e-3 * rng.standard_normal((nx, ny, 2)) for nx, ny in sizes]
+    return sizes, lams, mus, forces
+
+
+@pytest.mark.parametrize("rp", [None, "f64"])
+def test_batched_four_column_kernel_identical(rp):
+    """xlbb_batched_elast_sweep4 (four columns per lane, shuffles along x) and
+    the one-column batched sweep give bit-identical V-cycles: populations and
+    correction norms; the residual norms group their FP64 partials differently."""
+    from xlb_biot_b200.batched import BatchedElasticity
+    sizes, lams, mus, forces = _mixed_batch()
+    out = []
+    for vec in (False, True):
+        b = BatchedElasticity(sizes, lams, mus, forces, levels="auto", precision="f32/f32", coarsest_precision="f64",
+                              residual_precision=rp, vectorized=vec)
+        assert any(ln.vec for lns in b.smooth_xy for ln in lns) == vec
+        b.reset()
+        for _ in range(3):
+            b.vcycle()
+        out.append(([b.populations(i).clone() for i in range(len(sizes))], b.norm2.clone(), b.corr2.clone()))
+    for i, (x, y) in enumerate(zip(out[0][0], out[1][0])):
+        assert torch.equal(x, y), i
+    assert torch.allclose(out[0][1], out[1][1], rtol=1e-12, atol=0) and torch.equal(out[0][2], out[1][2])
+
+
+def test_four_column_kernel_skips_instances_that_do_not_qualify():
+    """An instance whose width is not a multiple of 4, given to the four-column
+    entry point, is skipped (its output untouched) and the device status word
+    reports XLBB_EBADARG."""
+    import ctypes
+    from xlb_biot_b200 import _lib, autotune
+    from xlb_biot_b200.batched import BatchedElasticity
+    sizes = [(34, 34)]
+    b = BatchedElasticity(sizes, [0.05], [0.05], [np.zeros((34, 34, 2))], levels=2, precision="f32/f32")
+    ln = b.smooth_xy[0][0]
+    assert not ln.vec
+    dst = b.Y[0][torch.float32].view(0)
+    dst.fill_(7.0)
+    autotune.device_status(reset=True)
+    lib = _lib.lib()
+    _lib.check(lib.xlbb_batched_elast_sweep4(ln.dcode, ctypes.c_void_p(ln.desc.data_ptr()),
+                                             ctypes.c_void_p(ln.tiles.data_ptr()), ln.ntiles, ln.ctas, 0.25, 0.75,
+                                             1, 0, 0, None, _lib.stream_ptr()), "xlbb_batched_elast_sweep4")
+    torch.cuda.synchronize()
+    assert autotune.device_status(reset=True) == -1        # XLBB_EBADARG
+    assert bool((dst == 7.0).all())

@@ -71,10 +71,12 @@ class _Arena:
 
 
 class _Launch:
-    """Descriptor array + tile work list of one batched sweep launch."""
+    """Descriptor array + tile work list of one batched sweep launch; ``vec``:
+    every instance qualifies for the four-column kernel."""
 
-    def __init__(self, desc, tiles, ntiles, ctas, dcode, begin=None):
+    def __init__(self, desc, tiles, ntiles, ctas, dcode, begin=None, vec=False):
         self.desc, self.tiles, self.ntiles, self.ctas, self.dcode, self.begin = desc, tiles, ntiles, ctas, dcode, begin
+        self.vec = vec
 
 
 class BatchedElasticity:
@@ -88,10 +90,12 @@ class BatchedElasticity:
     ``MG_relaxation``, ``MG_n_smoothing`` (k_smooth even).
     ``coarsest_precision="f64"`` runs each instance's coarsest level in FP64;
     ``residual_precision="f64"`` computes the level-0 residual sweep of an FP32
-    batch in FP64 arithmetic (FP32 storage)."""
+    batch in FP64 arithmetic (FP32 storage).  ``vectorized``: FP32 launches
+    whose instances all have widths divisible by 4 use the four-column kernel
+    (``xlbb_batched_elast_sweep4``; same results)."""
 
     def __init__(self, sizes, lams, mus, forces, levels=5, gamma=0.75, k_smooth=2, precision="f32/f32",
-                 coarsest_precision=None, residual_precision=None, strip_rows=16, ctas_per_sm=4):
+                 coarsest_precision=None, residual_precision=None, strip_rows=16, ctas_per_sm=4, vectorized=True):
         _lib.require_cuda()
         lib = _lib.lib()
         if k_smooth % 2:
@@ -170,13 +174,23 @@ class BatchedElasticity:
                 begin.append(len(tl))
             tiles = torch.as_tensor(np.asarray(tl, dtype=np.int32).reshape(-1), device=dev)
             b = torch.as_tensor(np.asarray(begin, dtype=np.int32), device=dev) if want_begin else None
-            return _Launch(desc, tiles, len(tl), min(len(tl), ctas_per_sm * sms), code, b)
+            # four-column kernel: FP32 (storage and arithmetic), widths (and so pitches and planes) multiples of 4
+            vec = vectorized and code == _lib.XLBB_F32 and all(self.shapes[l][g][0] % 4 == 0 for g in ids)
+            return _Launch(desc, tiles, len(tl), min(len(tl), ctas_per_sm * sms), code, b, vec)
 
         # smoothing launches (X->Y, Y->X) per level and dtype group; residual launch per level
+        # (FP32 groups split into the instances the four-column kernel takes and the rest)
         self.smooth_xy, self.smooth_yx, self.res = [], [], []
         for l in range(self.levels):
-            self.smooth_xy.append([launch(l, ids, d, self.X[l][d], self.Y[l][d]) for d, ids in self.groups[l].items()])
-            self.smooth_yx.append([launch(l, ids, d, self.Y[l][d], self.X[l][d]) for d, ids in self.groups[l].items()])
+            parts = []
+            for d, ids in self.groups[l].items():
+                if vectorized and d == torch.float32:
+                    q4 = [g for g in ids if self.shapes[l][g][0] % 4 == 0]
+                    parts += [(d, p) for p in (q4, [g for g in ids if g not in set(q4)]) if p]
+                else:
+                    parts.append((d, ids))
+            self.smooth_xy.append([launch(l, ids, d, self.X[l][d], self.Y[l][d]) for d, ids in parts])
+            self.smooth_yx.append([launch(l, ids, d, self.Y[l][d], self.X[l][d]) for d, ids in parts])
             if l < self.levels - 1:
                 acc64 = l == 0 and residual_precision == "f64" and dt == torch.float32
                 self.res.append(launch(l, self.deeper[l], dt, self.X[l][dt], self.RES[l], want_begin=(l == 0),
@@ -218,11 +232,11 @@ class BatchedElasticity:
 
     # ------------------------------------------------------------------ kernels
     def _sweep(self, l, ln, a, b, sumsq=False):
-        _lib.check(_lib.lib().xlbb_batched_elast_sweep(
+        fn = "xlbb_batched_elast_sweep4" if ln.vec else "xlbb_batched_elast_sweep"
+        _lib.check(getattr(_lib.lib(), fn)(
             ln.dcode, ctypes.c_void_p(ln.desc.data_ptr()), ctypes.c_void_p(ln.tiles.data_ptr()), ln.ntiles, ln.ctas,
             float(a), float(b), 1 if l == 0 else 0, 1 if l > 0 else 0, 0,
-            ctypes.c_void_p(self.tile_sumsq.data_ptr()) if sumsq else None, _lib.stream_ptr()),
-            "xlbb_batched_elast_sweep")
+            ctypes.c_void_p(self.tile_sumsq.data_ptr()) if sumsq else None, _lib.stream_ptr()), fn)
         self.launches_per_cycle += 1
 
     def _smooth(self, l):

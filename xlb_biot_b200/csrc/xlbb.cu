@@ -118,12 +118,17 @@ __device__ __forceinline__ void elast_collide(const T (&f)[8], bool hasF, T F0, 
     const T m2 = f[0] + f[1] + f[2] + f[3] + T(2) * (f[4] + f[5] + f[6] + f[7]);
     const T m3 = f[0] - f[1] + f[2] - f[3];
     const T m4 = f[4] - f[5] + f[6] - f[7];
-    T M0 = m0, M1 = m1, M5 = m0 / T(3), M6 = m1 / T(3);
+    // thirds and sixths by multiplication with the rounded constants (one
+    // rounding each, like the division, at a fraction of its instructions);
+    // the sums with one explicit fused multiply-add, so that every kernel
+    // rounds them alike
+    constexpr T third = T(1.0 / 3.0), sixth = T(1.0 / 6.0);
+    T M0 = m0, M1 = m1, M5 = third * m0, M6 = third * m1;
     if (hasF) {
         M0 = m0 + F0;
         M1 = m1 + F1;
-        M5 = m0 / T(3) + F0 / T(6);
-        M6 = m1 / T(3) + F1 / T(6);
+        M5 = fma(sixth, F0, M5);
+        M6 = fma(sixth, F1, M6);
     }
     const T M2 = m2 * cs, M3 = m3 * cd, M4 = m4 * cd;
     o[0] = T(0.5) * M0 + h * M2 + T(0.25) * M3 - T(0.5) * M5;
@@ -246,7 +251,7 @@ struct ElastPhys {
         T v = s;
         T fz = T(0);
         if (p.mix || (SUMSQ && p.sumsq_diff)) fz = T(__ldg(p.ip[i] + o));
-        if (p.mix) v = p.a * fz + p.b * s;
+        if (p.mix) v = mix_ab(p.a, fz, p.b, s);
         const S_ sv = S_(v);
         p.op[i][o] = sv;
         if constexpr (SUMSQ) {
@@ -278,7 +283,7 @@ struct ElastPhys {
         for (int i = 0; i < 8; ++i) {
             T v = S[i];
             if constexpr (PREV) {
-                if (p.mix) v = p.a * fprev[i] + p.b * S[i];
+                if (p.mix) v = mix_ab(p.a, fprev[i], p.b, S[i]);
             }
             const S_ sv = S_(v);
             p.op[i][o] = sv;
@@ -854,6 +859,7 @@ struct BatchInst {
     const S* resid;
     SweepGeom geom;
     T cs, cd, h, n;
+    int vec4;   // FP32 storage, nx / pitch / plane multiples of 4, 16-byte aligned planes
 };
 
 template <typename T, typename S = T>
@@ -865,6 +871,9 @@ static BatchInst<T, S> to_batch_inst(const XlbbBatchInstance& s) {
     b.resid = static_cast<const S*>(s.resid);
     b.geom = SweepGeom{s.nx, s.ny, s.pitch, s.plane};
     elast_rates<T>(T(s.lam), T(s.mu), b.cs, b.cd, b.h, b.n);
+    auto a16 = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
+    b.vec4 = sizeof(S) == 4 && s.nx % 4 == 0 && s.pitch % 4 == 0 && s.plane % 4 == 0 && a16(s.f_in) &&
+             a16(s.f_out) && a16(s.force) && a16(s.resid);
     return b;
 }
 
@@ -907,28 +916,71 @@ batched_elast_kernel(const BatchInst<T, S>* __restrict__ inst, const XlbbBatchTi
     }
 }
 
+// Volatile shared loads: a value read this way is not kept in a register
+// beyond its use (the compiler can neither merge nor hoist the reads).
+__device__ __forceinline__ unsigned long long lds64(const void* p) {
+    unsigned long long v;
+    asm volatile("ld.shared.u64 %0, [%1];" : "=l"(v) : "r"(smem_u32(p)));
+    return v;
+}
+__device__ __forceinline__ unsigned lds32(const void* p) {
+    unsigned v;
+    asm volatile("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"(smem_u32(p)));
+    return v;
+}
+template <typename T>
+__device__ __forceinline__ T ldsT(const T* p) {
+    if constexpr (sizeof(T) == 4) return __uint_as_float(lds32(p));
+    else return __longlong_as_double((long long)lds64(p));
+}
+template <typename P_>
+__device__ __forceinline__ P_* ldsP(P_* const* p) { return reinterpret_cast<P_*>(lds64(p)); }
+
+// A warp's copy of its current tile and that tile's instance record, in
+// shared memory: lane 0 fetches it once per tile, every lane reads the fields
+// it needs with volatile shared loads right where it uses them.
+template <typename T, typename S>
+struct __align__(16) TileRec {
+    const S* fi;
+    S* fo;
+    const S* fc;
+    const S* rs;
+    unsigned P;      // plane stride (the upload checks 8 planes fit in 32-bit offsets)
+    int pitch, nx, ny;
+    int x0, ys, ye, pad;
+    T cs, cd, h, n;
+};
+
 // One cell of the batched collide-and-push sweep (periodic, no boundary rules):
-// the arithmetic of ElastPhys's load / collide / put with the instance record
-// held in a few registers: plane i of a cell at offset o is base + (i * P + o),
-// 32-bit offsets (the upload checks the 8 planes fit), so no per-plane pointer
-// table stays live across the row loop.
+// the arithmetic of ElastPhys's load / collide / put; plane i of the cell at
+// offset o is fi + (i * P + o).
 template <typename T, bool RESID, bool SUMSQ, typename S>
-__device__ __forceinline__ double batched_push_cell(const S* __restrict__ fi, S* __restrict__ fo,
-                                                    const S* __restrict__ fc, const S* __restrict__ rs, unsigned P,
-                                                    int pitch, int nx, int ny, T cs, T cd, T h, T n, T a, T b,
-                                                    int mix, int sumsq_diff, int y, int x) {
-    const unsigned o = unsigned(y * pitch + x);
+__device__ __forceinline__ double batched_push_cell(const TileRec<T, S>* r, T a, T b, int mix, int sumsq_diff, int y,
+                                                    int x) {
     T g[8];
-#pragma unroll
-    for (unsigned i = 0; i < 8; ++i) g[i] = T(__ldg(fi + (o + i * P)));
-    if constexpr (RESID) {
-#pragma unroll
-        for (unsigned i = 0; i < 8; ++i) g[i] = g[i] - T(__ldg(rs + (o + i * P)));
-    }
     T F0 = T(0), F1 = T(0);
-    if (fc) { F0 = T(__ldg(fc + o)); F1 = T(__ldg(fc + (o + P))); }
+    bool hasF;
+    {
+        const S* fi = ldsP(&r->fi);
+        const unsigned P = lds32(&r->P);
+        const unsigned o = unsigned(y * (int)lds32(&r->pitch) + x);
+#pragma unroll
+        for (unsigned i = 0; i < 8; ++i) g[i] = T(__ldg(fi + (o + i * P)));
+        if constexpr (RESID) {
+            const S* rs = ldsP(&r->rs);
+#pragma unroll
+            for (unsigned i = 0; i < 8; ++i) g[i] = g[i] - T(__ldg(rs + (o + i * P)));
+        }
+        const S* fc = ldsP(&r->fc);
+        hasF = fc != nullptr;
+        if (fc) { F0 = T(__ldg(fc + o)); F1 = T(__ldg(fc + (o + P))); }
+    }
     T fs[8];
-    elast_collide<T>(g, fc != nullptr, F0, F1, cs, cd, h, n, fs);
+    elast_collide<T>(g, hasF, F0, F1, ldsT(&r->cs), ldsT(&r->cd), ldsT(&r->h), ldsT(&r->n), fs);
+    const int pitch = (int)lds32(&r->pitch), nx = (int)lds32(&r->nx), ny = (int)lds32(&r->ny);
+    const unsigned P = lds32(&r->P);
+    const S* fi = ldsP(&r->fi);
+    S* fo = ldsP(&r->fo);
     const int rm = (y == 0 ? ny - 1 : y - 1) * pitch, r0 = y * pitch, rp = (y == ny - 1 ? 0 : y + 1) * pitch;
     const int xm = x == 0 ? nx - 1 : x - 1, xp = x == nx - 1 ? 0 : x + 1;
     double acc = 0.0;
@@ -939,7 +991,7 @@ __device__ __forceinline__ double batched_push_cell(const S* __restrict__ fi, S*
         T v = fs[i];
         T fz = T(0);
         if (mix || (SUMSQ && sumsq_diff)) fz = T(__ldg(fi + oz));
-        if (mix) v = a * fz + b * fs[i];
+        if (mix) v = mix_ab(a, fz, b, fs[i]);
         const S sv = S(v);
         fo[oz] = sv;
         if constexpr (SUMSQ) {
@@ -953,33 +1005,244 @@ __device__ __forceinline__ double batched_push_cell(const S* __restrict__ fi, S*
 
 // Collide-and-push form of the batched sweep: a block of 128 x 8 threads takes
 // a tile, thread (tx, ty) its column x0 + tx and every 8th row from ys + ty
-// (independent cells: no barrier); with SUMSQ one FP64 partial per tile.
-// Measured on B200 (512 instances, 26 M cells): this form with one resident
-// wave of 1024-thread CTAs beat 512- and 256-thread CTAs held to 40 registers
-// (more CTAs per SM, fewer loads in flight per thread), two rows per thread
-// loaded before either is collided (register spills), and taller tiles.
+// (independent cells: no block barrier); with SUMSQ one FP64 partial per tile.
+// Measured on B200 (512 instances, 26 M cells, level-0 smoothing sweep): the
+// record in shared memory beat every thread loading it into registers by 15%;
+// CTAs held to 32 or 40 registers for more CTAs per SM, two rows per thread
+// loaded before either is collided, a cp.async prefetch of the next tile's
+// record, and taller tiles were all slower.  The explicit minimum of one CTA
+// per SM lets the compiler keep up to 64 registers per thread (more loads in
+// flight per thread), which measured faster than its 32-register choice.
 template <typename T, bool RESID, bool SUMSQ, typename S = T>
-__global__ void __launch_bounds__(1024)
+__global__ void __launch_bounds__(1024, 1)
 batched_push_kernel(const BatchInst<T, S>* __restrict__ inst, const XlbbBatchTile* __restrict__ tiles, int ntiles,
                     T a, T b, int mix, int use_force, int sumsq_diff, double* tile_sumsq) {
     __shared__ double red[32];
+    __shared__ TileRec<T, S> rec[32];
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    TileRec<T, S>* r = rec + (tid >> 5);
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        const XlbbBatchTile tl = tiles[t];
-        const BatchInst<T, S>& I = inst[tl.inst];
-        const int nx = I.geom.nx, ny = I.geom.ny, pitch = I.geom.pitch;
-        const unsigned P = (unsigned)I.geom.plane;
-        const S* fi = I.f_in;
-        S* fo = I.f_out;
-        const S* fc = use_force ? I.force : nullptr;
-        const S* rs = RESID ? I.resid : nullptr;
-        const T cs = I.cs, cd = I.cd, h = I.h, n = I.n;
-        const int x = tl.x0 + threadIdx.x;
+        __syncwarp();                 // every lane is done with the previous record
+        if ((tid & 31) == 0) {
+            const XlbbBatchTile tl = tiles[t];
+            const BatchInst<T, S>& I = inst[tl.inst];
+            r->fi = I.f_in;
+            r->fo = I.f_out;
+            r->fc = use_force ? I.force : nullptr;
+            r->rs = RESID ? I.resid : nullptr;
+            r->P = (unsigned)I.geom.plane;
+            r->pitch = I.geom.pitch;
+            r->nx = I.geom.nx;
+            r->ny = I.geom.ny;
+            r->x0 = tl.x0;
+            r->ys = tl.ys;
+            r->ye = tl.ye;
+            r->cs = I.cs;
+            r->cd = I.cd;
+            r->h = I.h;
+            r->n = I.n;
+        }
+        __syncwarp();
+        const int x = (int)lds32(&r->x0) + threadIdx.x;
         double acc = 0.0;
-        if (x < nx)
-            for (int y = tl.ys + threadIdx.y; y < tl.ye; y += blockDim.y)
-                acc += batched_push_cell<T, RESID, SUMSQ, S>(fi, fo, fc, rs, P, pitch, nx, ny, cs, cd, h, n, a, b,
-                                                             mix, sumsq_diff, y, x);
+        if (x < (int)lds32(&r->nx))
+            for (int y = (int)lds32(&r->ys) + threadIdx.y; y < (int)lds32(&r->ye); y += blockDim.y)
+                acc += batched_push_cell<T, RESID, SUMSQ, S>(r, a, b, mix, sumsq_diff, y, x);
         if constexpr (SUMSQ) {   // the tile's writes: every output of the instance is written once
+            const double s = block_sum_2d(acc, red);
+            if (threadIdx.x == 0 && threadIdx.y == 0) tile_sumsq[t] = s;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Four-column form of the batched sweep (FP32 storage): a warp takes one row
+// of a 128-column tile, lane c the columns x0 + 4c .. x0 + 4c + 3, with float4
+// loads and stores of every plane.  Streaming along x moves the values that
+// cross a 4-column chunk between lanes by shuffles, so each destination chunk
+// is written with one aligned float4 store; the mixing reads of the row's own
+// directions (c_y = 0) are the lane's own inputs.  Where an instance spans
+// several tiles, the one value of a direction that crosses a tile edge is
+// written by its pusher with a scalar store, and the receiving lane writes the
+// other three values of its chunk: every output is written exactly once, with
+// the arithmetic of the scalar sweep.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float4 ldg4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
+
+template <typename T>
+__device__ __forceinline__ T mixv(int mix, T a, T fz, T b, T s) { return mix ? mix_ab(a, fz, b, s) : s; }
+
+template <typename T, bool RESID, bool SUMSQ>
+__device__ __forceinline__ double batched_push_row4(const TileRec<T, float>* r, T a, T b, int mix, int sumsq_diff,
+                                                    int y, int x, int lane, bool active, int nlan, bool single) {
+    const unsigned P = lds32(&r->P);
+    const int pitch = (int)lds32(&r->pitch);
+    const unsigned o = unsigned(y * pitch + x);
+    const int ny = (int)lds32(&r->ny);
+    const int yu = y == ny - 1 ? 0 : y + 1, yl = y == 0 ? ny - 1 : y - 1;
+    const bool need_fz = mix || (SUMSQ && sumsq_diff);
+    T ps[8][4];
+    T f0[4], f2[4];   // the inputs of the directions that stay in the row (mixing)
+    // the mixing inputs of the destination chunks in the rows above and below,
+    // loaded with the row's own inputs (all loads of the row in flight at once)
+    float4 fzv[8];
+    {
+        const float* fi = ldsP(&r->fi);
+        float4 v[8];
+#pragma unroll
+        for (unsigned i = 0; i < 8; ++i) v[i] = active ? ldg4(fi + (o + i * P)) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            fzv[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (cy8(i) != 0 && need_fz && active)
+                fzv[i] = ldg4(fi + (unsigned((cy8(i) > 0 ? yu : yl) * pitch + x) + unsigned(i) * P));
+        }
+        f0[0] = T(v[0].x); f0[1] = T(v[0].y); f0[2] = T(v[0].z); f0[3] = T(v[0].w);
+        f2[0] = T(v[2].x); f2[1] = T(v[2].y); f2[2] = T(v[2].z); f2[3] = T(v[2].w);
+        T g[4][8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            g[0][i] = T(v[i].x); g[1][i] = T(v[i].y); g[2][i] = T(v[i].z); g[3][i] = T(v[i].w);
+        }
+        if constexpr (RESID) {
+            const float* rs = ldsP(&r->rs);
+#pragma unroll
+            for (unsigned i = 0; i < 8; ++i) {
+                const float4 q = active ? ldg4(rs + (o + i * P)) : make_float4(0.f, 0.f, 0.f, 0.f);
+                g[0][i] = g[0][i] - T(q.x); g[1][i] = g[1][i] - T(q.y);
+                g[2][i] = g[2][i] - T(q.z); g[3][i] = g[3][i] - T(q.w);
+            }
+        }
+        const float* fc = ldsP(&r->fc);
+        float4 F0 = make_float4(0.f, 0.f, 0.f, 0.f), F1 = F0;
+        if (fc && active) { F0 = ldg4(fc + o); F1 = ldg4(fc + (o + P)); }
+        const T F0j[4] = {T(F0.x), T(F0.y), T(F0.z), T(F0.w)}, F1j[4] = {T(F1.x), T(F1.y), T(F1.z), T(F1.w)};
+        const T cs = ldsT(&r->cs), cd = ldsT(&r->cd), h = ldsT(&r->h), n = ldsT(&r->n);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            T fs[8];
+            elast_collide<T>(g[j], fc != nullptr, F0j[j], F1j[j], cs, cd, h, n, fs);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) ps[i][j] = fs[i];
+        }
+    }
+    const int nx = (int)lds32(&r->nx);
+    const float* fi = ldsP(&r->fi);
+    float* fo = ldsP(&r->fo);
+    const int src_l = lane == 0 ? nlan - 1 : lane - 1;          // chunk to the left (wrap inside one tile)
+    const int src_r = lane >= nlan - 1 ? 0 : lane + 1;          // chunk to the right
+    double acc = 0.0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int cxi = cx8(i), cyi = cy8(i);
+        const int yd = cyi > 0 ? yu : (cyi < 0 ? yl : y);
+        T e[4];
+        bool has0 = true, has3 = true;
+        if (cxi > 0) {
+            const T left = __shfl_sync(0xffffffffu, ps[i][3], src_l);
+            e[0] = left; e[1] = ps[i][0]; e[2] = ps[i][1]; e[3] = ps[i][2];
+            has0 = lane > 0 || single;
+        } else if (cxi < 0) {
+            const T right = __shfl_sync(0xffffffffu, ps[i][0], src_r);
+            e[0] = ps[i][1]; e[1] = ps[i][2]; e[2] = ps[i][3]; e[3] = right;
+            has3 = lane < nlan - 1 || single;
+        } else {
+            e[0] = ps[i][0]; e[1] = ps[i][1]; e[2] = ps[i][2]; e[3] = ps[i][3];
+        }
+        if (!active) continue;
+        const unsigned od = unsigned(yd * pitch + x) + unsigned(i) * P;
+        T fz[4] = {T(0), T(0), T(0), T(0)};
+        if (need_fz) {
+            if (cyi == 0) {
+#pragma unroll
+                for (int j = 0; j < 4; ++j) fz[j] = i == 0 ? f0[j] : f2[j];
+            } else {
+                fz[0] = T(fzv[i].x); fz[1] = T(fzv[i].y); fz[2] = T(fzv[i].z); fz[3] = T(fzv[i].w);
+            }
+        }
+        float out[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) out[j] = float(mixv<T>(mix, a, fz[j], b, e[j]));
+        if (has0 && has3) {
+            *reinterpret_cast<float4*>(fo + od) = make_float4(out[0], out[1], out[2], out[3]);
+        } else if (!has0) {   // element 0 comes from the tile to the left
+            fo[od + 1] = out[1];
+            *reinterpret_cast<float2*>(fo + od + 2) = make_float2(out[2], out[3]);
+        } else {              // element 3 comes from the tile to the right
+            *reinterpret_cast<float2*>(fo + od) = make_float2(out[0], out[1]);
+            fo[od + 2] = out[2];
+        }
+        if constexpr (SUMSQ) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                if ((j == 0 && !has0) || (j == 3 && !has3)) continue;
+                double d = (double)out[j];
+                if (sumsq_diff) d -= (double)float(fz[j]);
+                acc += d * d;
+            }
+        }
+        // the value that leaves the tile: one scalar store by its pusher
+        if (!single && ((cxi > 0 && lane == nlan - 1) || (cxi < 0 && lane == 0))) {
+            const int xd = cxi > 0 ? (x + 4 == nx ? 0 : x + 4) : (x == 0 ? nx - 1 : x - 1);
+            const unsigned oz = unsigned(yd * pitch + xd) + unsigned(i) * P;
+            const T sv = cxi > 0 ? ps[i][3] : ps[i][0];
+            T fzs = T(0);
+            if (need_fz) fzs = T(__ldg(fi + oz));
+            const float w = float(mixv<T>(mix, a, fzs, b, sv));
+            fo[oz] = w;
+            if constexpr (SUMSQ) {
+                double d = (double)w;
+                if (sumsq_diff) d -= (double)float(fzs);
+                acc += d * d;
+            }
+        }
+    }
+    return acc;
+}
+
+// 16 warps (one per row of a 16-row tile), up to 128 registers: the row's 16
+// float4 loads stay in flight together.  Measured on B200 against 8-warp CTAs
+// held to 80 registers (three per SM) and CTAs held to 64: both slower (spills,
+// or the mixing loads issued late).
+template <typename T, bool RESID, bool SUMSQ>
+__global__ void __launch_bounds__(512, 1)
+batched_push4_kernel(const BatchInst<T, float>* __restrict__ inst, const XlbbBatchTile* __restrict__ tiles, int ntiles,
+                     T a, T b, int mix, int use_force, int sumsq_diff, double* tile_sumsq) {
+    __shared__ double red[16];
+    __shared__ TileRec<T, float> rec[16];
+    const int lane = threadIdx.x;                // blockDim = (32, 16): a warp per tile row
+    TileRec<T, float>* r = rec + threadIdx.y;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        __syncwarp();
+        if (lane == 0) {
+            const XlbbBatchTile tl = tiles[t];
+            const BatchInst<T, float>& I = inst[tl.inst];
+            r->fi = I.f_in;
+            r->fo = I.f_out;
+            r->fc = use_force ? I.force : nullptr;
+            r->rs = RESID ? I.resid : nullptr;
+            r->P = (unsigned)I.geom.plane;
+            r->pitch = I.geom.pitch;
+            r->nx = I.geom.nx;
+            r->ny = I.geom.ny;
+            r->x0 = tl.x0;
+            r->ys = tl.ys;
+            r->ye = I.vec4 && (tl.x0 & 3) == 0 ? tl.ye : tl.ys;   // an instance that does not qualify: skipped
+            r->cs = I.cs;
+            r->cd = I.cd;
+            r->h = I.h;
+            r->n = I.n;
+            if (!(I.vec4 && (tl.x0 & 3) == 0) && threadIdx.y == 0) atomicExch(&g_xlbb_status, XLBB_EBADARG);
+        }
+        __syncwarp();
+        const int x0 = (int)lds32(&r->x0), nx = (int)lds32(&r->nx);
+        const int x = x0 + 4 * lane;
+        const int nlan = min(32, (nx - x0) >> 2);
+        const bool single = nx <= 128;           // the whole row is this warp's
+        double acc = 0.0;
+        for (int y = (int)lds32(&r->ys) + threadIdx.y; y < (int)lds32(&r->ye); y += blockDim.y)
+            acc += batched_push_row4<T, RESID, SUMSQ>(r, a, b, mix, sumsq_diff, y, x, lane, lane < nlan, nlan, single);
+        if constexpr (SUMSQ) {
             const double s = block_sum_2d(acc, red);
             if (threadIdx.x == 0 && threadIdx.y == 0) tile_sumsq[t] = s;
         }
@@ -1431,6 +1694,32 @@ static int batched_sweep_t(const void* inst, const XlbbBatchTile* tiles, int nti
     return check_launch("xlbb_batched_elast_sweep");
 }
 
+// Four-column batched sweep: CTAs of 32 x 16 threads (a warp per tile row),
+// at most one wave of resident CTAs.
+template <typename T>
+static int batched_sweep4_t(const void* inst, const XlbbBatchTile* tiles, int ntiles, int ctas, double a, double b,
+                            int use_force, int has_resid, int sumsq_diff, double* tile_sumsq, cudaStream_t st) {
+    const int mix = (a == 0.0 && b == 1.0) ? 0 : 1;
+    const BatchInst<T, float>* I = static_cast<const BatchInst<T, float>*>(inst);
+    const dim3 blk(32, 16);
+#define XLBB_BP4(R, Q_)                                                                                       \
+    do {                                                                                                      \
+        static int resident = 0;                                                                              \
+        if (resident == 0) {                                                                                  \
+            int per_sm = 0;                                                                                   \
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batched_push4_kernel<T, R, Q_>,            \
+                                                          (int)(blk.x * blk.y), 0);                           \
+            resident = (per_sm > 0 ? per_sm : 1) * num_sms();                                                 \
+        }                                                                                                     \
+        batched_push4_kernel<T, R, Q_><<<ctas < resident ? ctas : resident, blk, 0, st>>>(                    \
+            I, tiles, ntiles, T(a), T(b), mix, use_force, sumsq_diff, tile_sumsq);                            \
+    } while (0)
+    if (has_resid) { if (tile_sumsq) XLBB_BP4(true, true); else XLBB_BP4(true, false); }
+    else { if (tile_sumsq) XLBB_BP4(false, true); else XLBB_BP4(false, false); }
+#undef XLBB_BP4
+    return check_launch("xlbb_batched_elast_sweep4");
+}
+
 extern "C" {
 
 int xlbb_batched_elast_sweep(int dtype, const void* inst_dev, const XlbbBatchTile* tiles_dev, int ntiles, int ctas,
@@ -1447,6 +1736,17 @@ int xlbb_batched_elast_sweep(int dtype, const void* inst_dev, const XlbbBatchTil
         return batched_sweep_t<double, float>(inst_dev, tiles_dev, ntiles, ctas, a, b, use_force, has_resid,
                                               sumsq_diff, tile_sumsq, XLBB_STREAM(stream));
     return fail(XLBB_EUNSUPPORTED, "xlbb_batched_elast_sweep: dtype");
+}
+
+int xlbb_batched_elast_sweep4(int dtype, const void* inst_dev, const XlbbBatchTile* tiles_dev, int ntiles, int ctas,
+                              double a, double b, int use_force, int has_resid, int sumsq_diff, double* tile_sumsq,
+                              void* stream) {
+    if (!inst_dev || !tiles_dev || ntiles <= 0 || ctas <= 0)
+        return fail(XLBB_EBADARG, "xlbb_batched_elast_sweep4: bad argument");
+    if (dtype == XLBB_F32)
+        return batched_sweep4_t<float>(inst_dev, tiles_dev, ntiles, ctas, a, b, use_force, has_resid, sumsq_diff,
+                                       tile_sumsq, XLBB_STREAM(stream));
+    return fail(XLBB_EUNSUPPORTED, "xlbb_batched_elast_sweep4: dtype (XLBB_F32 only)");
 }
 
 int xlbb_batched_restrict(int dtype_fine, int dtype_coarse, const XlbbBatchTransfer* tr_dev, int ninst, void* stream) {

@@ -141,7 +141,7 @@ __global__ void elast_sweep_adjoint_kernel(const ElastAdjArgs<T> p) {
     const T lM4 = T(0.25) * (lp[4] - lp[5] + lp[6] - lp[7]);
     const T lM5 = T(-0.5) * lp[0] + T(0.5) * lp[2] + T(0.25) * (lp[4] - lp[5] - lp[6] + lp[7]);
     const T lM6 = T(-0.5) * lp[1] + T(0.5) * lp[3] + T(0.25) * (lp[4] + lp[5] - lp[6] - lp[7]);
-    const T lm0 = lM0 + lM5 / T(3), lm1 = lM1 + lM6 / T(3);
+    const T lm0 = lM0 + T(1.0 / 3.0) * lM5, lm1 = lM1 + T(1.0 / 3.0) * lM6;   // transposes of the collision's thirds
     const T lm2 = cs * lM2, lm3 = cd * lM3, lm4 = cd * lM4;
     T lg[8];
 #pragma unroll
@@ -160,8 +160,8 @@ __global__ void elast_sweep_adjoint_kernel(const ElastAdjArgs<T> p) {
     // the collision with F absent is the same map as with F = 0: the adjoint
     // of the force is defined either way
     if (p.lam_force) {
-        p.lam_force[o] = lM0 + lM5 / T(6);
-        p.lam_force[o + P] = lM1 + lM6 / T(6);
+        p.lam_force[o] = lM0 + T(1.0 / 6.0) * lM5;
+        p.lam_force[o + P] = lM1 + T(1.0 / 6.0) * lM6;
     }
     if (p.g_mu) {
         // moments of the forward sweep's pre-collision input g = f - resid

@@ -84,6 +84,12 @@ __device__ __forceinline__ double block_sum(double v, double* sh) {
     return s;
 }
 
+// The smoothers' mixing a * f + b * s with one fixed rounding (b * s rounded,
+// then a fused multiply-add), the same in every sweep kernel, so that all launch
+// forms of a sweep give bit-identical results.
+template <typename T>
+__device__ __forceinline__ T mix_ab(T a, T f, T b, T s) { return fma(a, f, b * s); }
+
 // Block-wide FP64 sum for 2D blocks (warps follow the linear thread index;
 // sh holds one double per warp): the total is returned in thread (0, 0).
 __device__ __forceinline__ double block_sum_2d(double v, double* sh) {
