@@ -951,32 +951,91 @@ struct __align__(16) TileRec {
     T cs, cd, h, n;
 };
 
+// Lane 0 copies tile t's record into `d`; with `vec4`, an instance that does
+// not qualify for the four-column kernel gets an empty row range and sets the
+// status word.
+template <typename T, typename S>
+__device__ __forceinline__ void fill_tile_rec(TileRec<T, S>* d, const BatchInst<T, S>* __restrict__ inst,
+                                              const XlbbBatchTile* __restrict__ tiles, int t, int use_force,
+                                              bool resid, bool vec4) {
+    const XlbbBatchTile tl = tiles[t];
+    const BatchInst<T, S>& I = inst[tl.inst];
+    const bool ok = !vec4 || (I.vec4 && (tl.x0 & 3) == 0);
+    d->fi = I.f_in;
+    d->fo = I.f_out;
+    d->fc = use_force ? I.force : nullptr;
+    d->rs = resid ? I.resid : nullptr;
+    d->P = (unsigned)I.geom.plane;
+    d->pitch = I.geom.pitch;
+    d->nx = I.geom.nx;
+    d->ny = I.geom.ny;
+    d->x0 = tl.x0;
+    d->ys = tl.ys;
+    d->ye = ok ? tl.ye : tl.ys;
+    d->cs = I.cs;
+    d->cd = I.cd;
+    d->h = I.h;
+    d->n = I.n;
+    if (!ok) atomicExch(&g_xlbb_status, XLBB_EBADARG);
+}
+
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
+// Prefetch into L2 a warp's cells of the next tile's row (`n` cells per lane
+// starting at column x): no registers stay held, the next row's loads are then
+// served from L2.
+template <typename T, typename S, bool RESID>
+__device__ __forceinline__ void prefetch_tile_row(const TileRec<T, S>* rn, int w, int x) {
+    const int yn = (int)lds32(&rn->ys) + w, xn = (int)lds32(&rn->x0) + x;
+    if (yn >= (int)lds32(&rn->ye) || xn >= (int)lds32(&rn->nx)) return;
+    const unsigned Pn = lds32(&rn->P), on = unsigned(yn * (int)lds32(&rn->pitch) + xn);
+    const S* fin = ldsP(&rn->fi);
+#pragma unroll
+    for (unsigned i = 0; i < 8; ++i) prefetch_l2(fin + (on + i * Pn));
+    const S* fcn = ldsP(&rn->fc);
+    if (fcn) { prefetch_l2(fcn + on); prefetch_l2(fcn + (on + Pn)); }
+    if constexpr (RESID) {
+        const S* rsn = ldsP(&rn->rs);
+#pragma unroll
+        for (unsigned i = 0; i < 8; ++i) prefetch_l2(rsn + (on + i * Pn));
+    }
+}
+
 // One cell of the batched collide-and-push sweep (periodic, no boundary rules):
 // the arithmetic of ElastPhys's load / collide / put; plane i of the cell at
-// offset o is fi + (i * P + o).
-template <typename T, bool RESID, bool SUMSQ, typename S>
-__device__ __forceinline__ double batched_push_cell(const TileRec<T, S>* r, T a, T b, int mix, int sumsq_diff, int y,
-                                                    int x) {
+// offset o is fi + (i * P + o).  Split in its loads and the rest, so that the
+// caller can overlap work with the loads' latency.
+template <typename T>
+struct BatchedCell {
     T g[8];
-    T F0 = T(0), F1 = T(0);
+    T F0, F1;
     bool hasF;
-    {
-        const S* fi = ldsP(&r->fi);
-        const unsigned P = lds32(&r->P);
-        const unsigned o = unsigned(y * (int)lds32(&r->pitch) + x);
+};
+
+template <typename T, bool RESID, typename S>
+__device__ __forceinline__ void batched_cell_load(const TileRec<T, S>* r, int y, int x, BatchedCell<T>& c) {
+    const S* fi = ldsP(&r->fi);
+    const unsigned P = lds32(&r->P);
+    const unsigned o = unsigned(y * (int)lds32(&r->pitch) + x);
 #pragma unroll
-        for (unsigned i = 0; i < 8; ++i) g[i] = T(__ldg(fi + (o + i * P)));
-        if constexpr (RESID) {
-            const S* rs = ldsP(&r->rs);
+    for (unsigned i = 0; i < 8; ++i) c.g[i] = T(__ldg(fi + (o + i * P)));
+    if constexpr (RESID) {
+        const S* rs = ldsP(&r->rs);
 #pragma unroll
-            for (unsigned i = 0; i < 8; ++i) g[i] = g[i] - T(__ldg(rs + (o + i * P)));
-        }
-        const S* fc = ldsP(&r->fc);
-        hasF = fc != nullptr;
-        if (fc) { F0 = T(__ldg(fc + o)); F1 = T(__ldg(fc + (o + P))); }
+        for (unsigned i = 0; i < 8; ++i) c.g[i] = c.g[i] - T(__ldg(rs + (o + i * P)));
     }
+    const S* fc = ldsP(&r->fc);
+    c.hasF = fc != nullptr;
+    c.F0 = T(0);
+    c.F1 = T(0);
+    if (fc) { c.F0 = T(__ldg(fc + o)); c.F1 = T(__ldg(fc + (o + P))); }
+}
+
+template <typename T, bool SUMSQ, typename S>
+__device__ __forceinline__ double batched_cell_push(const TileRec<T, S>* r, const BatchedCell<T>& c, T a, T b, int mix,
+                                                    int sumsq_diff, int y, int x) {
     T fs[8];
-    elast_collide<T>(g, hasF, F0, F1, ldsT(&r->cs), ldsT(&r->cd), ldsT(&r->h), ldsT(&r->n), fs);
+    elast_collide<T>(c.g, c.hasF, c.F0, c.F1, ldsT(&r->cs), ldsT(&r->cd), ldsT(&r->h), ldsT(&r->n), fs);
     const int pitch = (int)lds32(&r->pitch), nx = (int)lds32(&r->nx), ny = (int)lds32(&r->ny);
     const unsigned P = lds32(&r->P);
     const S* fi = ldsP(&r->fi);
@@ -1006,52 +1065,66 @@ __device__ __forceinline__ double batched_push_cell(const TileRec<T, S>* r, T a,
 // Collide-and-push form of the batched sweep: a block of 128 x 8 threads takes
 // a tile, thread (tx, ty) its column x0 + tx and every 8th row from ys + ty
 // (independent cells: no block barrier); with SUMSQ one FP64 partial per tile.
-// Measured on B200 (512 instances, 26 M cells, level-0 smoothing sweep): the
-// record in shared memory beat every thread loading it into registers by 15%;
-// CTAs held to 32 or 40 registers for more CTAs per SM, two rows per thread
-// loaded before either is collided, a cp.async prefetch of the next tile's
-// record, and taller tiles were all slower.  The explicit minimum of one CTA
-// per SM lets the compiler keep up to 64 registers per thread (more loads in
-// flight per thread), which measured faster than its 32-register choice.
+// Each warp keeps its tile record, and the next one, in shared memory: while
+// the first row's loads are in flight lane 0 fetches the next tile's record
+// and the warp prefetches its cells of the next tile into L2.  Measured on
+// B200 (512 instances, 26 M cells, level-0 smoothing sweep): the record in
+// shared memory beat every thread loading it into registers by 15%; CTAs held
+// to 32 or 40 registers for more CTAs per SM, two rows per thread loaded
+// before either is collided, and taller tiles were all slower.  The explicit
+// minimum of one CTA per SM lets the compiler keep up to 64 registers per
+// thread (more loads in flight per thread), which measured faster than its
+// 32-register choice.
 template <typename T, bool RESID, bool SUMSQ, typename S = T>
 __global__ void __launch_bounds__(1024, 1)
 batched_push_kernel(const BatchInst<T, S>* __restrict__ inst, const XlbbBatchTile* __restrict__ tiles, int ntiles,
                     T a, T b, int mix, int use_force, int sumsq_diff, double* tile_sumsq) {
     __shared__ double red[32];
-    __shared__ TileRec<T, S> rec[32];
-    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-    TileRec<T, S>* r = rec + (tid >> 5);
-    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        __syncwarp();                 // every lane is done with the previous record
-        if ((tid & 31) == 0) {
-            const XlbbBatchTile tl = tiles[t];
-            const BatchInst<T, S>& I = inst[tl.inst];
-            r->fi = I.f_in;
-            r->fo = I.f_out;
-            r->fc = use_force ? I.force : nullptr;
-            r->rs = RESID ? I.resid : nullptr;
-            r->P = (unsigned)I.geom.plane;
-            r->pitch = I.geom.pitch;
-            r->nx = I.geom.nx;
-            r->ny = I.geom.ny;
-            r->x0 = tl.x0;
-            r->ys = tl.ys;
-            r->ye = tl.ye;
-            r->cs = I.cs;
-            r->cd = I.cd;
-            r->h = I.h;
-            r->n = I.n;
+    __shared__ TileRec<T, S> rec[2][32];
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x, wid = tid >> 5;
+    if (blockIdx.x >= ntiles) return;          // uniform over the block
+    if ((tid & 31) == 0) fill_tile_rec(&rec[0][wid], inst, tiles, blockIdx.x, use_force, RESID, false);
+    __syncwarp();
+    // FP32 arithmetic overlaps the next tile's record and prefetch with the
+    // loads; the FP64-arithmetic variants, at their 64-register limit, fetch
+    // each record when they reach the tile (the overlap measured slower: spills)
+    constexpr bool OVERLAP = sizeof(T) == 4;
+    int k = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++k) {
+        TileRec<T, S>* r = &rec[OVERLAP ? (k & 1) : 0][wid];
+        TileRec<T, S>* rn = &rec[OVERLAP ? ((k + 1) & 1) : 0][wid];
+        const int tn = t + gridDim.x;
+        if constexpr (!OVERLAP) {
+            if (k > 0) {
+                if ((tid & 31) == 0) fill_tile_rec(r, inst, tiles, t, use_force, RESID, false);
+                __syncwarp();
+            }
         }
-        __syncwarp();
+        bool pending = OVERLAP;                // the next record is still to be fetched
         const int x = (int)lds32(&r->x0) + threadIdx.x;
+        const bool active = x < (int)lds32(&r->nx);
         double acc = 0.0;
-        if (x < (int)lds32(&r->nx))
-            for (int y = (int)lds32(&r->ys) + threadIdx.y; y < (int)lds32(&r->ye); y += blockDim.y)
-                acc += batched_push_cell<T, RESID, SUMSQ, S>(r, a, b, mix, sumsq_diff, y, x);
+        // warp-uniform loop (a warp spans one threadIdx.y); inactive lanes only join the next-tile work
+        for (int y = (int)lds32(&r->ys) + threadIdx.y; y < (int)lds32(&r->ye); y += blockDim.y) {
+            BatchedCell<T> c;
+            if (active) batched_cell_load<T, RESID, S>(r, y, x, c);
+            if (pending) {
+                pending = false;
+                if (tn < ntiles && (tid & 31) == 0) fill_tile_rec(rn, inst, tiles, tn, use_force, RESID, false);
+                __syncwarp();
+                if (tn < ntiles) prefetch_tile_row<T, S, RESID>(rn, threadIdx.y, threadIdx.x);
+            }
+            if (active) acc += batched_cell_push<T, SUMSQ, S>(r, c, a, b, mix, sumsq_diff, y, x);
+        }
+        if (pending) {                          // a warp without a row in this tile
+            if (tn < ntiles && (tid & 31) == 0) fill_tile_rec(rn, inst, tiles, tn, use_force, RESID, false);
+            __syncwarp();
+        }
         if constexpr (SUMSQ) {   // the tile's writes: every output of the instance is written once
             const double s = block_sum_2d(acc, red);
             if (threadIdx.x == 0 && threadIdx.y == 0) tile_sumsq[t] = s;
         }
+        __syncwarp();                           // every lane is done with r before it is refilled
     }
 }
 
@@ -1072,9 +1145,11 @@ __device__ __forceinline__ float4 ldg4(const float* p) { return __ldg(reinterpre
 template <typename T>
 __device__ __forceinline__ T mixv(int mix, T a, T fz, T b, T s) { return mix ? mix_ab(a, fz, b, s) : s; }
 
-template <typename T, bool RESID, bool SUMSQ>
+// `mid` runs once the row's loads are issued (work that overlaps their latency).
+template <typename T, bool RESID, bool SUMSQ, class Mid>
 __device__ __forceinline__ double batched_push_row4(const TileRec<T, float>* r, T a, T b, int mix, int sumsq_diff,
-                                                    int y, int x, int lane, bool active, int nlan, bool single) {
+                                                    int y, int x, int lane, bool active, int nlan, bool single,
+                                                    Mid&& mid) {
     const unsigned P = lds32(&r->P);
     const int pitch = (int)lds32(&r->pitch);
     const unsigned o = unsigned(y * pitch + x);
@@ -1116,6 +1191,7 @@ __device__ __forceinline__ double batched_push_row4(const TileRec<T, float>* r, 
         const float* fc = ldsP(&r->fc);
         float4 F0 = make_float4(0.f, 0.f, 0.f, 0.f), F1 = F0;
         if (fc && active) { F0 = ldg4(fc + o); F1 = ldg4(fc + (o + P)); }
+        mid();
         const T F0j[4] = {T(F0.x), T(F0.y), T(F0.z), T(F0.w)}, F1j[4] = {T(F1.x), T(F1.y), T(F1.z), T(F1.w)};
         const T cs = ldsT(&r->cs), cd = ldsT(&r->cd), h = ldsT(&r->h), n = ldsT(&r->n);
 #pragma unroll
@@ -1200,52 +1276,66 @@ __device__ __forceinline__ double batched_push_row4(const TileRec<T, float>* r, 
     return acc;
 }
 
+
 // 16 warps (one per row of a 16-row tile), up to 128 registers: the row's 16
-// float4 loads stay in flight together.  Measured on B200 against 8-warp CTAs
-// held to 80 registers (three per SM) and CTAs held to 64: both slower (spills,
-// or the mixing loads issued late).
+// float4 loads stay in flight together.  While they are in flight, lane 0
+// copies the warp's next tile record into the second slot and every lane asks
+// L2 for its columns of the next tile's row (prefetch: no registers held), so
+// the next row's loads are served from L2.  Measured on B200 against 8-warp
+// CTAs held to 80 registers (three per SM) and CTAs held to 64: both slower
+// (spills, or the mixing loads issued late).
 template <typename T, bool RESID, bool SUMSQ>
 __global__ void __launch_bounds__(512, 1)
 batched_push4_kernel(const BatchInst<T, float>* __restrict__ inst, const XlbbBatchTile* __restrict__ tiles, int ntiles,
                      T a, T b, int mix, int use_force, int sumsq_diff, double* tile_sumsq) {
     __shared__ double red[16];
-    __shared__ TileRec<T, float> rec[16];
-    const int lane = threadIdx.x;                // blockDim = (32, 16): a warp per tile row
-    TileRec<T, float>* r = rec + threadIdx.y;
-    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        __syncwarp();
-        if (lane == 0) {
-            const XlbbBatchTile tl = tiles[t];
-            const BatchInst<T, float>& I = inst[tl.inst];
-            r->fi = I.f_in;
-            r->fo = I.f_out;
-            r->fc = use_force ? I.force : nullptr;
-            r->rs = RESID ? I.resid : nullptr;
-            r->P = (unsigned)I.geom.plane;
-            r->pitch = I.geom.pitch;
-            r->nx = I.geom.nx;
-            r->ny = I.geom.ny;
-            r->x0 = tl.x0;
-            r->ys = tl.ys;
-            r->ye = I.vec4 && (tl.x0 & 3) == 0 ? tl.ye : tl.ys;   // an instance that does not qualify: skipped
-            r->cs = I.cs;
-            r->cd = I.cd;
-            r->h = I.h;
-            r->n = I.n;
-            if (!(I.vec4 && (tl.x0 & 3) == 0) && threadIdx.y == 0) atomicExch(&g_xlbb_status, XLBB_EBADARG);
-        }
-        __syncwarp();
+    __shared__ TileRec<T, float> rec[2][16];
+    const int lane = threadIdx.x, w = threadIdx.y;   // blockDim = (32, 16): a warp per tile row
+    if (blockIdx.x >= ntiles) return;                 // uniform over the block
+    if (lane == 0) fill_tile_rec(&rec[0][w], inst, tiles, blockIdx.x, use_force, RESID, true);
+    __syncwarp();
+    int k = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++k) {
+        TileRec<T, float>* r = &rec[k & 1][w];
+        TileRec<T, float>* rn = &rec[(k + 1) & 1][w];
+        const int tn = t + gridDim.x;
+        bool pending = true;                          // the next record is still to be fetched
+        auto next = [&]() {
+            if (!pending) return;
+            pending = false;
+            if (tn < ntiles && lane == 0) fill_tile_rec(rn, inst, tiles, tn, use_force, RESID, true);
+            __syncwarp();
+            if (tn < ntiles) {
+                const int yn = (int)lds32(&rn->ys) + w, xn = (int)lds32(&rn->x0) + 4 * lane;
+                if (yn < (int)lds32(&rn->ye) && xn < (int)lds32(&rn->nx)) {
+                    const unsigned Pn = lds32(&rn->P), on = unsigned(yn * (int)lds32(&rn->pitch) + xn);
+                    const float* fin = ldsP(&rn->fi);
+#pragma unroll
+                    for (unsigned i = 0; i < 8; ++i) prefetch_l2(fin + (on + i * Pn));
+                    const float* fcn = ldsP(&rn->fc);
+                    if (fcn) { prefetch_l2(fcn + on); prefetch_l2(fcn + (on + Pn)); }
+                    if constexpr (RESID) {
+                        const float* rsn = ldsP(&rn->rs);
+#pragma unroll
+                        for (unsigned i = 0; i < 8; ++i) prefetch_l2(rsn + (on + i * Pn));
+                    }
+                }
+            }
+        };
         const int x0 = (int)lds32(&r->x0), nx = (int)lds32(&r->nx);
         const int x = x0 + 4 * lane;
         const int nlan = min(32, (nx - x0) >> 2);
         const bool single = nx <= 128;           // the whole row is this warp's
         double acc = 0.0;
-        for (int y = (int)lds32(&r->ys) + threadIdx.y; y < (int)lds32(&r->ye); y += blockDim.y)
-            acc += batched_push_row4<T, RESID, SUMSQ>(r, a, b, mix, sumsq_diff, y, x, lane, lane < nlan, nlan, single);
+        for (int y = (int)lds32(&r->ys) + w; y < (int)lds32(&r->ye); y += blockDim.y)
+            acc += batched_push_row4<T, RESID, SUMSQ>(r, a, b, mix, sumsq_diff, y, x, lane, lane < nlan, nlan, single,
+                                                      next);
+        next();                                  // a warp without a row in this tile
         if constexpr (SUMSQ) {
             const double s = block_sum_2d(acc, red);
             if (threadIdx.x == 0 && threadIdx.y == 0) tile_sumsq[t] = s;
         }
+        __syncwarp();                            // every lane is done with r before it is refilled
     }
 }
 
