@@ -9,6 +9,8 @@
 #include <string>
 #include <type_traits>
 #include <vector>
+#include <cstdlib>
+#include <utility>
 
 #include "xlbb.h"
 #include "xlbb_common.cuh"
@@ -30,6 +32,36 @@ static int check_launch(const char* what) {
         return XLBB_ELAUNCH;
     }
     return XLBB_OK;
+}
+
+// Every kernel of the library is launched here, with programmatic stream
+// serialization (programmatic dependent launch): the next kernel of a stream
+// (or of a captured CUDA graph) may be scheduled while its predecessor drains,
+// which hides most of the launch gap between the short dependent sweeps of the
+// multigrid levels; each kernel starts with grid_dep_wait(), so it touches no
+// memory before its predecessor has finished.  XLBB_PDL=0 in the environment
+// launches ordinarily.  Errors surface through cudaGetLastError (check_launch).
+static bool pdl_enabled() {
+    static const bool on = [] {
+        const char* v = getenv("XLBB_PDL");
+        return !(v && v[0] == '0');
+    }();
+    return on;
+}
+
+template <typename... KArgs, typename... Args>
+static void launch_k(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = pdl_enabled() ? 1 : 0;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
 // Offsets inside one plane are 32-bit in the kernels: a plane holds < 2^31 elements.
@@ -463,7 +495,7 @@ static void launch_bulk(dim3 grid, cudaStream_t st, const typename Ph::Args& a) 
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
         configured = bytes;
     }
-    k<<<grid, TX + 32, bytes, st>>>(a);
+    launch_k(k, grid, TX + 32, bytes, st, a);
 }
 
 // 16-byte alignment of every input plane and of the row pitch: the bulk copies need it.
@@ -481,8 +513,8 @@ static bool bulk_aligned(const typename Ph::Args& a) {
 template <class Ph>
 static void launch_push(const XlbbSweepConfig& c, const XlbbGrid* g, cudaStream_t st, const typename Ph::Args& a) {
     const dim3 grid((g->nx + c.tx - 1) / c.tx, g->ny);
-    if (a.sumsq) push_kernel<Ph, true><<<grid, c.tx, 0, st>>>(a);
-    else push_kernel<Ph, false><<<grid, c.tx, 0, st>>>(a);
+    if (a.sumsq) launch_k(push_kernel<Ph, true>, grid, c.tx, 0, st, a);
+    else launch_k(push_kernel<Ph, false>, grid, c.tx, 0, st, a);
 }
 
 // Runtime (bulk, tx, depth) -> template instance.  The register-prefetch
@@ -502,8 +534,8 @@ static void launch_sweep(XlbbSweepConfig c, const XlbbGrid* g, cudaStream_t st, 
     const dim3 grid = sweep_grid(g, c);
     if (c.pipeline == 2) {
         const WarpGrid wg = warp_grid(g, c);
-        if (c.depth == 2) sweep_warp_kernel<Ph, 2, PREV><<<wg.ctas, 128, 0, st>>>(a, wg.nbx, wg.nstrips);
-        else sweep_warp_kernel<Ph, 1, PREV><<<wg.ctas, 128, 0, st>>>(a, wg.nbx, wg.nstrips);
+        if (c.depth == 2) launch_k(sweep_warp_kernel<Ph, 2, PREV>, wg.ctas, 128, 0, st, a, wg.nbx, wg.nstrips);
+        else launch_k(sweep_warp_kernel<Ph, 1, PREV>, wg.ctas, 128, 0, st, a, wg.nbx, wg.nstrips);
         return;
     }
     Ph::make_planes(a);
@@ -525,13 +557,13 @@ static void launch_sweep(XlbbSweepConfig c, const XlbbGrid* g, cudaStream_t st, 
     }
 #define XLBB_CASE(TX_, D_)                                                            \
     if (c.tx == TX_ && c.depth == D_) {                                                \
-        sweep_kernel<Ph, TX_, D_, PREV><<<grid, TX_ + 32, 0, st>>>(a);                 \
+        launch_k(sweep_kernel<Ph, TX_, D_, PREV>, grid, TX_ + 32, 0, st, a);                 \
         return;                                                                        \
     }
     XLBB_CASE(128, 1) XLBB_CASE(128, 2)
     if constexpr (F32) { XLBB_CASE(256, 1) XLBB_CASE(256, 2) }
 #undef XLBB_CASE
-    sweep_kernel<Ph, 128, 1, PREV><<<grid, 128 + 32, 0, st>>>(a);
+    launch_k(sweep_kernel<Ph, 128, 1, PREV>, grid, 128 + 32, 0, st, a);
 }
 
 // FP32 storage / FP64 arithmetic: the register-prefetch kernel at tx = 128.
@@ -540,8 +572,8 @@ static void launch_sweep_regs(const XlbbSweepConfig& c, const XlbbGrid* g, cudaS
                               typename Ph::Args& a) {
     Ph::fill_ptrs(a);
     const dim3 grid = sweep_grid(g, c);
-    if (c.depth == 2) sweep_kernel<Ph, 128, 2, PREV><<<grid, 128 + 32, 0, st>>>(a);
-    else sweep_kernel<Ph, 128, 1, PREV><<<grid, 128 + 32, 0, st>>>(a);
+    if (c.depth == 2) launch_k(sweep_kernel<Ph, 128, 2, PREV>, grid, 128 + 32, 0, st, a);
+    else launch_k(sweep_kernel<Ph, 128, 1, PREV>, grid, 128 + 32, 0, st, a);
 }
 
 // The configuration a launch actually uses (FP64 arithmetic caps tx at 128;
@@ -562,6 +594,7 @@ static XlbbSweepConfig effective_cfg(int kernel, int dtype) {
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void gradient_kernel(SweepGeom G, const T* q, T scale, RulesView<T, 9> rules, const T* base, T* out) {
+    grid_dep_wait();
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
     if (x >= G.nx) return;
@@ -600,6 +633,7 @@ __global__ void gradient_kernel(SweepGeom G, const T* q, T scale, RulesView<T, 9
 template <typename T>
 __global__ void elast_moments_kernel(SweepGeom G, ElastMat<T> mat, T lam, T mu, const T* f, const T* force,
                                      const T* fext, T* eta, T* sigma, T* div, T div_scale) {
+    grid_dep_wait();
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
     if (x >= G.nx) return;
@@ -639,6 +673,7 @@ __global__ void elast_moments_kernel(SweepGeom G, ElastMat<T> mat, T lam, T mu, 
 template <typename T>
 __global__ void elast_equilibrium_kernel(SweepGeom G, T lam, T mu, const T* lam_f, const T* mu_f, const T* eta,
                                          const T* sigma, const T* force, const T* fext, T* fo) {
+    grid_dep_wait();
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
     if (x >= G.nx) return;
@@ -669,6 +704,7 @@ __global__ void elast_equilibrium_kernel(SweepGeom G, T lam, T mu, const T* lam_
 template <typename T>
 __global__ void darcy_moments_kernel(SweepGeom G, const T* f, T omega, const T* omega_f, const T* src,
                                      const T* ext, T* rho, T* grad) {
+    grid_dep_wait();
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
     if (x >= G.nx) return;
@@ -704,6 +740,7 @@ __global__ void darcy_moments_kernel(SweepGeom G, const T* f, T omega, const T* 
 template <typename Tf, typename Tc>
 __global__ void restrict_kernel(SweepGeom F, SweepGeom C, int q, int x0, int y0, int nix, int niy, const Tf* res,
                                 Tc* rc) {
+    grid_dep_wait();
     // one thread per coarse cell (all q planes); zero outside the coarse interior
     using Ts = typename std::conditional<(sizeof(Tf) > sizeof(Tc)), Tf, Tc>::type;
     const int X = blockIdx.x * blockDim.x + threadIdx.x;
@@ -726,6 +763,7 @@ __global__ void restrict_kernel(SweepGeom F, SweepGeom C, int q, int x0, int y0,
 template <typename Tf, typename Tc>
 __global__ void prolong_add_kernel(SweepGeom F, SweepGeom C, int q, int x0, int y0, int nfx, int nfy,
                                    const Tc* fc, Tf* ff) {
+    grid_dep_wait();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y;
     if (i >= nfx || j >= nfy) return;
@@ -737,6 +775,7 @@ __global__ void prolong_add_kernel(SweepGeom F, SweepGeom C, int q, int x0, int 
 template <typename T>
 __global__ void sumsq_kernel(SweepGeom G, int nplanes, const T* d, int bx0, int bx1, int by0, int by1,
                              double* partials) {
+    grid_dep_wait();
     __shared__ double red[8];
     double acc = 0.0;
     const long long n = (long long)(bx1 - bx0) * (by1 - by0);
@@ -754,6 +793,7 @@ __global__ void sumsq_kernel(SweepGeom G, int nplanes, const T* d, int bx0, int 
 }
 
 __global__ void reduce_sum_kernel(const double* p, int n, double* out) {
+    grid_dep_wait();
     __shared__ double red[32];
     double acc = 0.0;
     for (int i = threadIdx.x; i < n; i += blockDim.x) acc += p[i];
@@ -763,6 +803,7 @@ __global__ void reduce_sum_kernel(const double* p, int n, double* out) {
 
 template <typename T>
 __global__ void axpby_kernel(long long n, T a, const T* x, T b, const T* y, T* o) {
+    grid_dep_wait();
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         o[i] = a * x[i] + b * y[i];
 }
@@ -881,6 +922,7 @@ template <typename T, int TX, bool RESID, bool PREV, typename S = T>
 __global__ void __launch_bounds__(TX + 32)
 batched_elast_kernel(const BatchInst<T, S>* __restrict__ inst, const XlbbBatchTile* __restrict__ tiles, int ntiles,
                      T a, T b, int mix, int use_force, int sumsq_diff, double* tile_sumsq) {
+    grid_dep_wait();
     using Ph = ElastPhys<T, RESID, S>;
     __shared__ T post[4][8][TX + 2];
     __shared__ double red[(TX + 32) / 32];
@@ -1079,6 +1121,7 @@ template <typename T, bool RESID, bool SUMSQ, typename S = T>
 __global__ void __launch_bounds__(1024, 1)
 batched_push_kernel(const BatchInst<T, S>* __restrict__ inst, const XlbbBatchTile* __restrict__ tiles, int ntiles,
                     T a, T b, int mix, int use_force, int sumsq_diff, double* tile_sumsq) {
+    grid_dep_wait();
     __shared__ double red[32];
     __shared__ TileRec<T, S> rec[2][32];
     const int tid = threadIdx.y * blockDim.x + threadIdx.x, wid = tid >> 5;
@@ -1288,6 +1331,7 @@ template <typename T, bool RESID, bool SUMSQ>
 __global__ void __launch_bounds__(512, 1)
 batched_push4_kernel(const BatchInst<T, float>* __restrict__ inst, const XlbbBatchTile* __restrict__ tiles, int ntiles,
                      T a, T b, int mix, int use_force, int sumsq_diff, double* tile_sumsq) {
+    grid_dep_wait();
     __shared__ double red[16];
     __shared__ TileRec<T, float> rec[2][16];
     const int lane = threadIdx.x, w = threadIdx.y;   // blockDim = (32, 16): a warp per tile row
@@ -1343,6 +1387,7 @@ batched_push4_kernel(const BatchInst<T, float>* __restrict__ inst, const XlbbBat
 // instance of a periodic batch; blockIdx.y = instance.
 template <typename Tf, typename Tc>
 __global__ void batched_restrict_kernel(const XlbbBatchTransfer* __restrict__ tr) {
+    grid_dep_wait();
     const XlbbBatchTransfer T_ = tr[blockIdx.y];
     const Tf* res = static_cast<const Tf*>(T_.fine);
     Tc* rc = static_cast<Tc*>(T_.coarse);
@@ -1364,6 +1409,7 @@ __global__ void batched_restrict_kernel(const XlbbBatchTransfer* __restrict__ tr
 // (block = blockIdx.y * gridDim.x + blockIdx.x).
 template <typename Tf, typename Tc>
 __global__ void batched_prolong_add_kernel(const XlbbBatchTransfer* __restrict__ tr, double* parts) {
+    grid_dep_wait();
     __shared__ double red[8];
     const XlbbBatchTransfer T_ = tr[blockIdx.y];
     Tf* ff = static_cast<Tf*>(const_cast<void*>(T_.fine));
@@ -1394,6 +1440,7 @@ __global__ void batched_prolong_add_kernel(const XlbbBatchTransfer* __restrict__
 // norms[2 i + k] = sum over the XLBB_PROLONG_BLOCKS blocks of instance i of
 // parts[2 block + k]; one warp per instance, fixed order.
 __global__ void prolong_norms_kernel(const double* parts, int ninst, double* norms) {
+    grid_dep_wait();
     const int i = blockIdx.x;
     if (i >= ninst) return;
     static_assert(XLBB_PROLONG_BLOCKS == 32, "one lane per block");
@@ -1412,6 +1459,7 @@ __global__ void prolong_norms_kernel(const double* parts, int ninst, double* nor
 
 // Per-instance FP64 sums of tile partials (tiles of one instance are contiguous).
 __global__ void segment_sum_kernel(const double* parts, const int* begin, int ninst, double* out) {
+    grid_dep_wait();
     __shared__ double red[8];
     const int i = blockIdx.x;
     if (i >= ninst) return;
@@ -1510,10 +1558,10 @@ int xlbb_darcy_gradient(int dtype, const XlbbGrid* g, const void* q, double scal
     const XlbbRules& r = rules ? *rules : none;
     const dim3 grid = row_grid(g->nx, g->ny, 128);
     if (dtype == XLBB_F32)
-        gradient_kernel<float><<<grid, 128, 0, XLBB_STREAM(stream)>>>(geom(g), (const float*)q, (float)scale,
+        launch_k(gradient_kernel<float>, grid, 128, 0, XLBB_STREAM(stream), geom(g), (const float*)q, (float)scale,
                                                                       rules_view<float, 9>(r), (const float*)base, (float*)out);
     else if (dtype == XLBB_F64)
-        gradient_kernel<double><<<grid, 128, 0, XLBB_STREAM(stream)>>>(geom(g), (const double*)q, scale,
+        launch_k(gradient_kernel<double>, grid, 128, 0, XLBB_STREAM(stream), geom(g), (const double*)q, scale,
                                                                        rules_view<double, 9>(r), (const double*)base, (double*)out);
     else return fail(XLBB_EUNSUPPORTED, "xlbb_darcy_gradient: dtype");
     return check_launch("xlbb_darcy_gradient");
@@ -1524,11 +1572,11 @@ int xlbb_elast_moments(int dtype, const XlbbGrid* g, const XlbbElastMaterial* ma
     if (!grid_ok(g) || !mat || !f) return fail(XLBB_EBADARG, "xlbb_elast_moments: bad argument");
     const dim3 grid = row_grid(g->nx, g->ny, 128);
     if (dtype == XLBB_F32)
-        elast_moments_kernel<float><<<grid, 128, 0, XLBB_STREAM(stream)>>>(
+        launch_k(elast_moments_kernel<float>, grid, 128, 0, XLBB_STREAM(stream), 
             geom(g), make_mat<float>(mat), (float)mat->lam, (float)mat->mu, (const float*)f, (const float*)force,
             (const float*)fext, (float*)eta, (float*)sigma, (float*)div, (float)div_scale);
     else if (dtype == XLBB_F64)
-        elast_moments_kernel<double><<<grid, 128, 0, XLBB_STREAM(stream)>>>(
+        launch_k(elast_moments_kernel<double>, grid, 128, 0, XLBB_STREAM(stream), 
             geom(g), make_mat<double>(mat), mat->lam, mat->mu, (const double*)f, (const double*)force,
             (const double*)fext, (double*)eta, (double*)sigma, (double*)div, div_scale);
     else return fail(XLBB_EUNSUPPORTED, "xlbb_elast_moments: dtype");
@@ -1540,11 +1588,11 @@ int xlbb_elast_equilibrium(int dtype, const XlbbGrid* g, const XlbbElastMaterial
     if (!grid_ok(g) || !mat || !eta || !sigma || !f_out) return fail(XLBB_EBADARG, "xlbb_elast_equilibrium: bad argument");
     const dim3 grid = row_grid(g->nx, g->ny, 128);
     if (dtype == XLBB_F32)
-        elast_equilibrium_kernel<float><<<grid, 128, 0, XLBB_STREAM(stream)>>>(
+        launch_k(elast_equilibrium_kernel<float>, grid, 128, 0, XLBB_STREAM(stream), 
             geom(g), (float)mat->lam, (float)mat->mu, (const float*)mat->lam_field, (const float*)mat->mu_field,
             (const float*)eta, (const float*)sigma, (const float*)force, (const float*)fext, (float*)f_out);
     else if (dtype == XLBB_F64)
-        elast_equilibrium_kernel<double><<<grid, 128, 0, XLBB_STREAM(stream)>>>(
+        launch_k(elast_equilibrium_kernel<double>, grid, 128, 0, XLBB_STREAM(stream), 
             geom(g), mat->lam, mat->mu, (const double*)mat->lam_field, (const double*)mat->mu_field,
             (const double*)eta, (const double*)sigma, (const double*)force, (const double*)fext, (double*)f_out);
     else return fail(XLBB_EUNSUPPORTED, "xlbb_elast_equilibrium: dtype");
@@ -1556,11 +1604,11 @@ int xlbb_darcy_moments(int dtype, const XlbbGrid* g, const void* f, double omega
     if (!grid_ok(g) || !f) return fail(XLBB_EBADARG, "xlbb_darcy_moments: bad argument");
     const dim3 grid = row_grid(g->nx, g->ny, 128);
     if (dtype == XLBB_F32)
-        darcy_moments_kernel<float><<<grid, 128, 0, XLBB_STREAM(stream)>>>(
+        launch_k(darcy_moments_kernel<float>, grid, 128, 0, XLBB_STREAM(stream), 
             geom(g), (const float*)f, (float)omega, (const float*)omega_field, (const float*)source,
             (const float*)ext_source, (float*)rho, (float*)grad);
     else if (dtype == XLBB_F64)
-        darcy_moments_kernel<double><<<grid, 128, 0, XLBB_STREAM(stream)>>>(
+        launch_k(darcy_moments_kernel<double>, grid, 128, 0, XLBB_STREAM(stream), 
             geom(g), (const double*)f, omega, (const double*)omega_field, (const double*)source,
             (const double*)ext_source, (double*)rho, (double*)grad);
     else return fail(XLBB_EUNSUPPORTED, "xlbb_darcy_moments: dtype");
@@ -1577,7 +1625,7 @@ int xlbb_restrict(int dtype_fine, int dtype_coarse, const XlbbGrid* fine, const 
     const dim3 grid = row_grid(coarse->nx, coarse->ny, 128);
     cudaStream_t st = XLBB_STREAM(stream);
 #define XLBB_R(TF, TC) \
-    restrict_kernel<TF, TC><<<grid, 128, 0, st>>>(geom(fine), geom(coarse), q, x0, y0, nfx / 2, nfy / 2, (const TF*)res, (TC*)r_coarse)
+    launch_k(restrict_kernel<TF, TC>, grid, 128, 0, st, geom(fine), geom(coarse), q, x0, y0, nfx / 2, nfy / 2, (const TF*)res, (TC*)r_coarse)
     if (dtype_fine == XLBB_F32 && dtype_coarse == XLBB_F32) XLBB_R(float, float);
     else if (dtype_fine == XLBB_F32 && dtype_coarse == XLBB_F64) XLBB_R(float, double);
     else if (dtype_fine == XLBB_F64 && dtype_coarse == XLBB_F64) XLBB_R(double, double);
@@ -1596,7 +1644,7 @@ int xlbb_prolong_add(int dtype_fine, int dtype_coarse, const XlbbGrid* fine, con
     const dim3 grid = row_grid(nfx, nfy, 128);
     cudaStream_t st = XLBB_STREAM(stream);
 #define XLBB_P(TF, TC) \
-    prolong_add_kernel<TF, TC><<<grid, 128, 0, st>>>(geom(fine), geom(coarse), q, x0, y0, nfx, nfy, (const TC*)f_coarse, (TF*)f_fine)
+    launch_k(prolong_add_kernel<TF, TC>, grid, 128, 0, st, geom(fine), geom(coarse), q, x0, y0, nfx, nfy, (const TC*)f_coarse, (TF*)f_fine)
     if (dtype_fine == XLBB_F32 && dtype_coarse == XLBB_F32) XLBB_P(float, float);
     else if (dtype_fine == XLBB_F32 && dtype_coarse == XLBB_F64) XLBB_P(float, double);
     else if (dtype_fine == XLBB_F64 && dtype_coarse == XLBB_F64) XLBB_P(double, double);
@@ -1617,10 +1665,10 @@ int xlbb_sumsq(int dtype, const XlbbGrid* g, int nplanes, const void* data, int 
         return fail(XLBB_EBADARG, "xlbb_sumsq: bad argument");
     const int nb = xlbb_sumsq_ctas(g);
     if (dtype == XLBB_F32)
-        sumsq_kernel<float><<<nb, 256, 0, XLBB_STREAM(stream)>>>(geom(g), nplanes, (const float*)data, bx0, bx1, by0,
+        launch_k(sumsq_kernel<float>, nb, 256, 0, XLBB_STREAM(stream), geom(g), nplanes, (const float*)data, bx0, bx1, by0,
                                                                  by1, partials);
     else if (dtype == XLBB_F64)
-        sumsq_kernel<double><<<nb, 256, 0, XLBB_STREAM(stream)>>>(geom(g), nplanes, (const double*)data, bx0, bx1,
+        launch_k(sumsq_kernel<double>, nb, 256, 0, XLBB_STREAM(stream), geom(g), nplanes, (const double*)data, bx0, bx1,
                                                                   by0, by1, partials);
     else return fail(XLBB_EUNSUPPORTED, "xlbb_sumsq: dtype");
     return check_launch("xlbb_sumsq");
@@ -1690,7 +1738,7 @@ int xlbb_darcy_sweep_residual_noalloc(int dtype, const XlbbGrid* g, const XlbbDa
 
 int xlbb_reduce_sum(const double* partials, int n, double* out, void* stream) {
     if (!partials || !out || n <= 0) return fail(XLBB_EBADARG, "xlbb_reduce_sum: bad argument");
-    reduce_sum_kernel<<<1, 1024, 0, XLBB_STREAM(stream)>>>(partials, n, out);
+    launch_k(reduce_sum_kernel, 1, 1024, 0, XLBB_STREAM(stream), partials, n, out);
     return check_launch("xlbb_reduce_sum");
 }
 
@@ -1700,10 +1748,10 @@ int xlbb_axpby(int dtype, long long n, double a, const void* x, double b, const 
     long long nb = (n + 255) / 256;
     if (nb > 8 * num_sms()) nb = 8 * num_sms();
     if (dtype == XLBB_F32)
-        axpby_kernel<float><<<(int)nb, 256, 0, XLBB_STREAM(stream)>>>(n, (float)a, (const float*)x, (float)b,
+        launch_k(axpby_kernel<float>, (int)nb, 256, 0, XLBB_STREAM(stream), n, (float)a, (const float*)x, (float)b,
                                                                       (const float*)y, (float*)out);
     else if (dtype == XLBB_F64)
-        axpby_kernel<double><<<(int)nb, 256, 0, XLBB_STREAM(stream)>>>(n, a, (const double*)x, b, (const double*)y,
+        launch_k(axpby_kernel<double>, (int)nb, 256, 0, XLBB_STREAM(stream), n, a, (const double*)x, b, (const double*)y,
                                                                        (double*)out);
     else return fail(XLBB_EUNSUPPORTED, "xlbb_axpby: dtype");
     return check_launch("xlbb_axpby");
@@ -1767,7 +1815,7 @@ static int batched_sweep_t(const void* inst, const XlbbBatchTile* tiles, int nti
                                                           (int)(blk.x * blk.y), 0);                           \
             resident = (per_sm > 0 ? per_sm : 1) * num_sms();                                                 \
         }                                                                                                     \
-        batched_push_kernel<T, R, Q_, S><<<ctas < resident ? ctas : resident, blk, 0, st>>>(                  \
+        launch_k(batched_push_kernel<T, R, Q_, S>, ctas < resident ? ctas : resident, blk, 0, st,                   \
             I, tiles, ntiles, T(a), T(b), mix, use_force, sumsq_diff, tile_sumsq);                            \
     } while (0)
         if (has_resid) { if (tile_sumsq) XLBB_BP(true, true); else XLBB_BP(true, false); }
@@ -1776,7 +1824,7 @@ static int batched_sweep_t(const void* inst, const XlbbBatchTile* tiles, int nti
         return check_launch("xlbb_batched_elast_sweep");
     }
 #define XLBB_B(R, P) \
-    batched_elast_kernel<T, 128, R, P, S><<<ctas, 160, 0, st>>>(I, tiles, ntiles, T(a), T(b), mix, use_force, \
+    launch_k(batched_elast_kernel<T, 128, R, P, S>, ctas, 160, 0, st, I, tiles, ntiles, T(a), T(b), mix, use_force, \
                                                                  sumsq_diff, tile_sumsq)
     if (has_resid) { if (prev) XLBB_B(true, true); else XLBB_B(true, false); }
     else { if (prev) XLBB_B(false, true); else XLBB_B(false, false); }
@@ -1801,7 +1849,7 @@ static int batched_sweep4_t(const void* inst, const XlbbBatchTile* tiles, int nt
                                                           (int)(blk.x * blk.y), 0);                           \
             resident = (per_sm > 0 ? per_sm : 1) * num_sms();                                                 \
         }                                                                                                     \
-        batched_push4_kernel<T, R, Q_><<<ctas < resident ? ctas : resident, blk, 0, st>>>(                    \
+        launch_k(batched_push4_kernel<T, R, Q_>, ctas < resident ? ctas : resident, blk, 0, st,                     \
             I, tiles, ntiles, T(a), T(b), mix, use_force, sumsq_diff, tile_sumsq);                            \
     } while (0)
     if (has_resid) { if (tile_sumsq) XLBB_BP4(true, true); else XLBB_BP4(true, false); }
@@ -1843,9 +1891,9 @@ int xlbb_batched_restrict(int dtype_fine, int dtype_coarse, const XlbbBatchTrans
     if (!tr_dev || ninst <= 0) return fail(XLBB_EBADARG, "xlbb_batched_restrict: bad argument");
     const dim3 grid(16, ninst);
     cudaStream_t st = XLBB_STREAM(stream);
-    if (dtype_fine == XLBB_F32 && dtype_coarse == XLBB_F32) batched_restrict_kernel<float, float><<<grid, 256, 0, st>>>(tr_dev);
-    else if (dtype_fine == XLBB_F32 && dtype_coarse == XLBB_F64) batched_restrict_kernel<float, double><<<grid, 256, 0, st>>>(tr_dev);
-    else if (dtype_fine == XLBB_F64 && dtype_coarse == XLBB_F64) batched_restrict_kernel<double, double><<<grid, 256, 0, st>>>(tr_dev);
+    if (dtype_fine == XLBB_F32 && dtype_coarse == XLBB_F32) launch_k(batched_restrict_kernel<float, float>, grid, 256, 0, st, tr_dev);
+    else if (dtype_fine == XLBB_F32 && dtype_coarse == XLBB_F64) launch_k(batched_restrict_kernel<float, double>, grid, 256, 0, st, tr_dev);
+    else if (dtype_fine == XLBB_F64 && dtype_coarse == XLBB_F64) launch_k(batched_restrict_kernel<double, double>, grid, 256, 0, st, tr_dev);
     else return fail(XLBB_EUNSUPPORTED, "xlbb_batched_restrict: dtype pair");
     return check_launch("xlbb_batched_restrict");
 }
@@ -1853,9 +1901,9 @@ int xlbb_batched_restrict(int dtype_fine, int dtype_coarse, const XlbbBatchTrans
 static int prolong_t(int dtype_fine, int dtype_coarse, const XlbbBatchTransfer* tr_dev, int ninst, double* parts,
                      cudaStream_t st) {
     const dim3 grid(XLBB_PROLONG_BLOCKS, ninst);
-    if (dtype_fine == XLBB_F32 && dtype_coarse == XLBB_F32) batched_prolong_add_kernel<float, float><<<grid, 256, 0, st>>>(tr_dev, parts);
-    else if (dtype_fine == XLBB_F32 && dtype_coarse == XLBB_F64) batched_prolong_add_kernel<float, double><<<grid, 256, 0, st>>>(tr_dev, parts);
-    else if (dtype_fine == XLBB_F64 && dtype_coarse == XLBB_F64) batched_prolong_add_kernel<double, double><<<grid, 256, 0, st>>>(tr_dev, parts);
+    if (dtype_fine == XLBB_F32 && dtype_coarse == XLBB_F32) launch_k(batched_prolong_add_kernel<float, float>, grid, 256, 0, st, tr_dev, parts);
+    else if (dtype_fine == XLBB_F32 && dtype_coarse == XLBB_F64) launch_k(batched_prolong_add_kernel<float, double>, grid, 256, 0, st, tr_dev, parts);
+    else if (dtype_fine == XLBB_F64 && dtype_coarse == XLBB_F64) launch_k(batched_prolong_add_kernel<double, double>, grid, 256, 0, st, tr_dev, parts);
     else return fail(XLBB_EUNSUPPORTED, "xlbb_batched_prolong_add: dtype pair");
     return check_launch("xlbb_batched_prolong_add");
 }
@@ -1871,13 +1919,13 @@ int xlbb_batched_prolong_add_norms(int dtype_fine, int dtype_coarse, const XlbbB
         return fail(XLBB_EBADARG, "xlbb_batched_prolong_add_norms: bad argument");
     const int st_ = prolong_t(dtype_fine, dtype_coarse, tr_dev, ninst, parts, XLBB_STREAM(stream));
     if (st_ != XLBB_OK) return st_;
-    prolong_norms_kernel<<<ninst, 32, 0, XLBB_STREAM(stream)>>>(parts, ninst, norms);
+    launch_k(prolong_norms_kernel, ninst, 32, 0, XLBB_STREAM(stream), parts, ninst, norms);
     return check_launch("xlbb_batched_prolong_add_norms");
 }
 
 int xlbb_segment_sum(const double* parts, const int* begin_dev, int nseg, double* out, void* stream) {
     if (!parts || !begin_dev || !out || nseg <= 0) return fail(XLBB_EBADARG, "xlbb_segment_sum: bad argument");
-    segment_sum_kernel<<<nseg, 256, 0, XLBB_STREAM(stream)>>>(parts, begin_dev, nseg, out);
+    launch_k(segment_sum_kernel, nseg, 256, 0, XLBB_STREAM(stream), parts, begin_dev, nseg, out);
     return check_launch("xlbb_segment_sum");
 }
 

@@ -92,6 +92,7 @@ struct ElastAdjArgs {
 
 template <typename T>
 __global__ void elast_sweep_adjoint_kernel(const ElastAdjArgs<T> p) {
+    grid_dep_wait();
     const SweepGeom& G = p.geom;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
@@ -205,6 +206,7 @@ struct DarcyAdjArgs {
 
 template <typename T>
 __global__ void darcy_sweep_adjoint_kernel(const DarcyAdjArgs<T> p) {
+    grid_dep_wait();
     const SweepGeom& G = p.geom;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
@@ -257,6 +259,7 @@ __global__ void darcy_sweep_adjoint_kernel(const DarcyAdjArgs<T> p) {
 // (G(q)(x) = sum_d K_d V_d(x), V_d(x) = q(x - c_d) or a rule of (q(x - c_d), q(x))).
 template <typename T>
 __global__ void gradient_adjoint_kernel(SweepGeom G, const T* lg, T scale, RulesView<T, 9> rules, T* lq) {
+    grid_dep_wait();
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
     if (x >= G.nx) return;
@@ -295,6 +298,7 @@ template <typename T>
 __global__ void elast_moments_adjoint_kernel(SweepGeom G, ElastMat<T> mat, T lam_u, T mu_u, T div_scale,
                                              const T* f, const T* lam_eta, const T* lam_div, T* lam_f,
                                              double* g_lam, double* g_mu) {
+    grid_dep_wait();
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
     if (x >= G.nx) return;
@@ -330,6 +334,7 @@ __global__ void elast_moments_adjoint_kernel(SweepGeom G, ElastMat<T> mat, T lam
 template <typename T>
 __global__ void darcy_moments_adjoint_kernel(SweepGeom G, const T* f, T omega, const T* omega_f, const T* lam_rho,
                                              const T* lam_grad, T* lam_f, double* g_omega) {
+    grid_dep_wait();
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
     if (x >= G.nx) return;
@@ -357,6 +362,7 @@ template <typename T>
 __global__ void divgrad_adjoint_kernel(SweepGeom G, ElastMat<T> mat, T lam_u, T mu_u, T div_scale, T scale,
                                        RulesView<T, 9> rules, const T* lg, const T* f, T* lam_f, T* lam_fe,
                                        double* g_lam, double* g_mu) {
+    grid_dep_wait();
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
     if (x >= G.nx) return;
@@ -447,7 +453,7 @@ int xlbb_elast_sweep_adjoint(int dtype, const XlbbGrid* g, const XlbbElastMateri
         a.mu_u = T(mat->mu);                                                        \
         a.pc = rules_view<T, 8>(s->pc);                                             \
         a.ps = rules_view<T, 8>(s->ps);                                             \
-        elast_sweep_adjoint_kernel<T><<<grid, 128, 0, st>>>(a);                     \
+        launch_k(elast_sweep_adjoint_kernel<T>, grid, 128, 0, st, a);                     \
     }
     if (dtype == XLBB_F32) XLBB_ADJ(float)
     else if (dtype == XLBB_F64) XLBB_ADJ(double)
@@ -479,7 +485,7 @@ int xlbb_darcy_sweep_adjoint(int dtype, const XlbbGrid* g, const XlbbDarcySweepA
         a.ext = (const T*)s->ext_source;                              \
         a.pc = rules_view<T, 9>(s->pc);                               \
         a.ps = rules_view<T, 9>(s->ps);                               \
-        darcy_sweep_adjoint_kernel<T><<<grid, 128, 0, st>>>(a);       \
+        launch_k(darcy_sweep_adjoint_kernel<T>, grid, 128, 0, st, a);       \
     }
     if (dtype == XLBB_F32) XLBB_ADJ(float)
     else if (dtype == XLBB_F64) XLBB_ADJ(double)
@@ -496,10 +502,10 @@ int xlbb_darcy_gradient_adjoint(int dtype, const XlbbGrid* g, const void* lam_gr
     const dim3 grid((g->nx + 127) / 128, g->ny);
     cudaStream_t st = XLBB_STREAM(stream);
     if (dtype == XLBB_F32)
-        gradient_adjoint_kernel<float><<<grid, 128, 0, st>>>(geom(g), (const float*)lam_grad, (float)scale,
+        launch_k(gradient_adjoint_kernel<float>, grid, 128, 0, st, geom(g), (const float*)lam_grad, (float)scale,
                                                              rules_view<float, 9>(*rules), (float*)lam_q);
     else if (dtype == XLBB_F64)
-        gradient_adjoint_kernel<double><<<grid, 128, 0, st>>>(geom(g), (const double*)lam_grad, scale,
+        launch_k(gradient_adjoint_kernel<double>, grid, 128, 0, st, geom(g), (const double*)lam_grad, scale,
                                                               rules_view<double, 9>(*rules), (double*)lam_q);
     else return fail(XLBB_EUNSUPPORTED, "xlbb_darcy_gradient_adjoint: dtype");
     return check_launch("xlbb_darcy_gradient_adjoint");
@@ -515,11 +521,11 @@ int xlbb_elast_moments_adjoint(int dtype, const XlbbGrid* g, const XlbbElastMate
     const dim3 grid((g->nx + 127) / 128, g->ny);
     cudaStream_t st = XLBB_STREAM(stream);
     if (dtype == XLBB_F32)
-        elast_moments_adjoint_kernel<float><<<grid, 128, 0, st>>>(
+        launch_k(elast_moments_adjoint_kernel<float>, grid, 128, 0, st, 
             geom(g), make_mat<float>(mat), (float)mat->lam, (float)mat->mu, (float)div_scale, (const float*)f,
             (const float*)lam_eta, (const float*)lam_div, (float*)lam_f, g_lam, g_mu);
     else if (dtype == XLBB_F64)
-        elast_moments_adjoint_kernel<double><<<grid, 128, 0, st>>>(
+        launch_k(elast_moments_adjoint_kernel<double>, grid, 128, 0, st, 
             geom(g), make_mat<double>(mat), mat->lam, mat->mu, div_scale, (const double*)f,
             (const double*)lam_eta, (const double*)lam_div, (double*)lam_f, g_lam, g_mu);
     else return fail(XLBB_EUNSUPPORTED, "xlbb_elast_moments_adjoint: dtype");
@@ -535,11 +541,11 @@ int xlbb_darcy_moments_adjoint(int dtype, const XlbbGrid* g, const void* f, doub
     const dim3 grid((g->nx + 127) / 128, g->ny);
     cudaStream_t st = XLBB_STREAM(stream);
     if (dtype == XLBB_F32)
-        darcy_moments_adjoint_kernel<float><<<grid, 128, 0, st>>>(
+        launch_k(darcy_moments_adjoint_kernel<float>, grid, 128, 0, st, 
             geom(g), (const float*)f, (float)omega, (const float*)omega_field, (const float*)lam_rho,
             (const float*)lam_grad, (float*)lam_f, g_omega);
     else if (dtype == XLBB_F64)
-        darcy_moments_adjoint_kernel<double><<<grid, 128, 0, st>>>(
+        launch_k(darcy_moments_adjoint_kernel<double>, grid, 128, 0, st, 
             geom(g), (const double*)f, omega, (const double*)omega_field, (const double*)lam_rho,
             (const double*)lam_grad, (double*)lam_f, g_omega);
     else return fail(XLBB_EUNSUPPORTED, "xlbb_darcy_moments_adjoint: dtype");
@@ -558,12 +564,12 @@ int xlbb_divgrad_adjoint(int dtype, const XlbbGrid* g, const XlbbElastMaterial* 
     cudaStream_t st = XLBB_STREAM(stream);
     const double div_scale = -1.5 / (3.0 * (mat->lam + mat->mu) + 1.0);
     if (dtype == XLBB_F32)
-        divgrad_adjoint_kernel<float><<<grid, 128, 0, st>>>(
+        launch_k(divgrad_adjoint_kernel<float>, grid, 128, 0, st, 
             geom(g), make_mat<float>(mat), (float)mat->lam, (float)mat->mu, (float)div_scale, (float)scale,
             rules_view<float, 9>(*rules), (const float*)lam_ext, (const float*)f, (float*)lam_f, (float*)lam_fe,
             g_lam, g_mu);
     else if (dtype == XLBB_F64)
-        divgrad_adjoint_kernel<double><<<grid, 128, 0, st>>>(
+        launch_k(divgrad_adjoint_kernel<double>, grid, 128, 0, st, 
             geom(g), make_mat<double>(mat), mat->lam, mat->mu, div_scale, scale, rules_view<double, 9>(*rules),
             (const double*)lam_ext, (const double*)f, (double*)lam_f, (double*)lam_fe, g_lam, g_mu);
     else return fail(XLBB_EUNSUPPORTED, "xlbb_divgrad_adjoint: dtype");

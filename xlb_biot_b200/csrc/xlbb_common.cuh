@@ -68,6 +68,12 @@ __device__ __forceinline__ T rule_value(uint8_t code, T cur, T src_val, T cst) {
 
 __device__ __forceinline__ int wrap(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
 
+// Programmatic dependent launch: a kernel launched with programmatic stream
+// serialization may be scheduled while its predecessor in the stream is still
+// draining; it waits here, before touching any memory, until the predecessor
+// has finished and its writes are visible (a no-op for an ordinary launch).
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // Block-wide FP64 sum (blockDim.x multiple of 32, <= 1024).
 __device__ __forceinline__ double block_sum(double v, double* sh) {
 #pragma unroll

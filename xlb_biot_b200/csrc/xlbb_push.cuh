@@ -92,6 +92,7 @@ __device__ __forceinline__ double push_cell(const typename Phys::Args& p, int y,
 
 template <class Phys, bool SUMSQ>
 __global__ void __launch_bounds__(256) push_kernel(const typename Phys::Args p) {
+    grid_dep_wait();
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y;
     if constexpr (SUMSQ) {        // one FP64 partial per block

@@ -155,6 +155,7 @@ __device__ __forceinline__ double sweep_strip(const typename Phys::Args& p, int 
 
 template <class Phys, int TX, int D, bool PREV>
 __global__ void __launch_bounds__(TX + 32) sweep_kernel(const typename Phys::Args p) {
+    grid_dep_wait();
     using T = typename Phys::T;
     constexpr int Q = Phys::Q;
     __shared__ T post[4][Q][TX + 2];
@@ -236,6 +237,7 @@ __host__ __device__ constexpr size_t bulk_smem_bytes(int np) {
 // registers, so deeper rings fit.  Requires 16-byte aligned planes and pitch.
 template <class Phys, int TX, int D, bool PREV>
 __global__ void __launch_bounds__(TX + 32) sweep_bulk_kernel(const typename Phys::Args p) {
+    grid_dep_wait();
     using T = typename Phys::T;
     constexpr int Q = Phys::Q;
     constexpr int NT = TX + 2;
@@ -398,6 +400,7 @@ namespace xlbb {
 // blocks / strips).
 template <class Phys, int D, bool PREV>
 __global__ void __launch_bounds__(128) sweep_warp_kernel(const typename Phys::Args p, int nbx, int nstrips) {
+    grid_dep_wait();
     using T = typename Phys::T;
     constexpr int Q = Phys::Q;
     constexpr int W = 30;
