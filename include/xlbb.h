@@ -194,6 +194,18 @@ int xlbb_elast_moments(int dtype, const XlbbGrid* g, const XlbbElastMaterial* ma
                        const void* f, const void* force, const void* fext,
                        void* eta, void* sigma, void* div, double div_scale, void* stream);
 
+/*
+ * The Biot coupling force out = base + G(div(f), scale) in one kernel: the
+ * divergence of xlbb_elast_moments followed by the gradient of
+ * xlbb_darcy_gradient (with its rules), bit for bit, without the divergence's
+ * round trip through memory (poroelasticity's nonlinear force,
+ * src/poroelasticity.py:324, evaluated before every elasticity sweep).
+ * base may be NULL; out must not alias f.
+ */
+int xlbb_elast_divgrad(int dtype, const XlbbGrid* g, const XlbbElastMaterial* mat, double div_scale,
+                       const void* f, double scale, const XlbbRules* rules, const void* base,
+                       void* out, void* stream);
+
 /* Elasticity equilibrium (LBMElasticity.equilibrium :909-957). */
 int xlbb_elast_equilibrium(int dtype, const XlbbGrid* g, const XlbbElastMaterial* mat,
                            const void* eta, const void* sigma, const void* force,

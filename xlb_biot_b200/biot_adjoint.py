@@ -69,8 +69,7 @@ class BiotAdjointModel:
 
     # ------------------------------------------------------------------ forward
     def _N(self, f, level, fe):
-        div = self.el.update_divergence(f, level)
-        return self.da.gradient(div, self.sN, base=fe, dtype=div.dtype)
+        return self.el.coupling_force(f, level, self.da, self.sN, base=fe)
 
     def _vcycle(self, f, level, resid, fe, rec):
         """``LBMElasticity._mg_step`` with the coupling force N(f); appends the

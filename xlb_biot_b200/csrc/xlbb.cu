@@ -592,6 +592,35 @@ static XlbbSweepConfig effective_cfg(int kernel, int dtype) {
 // ---------------------------------------------------------------------------
 // Small kernels: gradient, moments, equilibrium, transfers, reductions.
 // ---------------------------------------------------------------------------
+// src/darcy.py:104: grad = sum_i p_i * (-3 * scale * w_i * c_i), each term with
+// one fused multiply-add (the same rounding in every kernel that forms it).
+template <typename T>
+__device__ __forceinline__ void gradient_sum(const T (&v)[9], T scale, T& gx, T& gy) {
+    gx = T(0);
+    gy = T(0);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+        const T k = T(-3) * scale * w9<T>(i);
+        gx = fma(v[i], k * T(cx9(i)), gx);
+        gy = fma(v[i], k * T(cy9(i)), gy);
+    }
+}
+
+// Divergence moment of the populations of the cell at offset o
+// (src/elasticity.py:1040-1058): c * m2 with c = -1.5 / (3 (lambda + mu) + 1).
+template <typename T>
+__device__ __forceinline__ T elast_div_at(const T* f, long long P, size_t o, const ElastMat<T>& mat, T lam, T mu,
+                                          T div_scale) {
+    T v[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) v[i] = f[o + i * P];
+    const T m2 = v[0] + v[1] + v[2] + v[3] + T(2) * (v[4] + v[5] + v[6] + v[7]);
+    T l = lam, m = mu;
+    if (mat.mu_f) { l = mat.lam_f[o]; m = mat.mu_f[o]; }
+    const T c = mat.mu_f ? T(-1.5) / (T(3) * (l + m) + T(1)) : div_scale;
+    return c * m2;
+}
+
 template <typename T>
 __global__ void gradient_kernel(SweepGeom G, const T* q, T scale, RulesView<T, 9> rules, const T* base, T* out) {
     grid_dep_wait();
@@ -614,14 +643,8 @@ __global__ void gradient_kernel(SweepGeom G, const T* q, T scale, RulesView<T, 9
             v[d] = rule_value<T, 9>(code, v[d], qc, rules.cst[(size_t)r * 9 + d]);
         }
     }
-    // src/darcy.py:104: sum_i p_i * (-3 * scale * w_i * c_i)
-    T gx = T(0), gy = T(0);
-#pragma unroll
-    for (int i = 0; i < 9; ++i) {
-        const T k = T(-3) * scale * w9<T>(i);
-        gx += v[i] * (k * T(cx9(i)));
-        gy += v[i] * (k * T(cy9(i)));
-    }
+    T gx, gy;
+    gradient_sum<T>(v, scale, gx, gy);
     if (base) {
         gx = base[o] + gx;
         gy = base[o + G.plane] + gy;
@@ -664,10 +687,52 @@ __global__ void elast_moments_kernel(SweepGeom G, ElastMat<T> mat, T lam, T mu, 
         sigma[o + P] = (T(2) * cd) * m4;
         sigma[o + 2 * P] = ms - md;
     }
-    if (div) {
-        const T c = mat.mu_f ? T(-1.5) / (T(3) * (l + m) + T(1)) : div_scale;
-        div[o] = c * m2;
+    if (div) div[o] = elast_div_at<T>(f, P, o, mat, lam, mu, div_scale);
+}
+
+// The Biot coupling force ext = base + G(div(f)) in one kernel: a 32 x 8 block
+// forms the divergence of its cells and a one-cell halo (periodic wrap) in
+// shared memory, then applies the Darcy gradient stencil with its boundary
+// rules -- the arithmetic of elast_moments_kernel's divergence followed by
+// gradient_kernel, without the divergence's round trip through memory or the
+// second launch.
+template <typename T>
+__global__ void __launch_bounds__(256) elast_divgrad_kernel(SweepGeom G, ElastMat<T> mat, T lam, T mu, T div_scale,
+                                                            const T* f, T scale, RulesView<T, 9> rules, const T* base,
+                                                            T* out) {
+    grid_dep_wait();
+    constexpr int BX = 32, BY = 8;
+    __shared__ T q[BY + 2][BX + 2];
+    const int x0 = blockIdx.x * BX, y0 = blockIdx.y * BY;
+    for (int k = threadIdx.y * BX + threadIdx.x; k < (BX + 2) * (BY + 2); k += BX * BY) {
+        const int lx = k % (BX + 2), ly = k / (BX + 2);
+        const int xs = ((x0 + lx - 1) % G.nx + G.nx) % G.nx, ys = ((y0 + ly - 1) % G.ny + G.ny) % G.ny;
+        q[ly][lx] = elast_div_at<T>(f, G.plane, (size_t)ys * G.pitch + xs, mat, lam, mu, div_scale);
     }
+    __syncthreads();
+    const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
+    if (x >= G.nx || y >= G.ny) return;
+    T v[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) v[i] = q[threadIdx.y + 1 - cy9(i)][threadIdx.x + 1 - cx9(i)];
+    const size_t o = (size_t)y * G.pitch + x;
+    const int r = find_rule(rules, y, x);
+    if (r >= 0) {
+        const T qc = q[threadIdx.y + 1][threadIdx.x + 1];
+#pragma unroll
+        for (int d = 0; d < 9; ++d) {
+            const uint8_t code = __ldg(rules.code + (size_t)r * 9 + d);
+            v[d] = rule_value<T, 9>(code, v[d], qc, rules.cst[(size_t)r * 9 + d]);
+        }
+    }
+    T gx, gy;
+    gradient_sum<T>(v, scale, gx, gy);
+    if (base) {
+        gx = base[o] + gx;
+        gy = base[o + G.plane] + gy;
+    }
+    out[o] = gx;
+    out[o + G.plane] = gy;
 }
 
 template <typename T>
@@ -1581,6 +1646,24 @@ int xlbb_elast_moments(int dtype, const XlbbGrid* g, const XlbbElastMaterial* ma
             (const double*)fext, (double*)eta, (double*)sigma, (double*)div, div_scale);
     else return fail(XLBB_EUNSUPPORTED, "xlbb_elast_moments: dtype");
     return check_launch("xlbb_elast_moments");
+}
+
+int xlbb_elast_divgrad(int dtype, const XlbbGrid* g, const XlbbElastMaterial* mat, double div_scale, const void* f,
+                       double scale, const XlbbRules* rules, const void* base, void* out, void* stream) {
+    if (!grid_ok(g) || !mat || !f || !out) return fail(XLBB_EBADARG, "xlbb_elast_divgrad: bad argument");
+    XlbbRules none = {0, nullptr, nullptr, nullptr, nullptr};
+    const XlbbRules& r = rules ? *rules : none;
+    const dim3 grid((g->nx + 31) / 32, (g->ny + 7) / 8), blk(32, 8);
+    if (dtype == XLBB_F32)
+        launch_k(elast_divgrad_kernel<float>, grid, blk, 0, XLBB_STREAM(stream), geom(g), make_mat<float>(mat),
+                 (float)mat->lam, (float)mat->mu, (float)div_scale, (const float*)f, (float)scale,
+                 rules_view<float, 9>(r), (const float*)base, (float*)out);
+    else if (dtype == XLBB_F64)
+        launch_k(elast_divgrad_kernel<double>, grid, blk, 0, XLBB_STREAM(stream), geom(g), make_mat<double>(mat),
+                 mat->lam, mat->mu, div_scale, (const double*)f, scale, rules_view<double, 9>(r),
+                 (const double*)base, (double*)out);
+    else return fail(XLBB_EUNSUPPORTED, "xlbb_elast_divgrad: dtype");
+    return check_launch("xlbb_elast_divgrad");
 }
 
 int xlbb_elast_equilibrium(int dtype, const XlbbGrid* g, const XlbbElastMaterial* mat, const void* eta,

@@ -457,6 +457,21 @@ class LBMElasticity:
             self._div_scale, _lib.stream_ptr()), "xlbb_elast_moments")
         return div
 
+    def coupling_force(self, f, level, darcy, scale, base=None):
+        """``base + darcy.gradient(self.update_divergence(f, level), scale)`` on
+        multigrid level ``level`` in that level's precision, in one kernel
+        (``xlbb_elast_divgrad``: the same values bit for bit).  The poroelastic
+        coupling force of ``src/poroelasticity.py:324``."""
+        L = self._L(level)
+        f = self._f(f, level)
+        base = L.field(base, 2)
+        out = L.empty(2)
+        rules = darcy.gradient_rules(L.nx, L.ny, L.dtype)
+        _lib.check(_lib.lib().xlbb_elast_divgrad(
+            _lib.dtype_code(L.dtype), L.grid(), self._mats[level], self._div_scale, _lib.ptr(f), float(scale),
+            rules.struct(), _lib.ptr(base), _lib.ptr(out), _lib.stream_ptr()), "xlbb_elast_divgrad")
+        return out
+
     def _level_of(self, f):
         shape = tuple(f.shape[:2])
         for level in range(self.levels):

@@ -27,9 +27,9 @@ class DivGradForce:
 
     def evaluate(self, el, f, level, external_force):
         """external_force + N(f) on multigrid level ``level``, computed in that
-        level's precision (the precision of the sweep that consumes it)."""
-        div = el.update_divergence(f, level)
-        return self.darcy.gradient(div, self.scale, base=external_force, dtype=div.dtype)
+        level's precision (the precision of the sweep that consumes it), by the
+        fused divergence-gradient kernel."""
+        return el.coupling_force(f, level, self.darcy, self.scale, base=external_force)
 
 
 class BiotStepGraph:
