@@ -803,10 +803,11 @@ __global__ void darcy_moments_kernel(SweepGeom G, const T* f, T omega, const T* 
 // Tf: fine-level type, Tc: coarse-level type (a multigrid may run its coarsest
 // level in FP64 under FP32 levels; the sum is formed in the wider type).
 template <typename Tf, typename Tc>
-__global__ void restrict_kernel(SweepGeom F, SweepGeom C, int q, int x0, int y0, int nix, int niy, const Tf* res,
-                                Tc* rc) {
+__global__ void restrict_kernel(SweepGeom F, SweepGeom C, int q, int x0, int y0, int nix, int niy,
+                                const Tf* __restrict__ res, Tc* __restrict__ rc) {
     grid_dep_wait();
-    // one thread per coarse cell (all q planes); zero outside the coarse interior
+    // one thread per coarse cell (all q planes); zero outside the coarse interior;
+    // every plane's loads are issued before the first store (up to 9 planes at once)
     using Ts = typename std::conditional<(sizeof(Tf) > sizeof(Tc)), Tf, Tc>::type;
     const int X = blockIdx.x * blockDim.x + threadIdx.x;
     const int Y = blockIdx.y;
@@ -814,27 +815,46 @@ __global__ void restrict_kernel(SweepGeom F, SweepGeom C, int q, int x0, int y0,
     const size_t oc = (size_t)Y * C.pitch + X;
     const int I = X - x0, J = Y - y0;
     const bool inside = I >= 0 && I < nix && J >= 0 && J < niy;
-    for (int i = 0; i < q; ++i) {
-        Ts v = Ts(0);
-        if (inside) {
-            const size_t of = (size_t)(y0 + 2 * J) * F.pitch + (x0 + 2 * I) + (size_t)i * F.plane;
-            const Ts a = res[of], b = res[of + 1], c = res[of + F.pitch], d = res[of + F.pitch + 1];
-            v = a + c + b + d;
+    const size_t of = inside ? (size_t)(y0 + 2 * J) * F.pitch + (x0 + 2 * I) : 0;
+    for (int i0 = 0; i0 < q; i0 += 9) {
+        Ts v[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            v[k] = Ts(0);
+            if (inside && i0 + k < q) {
+                const Tf* s = res + of + (size_t)(i0 + k) * F.plane;
+                const Ts a = __ldg(s), b = __ldg(s + 1), c = __ldg(s + F.pitch), d = __ldg(s + F.pitch + 1);
+                v[k] = a + c + b + d;
+            }
         }
-        rc[oc + (size_t)i * C.plane] = Tc(v);
+#pragma unroll
+        for (int k = 0; k < 9; ++k)
+            if (i0 + k < q) rc[oc + (size_t)(i0 + k) * C.plane] = Tc(v[k]);
     }
 }
 
 template <typename Tf, typename Tc>
 __global__ void prolong_add_kernel(SweepGeom F, SweepGeom C, int q, int x0, int y0, int nfx, int nfy,
-                                   const Tc* fc, Tf* ff) {
+                                   const Tc* __restrict__ fc, Tf* __restrict__ ff) {
     grid_dep_wait();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y;
     if (i >= nfx || j >= nfy) return;
     const size_t of = (size_t)(y0 + j) * F.pitch + (x0 + i);
     const size_t oc = (size_t)(y0 + j / 2) * C.pitch + (x0 + i / 2);
-    for (int k = 0; k < q; ++k) ff[of + (size_t)k * F.plane] = Tf(ff[of + (size_t)k * F.plane] + fc[oc + (size_t)k * C.plane]);
+    for (int k0 = 0; k0 < q; k0 += 9) {      // loads of up to 9 planes before the stores
+        Tf a[9];
+        Tc c[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k)
+            if (k0 + k < q) {
+                a[k] = ff[of + (size_t)(k0 + k) * F.plane];
+                c[k] = __ldg(fc + oc + (size_t)(k0 + k) * C.plane);
+            }
+#pragma unroll
+        for (int k = 0; k < 9; ++k)
+            if (k0 + k < q) ff[of + (size_t)(k0 + k) * F.plane] = Tf(a[k] + c[k]);
+    }
 }
 
 template <typename T>
@@ -1454,18 +1474,21 @@ template <typename Tf, typename Tc>
 __global__ void batched_restrict_kernel(const XlbbBatchTransfer* __restrict__ tr) {
     grid_dep_wait();
     const XlbbBatchTransfer T_ = tr[blockIdx.y];
-    const Tf* res = static_cast<const Tf*>(T_.fine);
-    Tc* rc = static_cast<Tc*>(T_.coarse);
+    const Tf* __restrict__ res = static_cast<const Tf*>(T_.fine);
+    Tc* __restrict__ rc = static_cast<Tc*>(T_.coarse);
     using Ts = typename std::conditional<(sizeof(Tf) > sizeof(Tc)), Tf, Tc>::type;
     const int ncx = T_.nx_f / 2, ncy = T_.ny_f / 2;
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < ncx * ncy; e += gridDim.x * blockDim.x) {
         const int X = e % ncx, Y = e / ncx;
         const size_t of = (size_t)(2 * Y) * T_.pitch_f + 2 * X, oc = (size_t)Y * T_.pitch_c + X;
+        Ts v[8];      // every plane's loads before the first store
+#pragma unroll
         for (int i = 0; i < 8; ++i) {
             const Tf* s = res + of + (size_t)i * T_.plane_f;
-            const Ts v = Ts(s[0]) + Ts(s[T_.pitch_f]) + Ts(s[1]) + Ts(s[T_.pitch_f + 1]);
-            rc[oc + (size_t)i * T_.plane_c] = Tc(v);
+            v[i] = Ts(__ldg(s)) + Ts(__ldg(s + T_.pitch_f)) + Ts(__ldg(s + 1)) + Ts(__ldg(s + T_.pitch_f + 1));
         }
+#pragma unroll
+        for (int i = 0; i < 8; ++i) rc[oc + (size_t)i * T_.plane_c] = Tc(v[i]);
     }
 }
 
@@ -1477,17 +1500,24 @@ __global__ void batched_prolong_add_kernel(const XlbbBatchTransfer* __restrict__
     grid_dep_wait();
     __shared__ double red[8];
     const XlbbBatchTransfer T_ = tr[blockIdx.y];
-    Tf* ff = static_cast<Tf*>(const_cast<void*>(T_.fine));
-    const Tc* fc = static_cast<const Tc*>(T_.coarse);
+    Tf* __restrict__ ff = static_cast<Tf*>(const_cast<void*>(T_.fine));
+    const Tc* __restrict__ fc = static_cast<const Tc*>(T_.coarse);
     double cc = 0.0, nn = 0.0;
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < T_.nx_f * T_.ny_f; e += gridDim.x * blockDim.x) {
         const int x = e % T_.nx_f, y = e / T_.nx_f;
         const size_t of = (size_t)y * T_.pitch_f + x, oc = (size_t)(y / 2) * T_.pitch_c + x / 2;
+        Tf a[8];      // every plane's loads before the first store
+        Tc c[8];
+#pragma unroll
         for (int i = 0; i < 8; ++i) {
-            const Tc c = fc[oc + (size_t)i * T_.plane_c];
-            const Tf v = Tf(ff[of + (size_t)i * T_.plane_f] + c);
+            a[i] = ff[of + (size_t)i * T_.plane_f];
+            c[i] = __ldg(fc + oc + (size_t)i * T_.plane_c);
+        }
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const Tf v = Tf(a[i] + c[i]);
             ff[of + (size_t)i * T_.plane_f] = v;
-            cc += (double)c * (double)c;
+            cc += (double)c[i] * (double)c[i];
             nn += (double)v * (double)v;
         }
     }
