@@ -81,7 +81,12 @@ typedef struct {
  *      rows in registers, streaming by warp shuffles, no barrier; register
  *      prefetch of depth (1, 2) rows; ctas_per_sm counts CTAs of 4 warps;
  *   3: collide and push (the default): one thread per cell, CTAs of tx
- *      columns of one row; depth, ctas_per_sm and min_rows are not used.
+ *      columns of one row; depth, ctas_per_sm and min_rows are not used;
+ *   4: as 3, except that FP32 elasticity sweeps of
+ *      at least 64 K cells without boundary rules, per-cell material, side
+ *      outputs or fused sums, with at most one force array and 16-byte
+ *      aligned rows and planes, run four columns per lane (float4 loads and
+ *      stores, streaming along x by warp shuffles); same results.
  * FP64 sweeps cap tx at 128.
  */
 typedef struct {
@@ -135,6 +140,10 @@ typedef struct {
 int xlbb_elast_sweep(int dtype, const XlbbGrid* g, const XlbbElastMaterial* mat,
                      const XlbbElastSweep* s, void* stream);
 int xlbb_elast_sweep_ctas(int dtype, const XlbbGrid* g);   /* CTAs of the next launch of this dtype */
+/* The pipeline (XlbbSweepConfig numbering; 0 for the row-marching kernel)
+ * that xlbb_elast_sweep would run for these arguments now (diagnostic). */
+int xlbb_elast_sweep_pipeline(int dtype, const XlbbGrid* g, const XlbbElastMaterial* mat,
+                              const XlbbElastSweep* s);
 
 /*
  * One D2Q9 advection-diffusion-reaction BGK sweep (AdvectionDiffusionReactionBGK.step,

@@ -89,6 +89,7 @@ D = ctypes.c_double
 PG = ctypes.POINTER(Grid)
 SIGNATURES = {
     "xlbb_elast_sweep": (I, [I, PG, ctypes.POINTER(ElastMaterial), ctypes.POINTER(ElastSweep), P]),
+    "xlbb_elast_sweep_pipeline": (I, [I, PG, ctypes.POINTER(ElastMaterial), ctypes.POINTER(ElastSweep)]),
     "xlbb_elast_sweep_ctas": (I, [I, PG]),
     "xlbb_darcy_sweep": (I, [I, PG, ctypes.POINTER(DarcySweep), P]),
     "xlbb_darcy_sweep_ctas": (I, [I, PG]),

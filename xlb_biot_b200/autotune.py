@@ -18,7 +18,7 @@ from . import _lib
 ELASTICITY, DARCY = 0, 1
 TX = (128, 256)
 # per pipeline: CTA+registers / CTA+bulk ring / warps / collide-and-push (one thread per cell)
-DEPTH = {0: (1, 2), 1: (2, 4, 6), 2: (1, 2), 3: (1,)}
+DEPTH = {0: (1, 2), 1: (2, 4, 6), 2: (1, 2), 3: (1,), 4: (1,)}
 CTAS_PER_SM = (1, 2, 3, 4, 6)
 MIN_ROWS = (8, 16, 32)
 
@@ -37,12 +37,14 @@ def set_config(kernel, tx, depth, ctas_per_sm, min_rows, pipeline=0):
 
 def candidates(dtype_bytes=4):
     """Every launch shape the library instantiates for the given element size
-    (pipeline 3 ignores depth, CTAs per SM and strip height)."""
+    (pipelines 3 and 4 ignore depth, CTAs per SM and strip height; pipeline 4,
+    the four-column form of eligible FP32 elasticity sweeps, is pipeline 3
+    for every other sweep)."""
     out = []
     for pipe, depths in DEPTH.items():
-        ctas, rows = (CTAS_PER_SM, MIN_ROWS) if pipe != 3 else ((1,), (8,))   # pipeline 3: only tx matters
+        ctas, rows = (CTAS_PER_SM, MIN_ROWS) if pipe < 3 else ((1,), (8,))   # pipelines 3, 4: only tx matters
         for t, d, c, m in itertools.product(TX if pipe != 2 else (128,), depths, ctas, rows):
-            if dtype_bytes == 8 and (t > 128 or d > 4):
+            if dtype_bytes == 8 and (t > 128 or d > 4 or pipe == 4):
                 continue
             out.append(dict(tx=t, depth=d, ctas_per_sm=c, min_rows=m, pipeline=pipe))
     return out

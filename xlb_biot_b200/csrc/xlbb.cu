@@ -104,6 +104,8 @@ static bool rules_ok(const XlbbRules& r, const XlbbGrid* g) {
 
 // Launch shapes of the sweeps, per kernel family (0: elasticity, 1: Darcy):
 // collide-and-push by default (sweeps with fused reductions use push_fallback).
+// (pipeline 4 measured no faster than 3 on single 1 M-cell grids: 3.5 waves of
+// its 512-thread CTAs; it stays a launch shape the autotuner can pick)
 static XlbbSweepConfig g_cfg[2] = {{128, 1, 1, 8, 3}, {128, 1, 1, 8, 3}};
 
 static constexpr int WARP_COLS = 30;   // output columns of one warp of sweep_warp_kernel
@@ -111,7 +113,7 @@ static constexpr int WARP_COLS = 30;   // output columns of one warp of sweep_wa
 static bool cfg_ok(const XlbbSweepConfig& c) {
     const bool depth_ok = c.pipeline == 1 ? (c.depth == 2 || c.depth == 4 || c.depth == 6) : (c.depth == 1 || c.depth == 2);
     return (c.tx == 128 || c.tx == 256) && depth_ok && c.ctas_per_sm >= 1 && c.ctas_per_sm <= 32 &&
-           c.min_rows >= 1 && c.pipeline >= 0 && c.pipeline <= 3;
+           c.min_rows >= 1 && c.pipeline >= 0 && c.pipeline <= 4;
 }
 
 // Pipeline 3 (collide-and-push) runs sweeps without fused reductions; the
@@ -581,6 +583,7 @@ static void launch_sweep_regs(const XlbbSweepConfig& c, const XlbbGrid* g, cudaS
 // pipeline, depth <= 2).
 static XlbbSweepConfig effective_cfg(int kernel, int dtype) {
     XlbbSweepConfig c = g_cfg[kernel];
+    if (c.pipeline == 4) c.pipeline = 3;   // the four-column form is chosen per sweep (launch_elast)
     if ((dtype == XLBB_F64 || dtype == XLBB_F32_ACC64) && c.tx > 128) c.tx = 128;
     if (dtype == XLBB_F32_ACC64 && (c.pipeline == 1 || c.pipeline == 2)) {
         c.pipeline = 0;
@@ -904,50 +907,6 @@ static ElastMat<T, S> make_mat(const XlbbElastMaterial* m) {
     return e;
 }
 
-template <typename T, bool RESID, bool PREV, typename S = T>
-static int launch_elast(const XlbbGrid* g, const XlbbElastMaterial* mat, const XlbbElastSweep* s, cudaStream_t st) {
-    using Ph = ElastPhys<T, RESID, S>;
-    typename Ph::Args a;
-    a.geom = geom(g);
-    a.f_in = static_cast<const S*>(s->f_in);
-    a.f_out = static_cast<S*>(s->f_out);
-    a.force = s->use_force ? static_cast<const S*>(s->force) : nullptr;
-    a.fext = static_cast<const S*>(s->fext);
-    a.resid = static_cast<const S*>(s->resid);
-    a.a = T(s->a);
-    a.b = T(s->b);
-    a.mix = (s->a == 0.0 && s->b == 1.0) ? 0 : 1;
-    a.sumsq_diff = (s->sumsq != nullptr && s->sumsq_diff) ? 1 : 0;
-    a.mat = make_mat<T, S>(mat);
-    a.pc = rules_view<T, 8>(s->pc);
-    a.ps = rules_view<T, 8>(s->ps);
-    a.sumsq = s->sumsq;
-    a.bx0 = s->bx0; a.bx1 = s->bx1; a.by0 = s->by0; a.by1 = s->by1;
-    a.div_out = static_cast<S*>(s->div_out);
-    a.div_scale = T(-1.5 / (3.0 * (mat->lam + mat->mu) + 1.0));
-    if constexpr (sizeof(T) != sizeof(S)) {
-        const XlbbSweepConfig c = effective_cfg(0, XLBB_F32_ACC64);
-        if (c.pipeline == 3 && Ph::push_ok(a) && (a.ps.count == 0 || a.ps.push != nullptr)) {
-            Ph::fill_ptrs(a);
-            launch_push<Ph>(c, g, st, a);
-        } else {
-            launch_sweep_regs<Ph, PREV>(c, g, st, a);
-        }
-    } else {
-        const XlbbSweepConfig c = effective_cfg(0, sizeof(T) == 4 ? XLBB_F32 : XLBB_F64);
-        launch_sweep<Ph, PREV>(c, g, st, a);
-    }
-    return check_launch("xlbb_elast_sweep");
-}
-
-template <typename T, typename S = T>
-static int elast_sweep_t(const XlbbGrid* g, const XlbbElastMaterial* mat, const XlbbElastSweep* s, cudaStream_t st) {
-    // the previous populations are kept when mixed or differenced
-    const bool mix = !(s->a == 0.0 && s->b == 1.0) || (s->sumsq != nullptr && s->sumsq_diff);
-    if (s->resid)
-        return mix ? launch_elast<T, true, true, S>(g, mat, s, st) : launch_elast<T, true, false, S>(g, mat, s, st);
-    return mix ? launch_elast<T, false, true, S>(g, mat, s, st) : launch_elast<T, false, false, S>(g, mat, s, st);
-}
 
 template <typename T>
 static int darcy_sweep_t(const XlbbGrid* g, const XlbbDarcySweep* s, cudaStream_t st) {
@@ -1468,6 +1427,116 @@ batched_push4_kernel(const BatchInst<T, float>* __restrict__ inst, const XlbbBat
     }
 }
 
+// The four-column sweep on one grid (pipeline 4): the batched form's row
+// code on a tile per CTA (128 columns x 16 rows; the CTA's record, from the
+// kernel parameters, in shared memory).  For periodic FP32 sweeps without
+// boundary rules, per-cell material, side outputs or fused sums; bit-identical
+// to the collide-and-push kernel.
+template <bool RESID>
+__global__ void __launch_bounds__(512, 1) grid_push4_kernel(const TileRec<float, float> rin, float a, float b, int mix) {
+    grid_dep_wait();
+    __shared__ TileRec<float, float> rec;
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        rec = rin;
+        rec.x0 = blockIdx.x * 128;
+        rec.ys = blockIdx.y * 16;
+        rec.ye = min(rec.ys + 16, rin.ny);
+    }
+    __syncthreads();
+    const int lane = threadIdx.x;
+    const int x0 = blockIdx.x * 128, nx = rin.nx;
+    const int x = x0 + 4 * lane;
+    const int nlan = min(32, (nx - x0) >> 2);
+    const int y = blockIdx.y * 16 + threadIdx.y;
+    if (y < rin.ny)
+        batched_push_row4<float, RESID, false>(&rec, a, b, mix, 0, y, x, lane, lane < nlan, nlan, nx <= 128, [] {});
+}
+
+// Whether an FP32 sweep can take the four-column kernel: periodic (no rules),
+// uniform material, no side output or fused sum, at most one force array,
+// 16-byte aligned rows and planes, 8 planes within 32-bit offsets, and a grid
+// of at least 64 K cells (smaller grids want one thread per cell).
+template <class Args>
+static bool grid_push4_ok(const XlbbGrid* g, const Args& a) {
+    auto a16 = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
+    return a.pc.count == 0 && a.ps.count == 0 && a.mat.mu_f == nullptr && a.div_out == nullptr &&
+           a.sumsq == nullptr && !(a.force && a.fext) && g->nx % 4 == 0 && g->pitch % 4 == 0 && g->plane % 4 == 0 &&
+           g->plane < (1LL << 28) && (long long)g->nx * g->ny >= 65536 && a16(a.f_in) && a16(a.f_out) &&
+           a16(a.force) && a16(a.fext) && a16(a.resid);
+}
+
+template <typename T, bool RESID, typename S = T>
+static typename ElastPhys<T, RESID, S>::Args elast_args(const XlbbGrid* g, const XlbbElastMaterial* mat,
+                                                        const XlbbElastSweep* s) {
+    typename ElastPhys<T, RESID, S>::Args a;
+    a.geom = geom(g);
+    a.f_in = static_cast<const S*>(s->f_in);
+    a.f_out = static_cast<S*>(s->f_out);
+    a.force = s->use_force ? static_cast<const S*>(s->force) : nullptr;
+    a.fext = static_cast<const S*>(s->fext);
+    a.resid = static_cast<const S*>(s->resid);
+    a.a = T(s->a);
+    a.b = T(s->b);
+    a.mix = (s->a == 0.0 && s->b == 1.0) ? 0 : 1;
+    a.sumsq_diff = (s->sumsq != nullptr && s->sumsq_diff) ? 1 : 0;
+    a.mat = make_mat<T, S>(mat);
+    a.pc = rules_view<T, 8>(s->pc);
+    a.ps = rules_view<T, 8>(s->ps);
+    a.sumsq = s->sumsq;
+    a.bx0 = s->bx0; a.bx1 = s->bx1; a.by0 = s->by0; a.by1 = s->by1;
+    a.div_out = static_cast<S*>(s->div_out);
+    a.div_scale = T(-1.5 / (3.0 * (mat->lam + mat->mu) + 1.0));
+    return a;
+}
+
+template <typename T, bool RESID, bool PREV, typename S = T>
+static int launch_elast(const XlbbGrid* g, const XlbbElastMaterial* mat, const XlbbElastSweep* s, cudaStream_t st) {
+    using Ph = ElastPhys<T, RESID, S>;
+    typename Ph::Args a = elast_args<T, RESID, S>(g, mat, s);
+    if constexpr (sizeof(T) != sizeof(S)) {
+        const XlbbSweepConfig c = effective_cfg(0, XLBB_F32_ACC64);
+        if (c.pipeline == 3 && Ph::push_ok(a) && (a.ps.count == 0 || a.ps.push != nullptr)) {
+            Ph::fill_ptrs(a);
+            launch_push<Ph>(c, g, st, a);
+        } else {
+            launch_sweep_regs<Ph, PREV>(c, g, st, a);
+        }
+    } else {
+        const XlbbSweepConfig c = effective_cfg(0, sizeof(T) == 4 ? XLBB_F32 : XLBB_F64);
+        if constexpr (sizeof(T) == 4) {
+            if (g_cfg[0].pipeline == 4 && grid_push4_ok(g, a)) {
+                TileRec<float, float> r{};
+                r.fi = a.f_in;
+                r.fo = a.f_out;
+                r.fc = a.force ? a.force : a.fext;
+                r.rs = RESID ? a.resid : nullptr;
+                r.P = (unsigned)g->plane;
+                r.pitch = g->pitch;
+                r.nx = g->nx;
+                r.ny = g->ny;
+                r.cs = a.mat.cs;
+                r.cd = a.mat.cd;
+                r.h = a.mat.h;
+                r.n = a.mat.n;
+                const dim3 grid((g->nx + 127) / 128, (g->ny + 15) / 16), blk(32, 16);
+                launch_k(grid_push4_kernel<RESID>, grid, blk, 0, st, r, a.a, a.b, a.mix);
+                return check_launch("xlbb_elast_sweep");
+            }
+        }
+        launch_sweep<Ph, PREV>(c, g, st, a);
+    }
+    return check_launch("xlbb_elast_sweep");
+}
+
+template <typename T, typename S = T>
+static int elast_sweep_t(const XlbbGrid* g, const XlbbElastMaterial* mat, const XlbbElastSweep* s, cudaStream_t st) {
+    // the previous populations are kept when mixed or differenced
+    const bool mix = !(s->a == 0.0 && s->b == 1.0) || (s->sumsq != nullptr && s->sumsq_diff);
+    if (s->resid)
+        return mix ? launch_elast<T, true, true, S>(g, mat, s, st) : launch_elast<T, true, false, S>(g, mat, s, st);
+    return mix ? launch_elast<T, false, true, S>(g, mat, s, st) : launch_elast<T, false, false, S>(g, mat, s, st);
+}
+
 // Restriction (2x2 block sums) and prolongation (injection, added) of every
 // instance of a periodic batch; blockIdx.y = instance.
 template <typename Tf, typename Tc>
@@ -1634,6 +1703,21 @@ int xlbb_elast_sweep(int dtype, const XlbbGrid* g, const XlbbElastMaterial* mat,
     if (dtype == XLBB_F64) return elast_sweep_t<double>(g, mat, s, XLBB_STREAM(stream));
     if (dtype == XLBB_F32_ACC64) return elast_sweep_t<double, float>(g, mat, s, XLBB_STREAM(stream));
     return fail(XLBB_EUNSUPPORTED, "xlbb_elast_sweep: dtype");
+}
+
+int xlbb_elast_sweep_pipeline(int dtype, const XlbbGrid* g, const XlbbElastMaterial* mat, const XlbbElastSweep* s) {
+    if (!grid_ok(g) || !mat || !s) return fail(XLBB_EBADARG, "xlbb_elast_sweep_pipeline: bad argument");
+    if (dtype == XLBB_F32 && g_cfg[0].pipeline == 4) {
+        const bool ok = s->resid ? grid_push4_ok(g, elast_args<float, true>(g, mat, s))
+                                 : grid_push4_ok(g, elast_args<float, false>(g, mat, s));
+        if (ok) return 4;
+    }
+    const XlbbSweepConfig c = effective_cfg(0, dtype);
+    if (c.pipeline == 3) {
+        const bool push = s->div_out == nullptr && (s->ps.count <= 0 || s->ps.row_ptr == nullptr || s->ps.push != nullptr);
+        return push ? 3 : 0;
+    }
+    return dtype == XLBB_F32_ACC64 && (c.pipeline == 1 || c.pipeline == 2) ? 0 : c.pipeline;
 }
 
 int xlbb_darcy_sweep(int dtype, const XlbbGrid* g, const XlbbDarcySweep* s, void* stream) {
@@ -1916,7 +2000,7 @@ static int batched_sweep_t(const void* inst, const XlbbBatchTile* tiles, int nti
     const int mix = (a == 0.0 && b == 1.0) ? 0 : 1;
     const bool prev = mix || (tile_sumsq && sumsq_diff);
     const BatchInst<T, S>* I = static_cast<const BatchInst<T, S>*>(inst);
-    if (g_cfg[0].pipeline == 3) {     // collide and push
+    if (g_cfg[0].pipeline >= 3) {     // collide and push
         const dim3 blk(128, 8);
         // the CTAs loop over the tile list: launch at most one wave of resident CTAs
 #define XLBB_BP(R, Q_)                                                                                        \

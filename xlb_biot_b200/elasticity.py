@@ -562,9 +562,10 @@ class LBMElasticity:
 
     # ------------------------------------------------------------------ kernels
     def _sweep(self, f, level, a=0.0, b=1.0, resid=None, fext=None, out=None, sumsq=False, div_out=None,
-               sumsq_diff=False, acc64=False):
+               sumsq_diff=False, acc64=False, query=False):
         """One fused sweep on ``level``; ``acc64``: FP64 arithmetic on the FP32
-        level-0 fields (``residual_precision="f64"``)."""
+        level-0 fields (``residual_precision="f64"``).  ``query``: launch
+        nothing, return the pipeline the library would run (diagnostic)."""
         L = self._L(level)
         out = L.empty(8) if out is None else out
         if fext is not None and not L.conforms(fext, 2):
@@ -583,6 +584,9 @@ class LBMElasticity:
                             pc.struct(), ps.struct(), self._partials.data_ptr() if sumsq else None,
                             bx0, bx1, by0, by1, div_out.data_ptr() if div_out is not None else None,
                             1 if sumsq_diff else 0)
+        if query:
+            return _lib.check(_lib.lib().xlbb_elast_sweep_pipeline(code, L.grid(), self._mats[level], s),
+                              "xlbb_elast_sweep_pipeline")
         _lib.check(_lib.lib().xlbb_elast_sweep(code, L.grid(), self._mats[level], s, _lib.stream_ptr()),
                    "xlbb_elast_sweep")
         return out
