@@ -254,6 +254,9 @@ int xlbb_prolong_add(int dtype_fine, int dtype_coarse, const XlbbGrid* fine, con
  * the one of xlbb_elast_sweep (out = a f + b STEP(f - resid)); tile_sumsq (one
  * double per tile, or NULL) receives sum(out^2) / sum((out - f_in)^2), reduced
  * per instance by xlbb_segment_sum over tile ranges begin[i]..begin[i+1].
+ * zero_in != 0 takes every f_in as zero without reading it (the first sweep of
+ * a coarse level, whose correction starts from zero): the results of a
+ * zero-filled input, bit for bit, without the fill and the reads.
  */
 typedef struct {
     const void* f_in;
@@ -280,7 +283,7 @@ int xlbb_batch_desc_bytes(int dtype);
 int xlbb_batch_upload(int dtype, const XlbbBatchInstance* host, int ninst, void* dev, void* stream);
 int xlbb_batched_elast_sweep(int dtype, const void* inst_dev, const XlbbBatchTile* tiles_dev, int ntiles,
                              int ctas, double a, double b, int use_force, int has_resid, int sumsq_diff,
-                             double* tile_sumsq, void* stream);
+                             double* tile_sumsq, int zero_in, void* stream);
 /*
  * The same sweep by the four-column kernel (dtype XLBB_F32 only): a warp
  * takes a tile row, a lane four adjacent columns, with
@@ -292,7 +295,7 @@ int xlbb_batched_elast_sweep(int dtype, const void* inst_dev, const XlbbBatchTil
  */
 int xlbb_batched_elast_sweep4(int dtype, const void* inst_dev, const XlbbBatchTile* tiles_dev, int ntiles,
                               int ctas, double a, double b, int use_force, int has_resid, int sumsq_diff,
-                              double* tile_sumsq, void* stream);
+                              double* tile_sumsq, int zero_in, void* stream);
 int xlbb_batched_restrict(int dtype_fine, int dtype_coarse, const XlbbBatchTransfer* tr_dev, int ninst,
                           void* stream);
 int xlbb_batched_prolong_add(int dtype_fine, int dtype_coarse, const XlbbBatchTransfer* tr_dev, int ninst,

@@ -181,7 +181,7 @@ def test_four_column_kernel_skips_instances_that_do_not_qualify():
     lib = _lib.lib()
     _lib.check(lib.xlbb_batched_elast_sweep4(ln.dcode, ctypes.c_void_p(ln.desc.data_ptr()),
                                              ctypes.c_void_p(ln.tiles.data_ptr()), ln.ntiles, ln.ctas, 0.25, 0.75,
-                                             1, 0, 0, None, _lib.stream_ptr()), "xlbb_batched_elast_sweep4")
+                                             1, 0, 0, None, 0, _lib.stream_ptr()), "xlbb_batched_elast_sweep4")
     torch.cuda.synchronize()
     assert autotune.device_status(reset=True) == -1        # XLBB_EBADARG
     assert bool((dst == 7.0).all())

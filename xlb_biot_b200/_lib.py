@@ -110,8 +110,8 @@ SIGNATURES = {
     "xlbb_device_status": (I, [ctypes.POINTER(ctypes.c_int), I]),
     "xlbb_batch_desc_bytes": (I, [I]),
     "xlbb_batch_upload": (I, [I, ctypes.POINTER(BatchInstance), I, P, P]),
-    "xlbb_batched_elast_sweep": (I, [I, P, P, I, I, D, D, I, I, I, P, P]),
-    "xlbb_batched_elast_sweep4": (I, [I, P, P, I, I, D, D, I, I, I, P, P]),
+    "xlbb_batched_elast_sweep": (I, [I, P, P, I, I, D, D, I, I, I, P, I, P]),
+    "xlbb_batched_elast_sweep4": (I, [I, P, P, I, I, D, D, I, I, I, P, I, P]),
     "xlbb_batched_restrict": (I, [I, I, P, I, P]),
     "xlbb_batched_prolong_add": (I, [I, I, P, I, P]),
     "xlbb_batched_prolong_add_norms": (I, [I, I, P, I, P, P, P]),

@@ -231,22 +231,26 @@ class BatchedElasticity:
         self.graph = None
 
     # ------------------------------------------------------------------ kernels
-    def _sweep(self, l, ln, a, b, sumsq=False):
+    def _sweep(self, l, ln, a, b, sumsq=False, zero_in=False):
         fn = "xlbb_batched_elast_sweep4" if ln.vec else "xlbb_batched_elast_sweep"
         _lib.check(getattr(_lib.lib(), fn)(
             ln.dcode, ctypes.c_void_p(ln.desc.data_ptr()), ctypes.c_void_p(ln.tiles.data_ptr()), ln.ntiles, ln.ctas,
             float(a), float(b), 1 if l == 0 else 0, 1 if l > 0 else 0, 0,
-            ctypes.c_void_p(self.tile_sumsq.data_ptr()) if sumsq else None, _lib.stream_ptr()), fn)
+            ctypes.c_void_p(self.tile_sumsq.data_ptr()) if sumsq else None, 1 if zero_in else 0,
+            _lib.stream_ptr()), fn)
         self.launches_per_cycle += 1
 
-    def _smooth(self, l):
+    def _smooth(self, l, from_zero=False):
+        """k_smooth damped sweeps X->Y->X...; ``from_zero``: X holds zeros (a
+        coarse level's correction starts from zero), so the first sweep takes
+        its input as zero instead of reading a zero-filled X."""
         g = self.gamma
         for k in range(self.k_smooth):
             for ln in (self.smooth_xy[l] if k % 2 == 0 else self.smooth_yx[l]):
-                self._sweep(l, ln, 1.0 - g, g)
+                self._sweep(l, ln, 1.0 - g, g, zero_in=from_zero and k == 0)
 
     def _level(self, l):
-        self._smooth(l)
+        self._smooth(l, from_zero=l > 0)
         if l < self.levels - 1:
             self._sweep(l, self.res[l], 1.0, -1.0, sumsq=(l == 0))
             if l == 0:
@@ -258,9 +262,7 @@ class BatchedElasticity:
                 _lib.check(_lib.lib().xlbb_batched_restrict(cf, cc, ctypes.c_void_p(buf.data_ptr()), cnt,
                                                             _lib.stream_ptr()), "xlbb_batched_restrict")
                 self.launches_per_cycle += 1
-            for arena in self.X[l + 1].values():
-                arena.buf.zero_()
-            self._level(l + 1)
+            self._level(l + 1)          # its correction starts from zero (first sweep: zero input)
             for k, (buf, cnt, cf, cc, _) in enumerate(self.t_prolong[l]):
                 if l == 0:   # instances of transfer list k occupy rows offset.. of corr2
                     off = sum(t[1] for t in self.t_prolong[0][:k])

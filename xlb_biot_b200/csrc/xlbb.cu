@@ -1071,13 +1071,15 @@ __device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefe
 // starting at column x): no registers stay held, the next row's loads are then
 // served from L2.
 template <typename T, typename S, bool RESID>
-__device__ __forceinline__ void prefetch_tile_row(const TileRec<T, S>* rn, int w, int x) {
+__device__ __forceinline__ void prefetch_tile_row(const TileRec<T, S>* rn, int w, int x, int zero_in) {
     const int yn = (int)lds32(&rn->ys) + w, xn = (int)lds32(&rn->x0) + x;
     if (yn >= (int)lds32(&rn->ye) || xn >= (int)lds32(&rn->nx)) return;
     const unsigned Pn = lds32(&rn->P), on = unsigned(yn * (int)lds32(&rn->pitch) + xn);
     const S* fin = ldsP(&rn->fi);
+    if (!zero_in) {
 #pragma unroll
-    for (unsigned i = 0; i < 8; ++i) prefetch_l2(fin + (on + i * Pn));
+        for (unsigned i = 0; i < 8; ++i) prefetch_l2(fin + (on + i * Pn));
+    }
     const S* fcn = ldsP(&rn->fc);
     if (fcn) { prefetch_l2(fcn + on); prefetch_l2(fcn + (on + Pn)); }
     if constexpr (RESID) {
@@ -1098,13 +1100,17 @@ struct BatchedCell {
     bool hasF;
 };
 
+// zero_in: the populations are taken as zero (not read) -- the first sweep of a
+// coarse level, whose correction starts from zero; the same values as a
+// zero-filled input, bit for bit.
 template <typename T, bool RESID, typename S>
-__device__ __forceinline__ void batched_cell_load(const TileRec<T, S>* r, int y, int x, BatchedCell<T>& c) {
+__device__ __forceinline__ void batched_cell_load(const TileRec<T, S>* r, int y, int x, BatchedCell<T>& c,
+                                                  int zero_in) {
     const S* fi = ldsP(&r->fi);
     const unsigned P = lds32(&r->P);
     const unsigned o = unsigned(y * (int)lds32(&r->pitch) + x);
 #pragma unroll
-    for (unsigned i = 0; i < 8; ++i) c.g[i] = T(__ldg(fi + (o + i * P)));
+    for (unsigned i = 0; i < 8; ++i) c.g[i] = zero_in ? T(0) : T(__ldg(fi + (o + i * P)));
     if constexpr (RESID) {
         const S* rs = ldsP(&r->rs);
 #pragma unroll
@@ -1119,7 +1125,7 @@ __device__ __forceinline__ void batched_cell_load(const TileRec<T, S>* r, int y,
 
 template <typename T, bool SUMSQ, typename S>
 __device__ __forceinline__ double batched_cell_push(const TileRec<T, S>* r, const BatchedCell<T>& c, T a, T b, int mix,
-                                                    int sumsq_diff, int y, int x) {
+                                                    int sumsq_diff, int y, int x, int zero_in) {
     T fs[8];
     elast_collide<T>(c.g, c.hasF, c.F0, c.F1, ldsT(&r->cs), ldsT(&r->cd), ldsT(&r->h), ldsT(&r->n), fs);
     const int pitch = (int)lds32(&r->pitch), nx = (int)lds32(&r->nx), ny = (int)lds32(&r->ny);
@@ -1135,7 +1141,7 @@ __device__ __forceinline__ double batched_cell_push(const TileRec<T, S>* r, cons
         const unsigned oz = unsigned((cy8(i) > 0 ? rp : (cy8(i) < 0 ? rm : r0)) + zx) + i * P;
         T v = fs[i];
         T fz = T(0);
-        if (mix || (SUMSQ && sumsq_diff)) fz = T(__ldg(fi + oz));
+        if ((mix || (SUMSQ && sumsq_diff)) && !zero_in) fz = T(__ldg(fi + oz));
         if (mix) v = mix_ab(a, fz, b, fs[i]);
         const S sv = S(v);
         fo[oz] = sv;
@@ -1164,7 +1170,7 @@ __device__ __forceinline__ double batched_cell_push(const TileRec<T, S>* r, cons
 template <typename T, bool RESID, bool SUMSQ, typename S = T>
 __global__ void __launch_bounds__(1024, 1)
 batched_push_kernel(const BatchInst<T, S>* __restrict__ inst, const XlbbBatchTile* __restrict__ tiles, int ntiles,
-                    T a, T b, int mix, int use_force, int sumsq_diff, double* tile_sumsq) {
+                    T a, T b, int mix, int use_force, int sumsq_diff, double* tile_sumsq, int zero_in) {
     grid_dep_wait();
     __shared__ double red[32];
     __shared__ TileRec<T, S> rec[2][32];
@@ -1194,14 +1200,14 @@ batched_push_kernel(const BatchInst<T, S>* __restrict__ inst, const XlbbBatchTil
         // warp-uniform loop (a warp spans one threadIdx.y); inactive lanes only join the next-tile work
         for (int y = (int)lds32(&r->ys) + threadIdx.y; y < (int)lds32(&r->ye); y += blockDim.y) {
             BatchedCell<T> c;
-            if (active) batched_cell_load<T, RESID, S>(r, y, x, c);
+            if (active) batched_cell_load<T, RESID, S>(r, y, x, c, zero_in);
             if (pending) {
                 pending = false;
                 if (tn < ntiles && (tid & 31) == 0) fill_tile_rec(rn, inst, tiles, tn, use_force, RESID, false);
                 __syncwarp();
-                if (tn < ntiles) prefetch_tile_row<T, S, RESID>(rn, threadIdx.y, threadIdx.x);
+                if (tn < ntiles) prefetch_tile_row<T, S, RESID>(rn, threadIdx.y, threadIdx.x, zero_in);
             }
-            if (active) acc += batched_cell_push<T, SUMSQ, S>(r, c, a, b, mix, sumsq_diff, y, x);
+            if (active) acc += batched_cell_push<T, SUMSQ, S>(r, c, a, b, mix, sumsq_diff, y, x, zero_in);
         }
         if (pending) {                          // a warp without a row in this tile
             if (tn < ntiles && (tid & 31) == 0) fill_tile_rec(rn, inst, tiles, tn, use_force, RESID, false);
@@ -1236,7 +1242,7 @@ __device__ __forceinline__ T mixv(int mix, T a, T fz, T b, T s) { return mix ? m
 template <typename T, bool RESID, bool SUMSQ, class Mid>
 __device__ __forceinline__ double batched_push_row4(const TileRec<T, float>* r, T a, T b, int mix, int sumsq_diff,
                                                     int y, int x, int lane, bool active, int nlan, bool single,
-                                                    Mid&& mid) {
+                                                    int zero_in, Mid&& mid) {
     const unsigned P = lds32(&r->P);
     const int pitch = (int)lds32(&r->pitch);
     const unsigned o = unsigned(y * pitch + x);
@@ -1252,11 +1258,12 @@ __device__ __forceinline__ double batched_push_row4(const TileRec<T, float>* r, 
         const float* fi = ldsP(&r->fi);
         float4 v[8];
 #pragma unroll
-        for (unsigned i = 0; i < 8; ++i) v[i] = active ? ldg4(fi + (o + i * P)) : make_float4(0.f, 0.f, 0.f, 0.f);
+        for (unsigned i = 0; i < 8; ++i)
+            v[i] = active && !zero_in ? ldg4(fi + (o + i * P)) : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
             fzv[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (cy8(i) != 0 && need_fz && active)
+            if (cy8(i) != 0 && need_fz && active && !zero_in)
                 fzv[i] = ldg4(fi + (unsigned((cy8(i) > 0 ? yu : yl) * pitch + x) + unsigned(i) * P));
         }
         f0[0] = T(v[0].x); f0[1] = T(v[0].y); f0[2] = T(v[0].z); f0[3] = T(v[0].w);
@@ -1350,7 +1357,7 @@ __device__ __forceinline__ double batched_push_row4(const TileRec<T, float>* r, 
             const unsigned oz = unsigned(yd * pitch + xd) + unsigned(i) * P;
             const T sv = cxi > 0 ? ps[i][3] : ps[i][0];
             T fzs = T(0);
-            if (need_fz) fzs = T(__ldg(fi + oz));
+            if (need_fz && !zero_in) fzs = T(__ldg(fi + oz));
             const float w = float(mixv<T>(mix, a, fzs, b, sv));
             fo[oz] = w;
             if constexpr (SUMSQ) {
@@ -1374,7 +1381,7 @@ __device__ __forceinline__ double batched_push_row4(const TileRec<T, float>* r, 
 template <typename T, bool RESID, bool SUMSQ>
 __global__ void __launch_bounds__(512, 1)
 batched_push4_kernel(const BatchInst<T, float>* __restrict__ inst, const XlbbBatchTile* __restrict__ tiles, int ntiles,
-                     T a, T b, int mix, int use_force, int sumsq_diff, double* tile_sumsq) {
+                     T a, T b, int mix, int use_force, int sumsq_diff, double* tile_sumsq, int zero_in) {
     grid_dep_wait();
     __shared__ double red[16];
     __shared__ TileRec<T, float> rec[2][16];
@@ -1398,8 +1405,10 @@ batched_push4_kernel(const BatchInst<T, float>* __restrict__ inst, const XlbbBat
                 if (yn < (int)lds32(&rn->ye) && xn < (int)lds32(&rn->nx)) {
                     const unsigned Pn = lds32(&rn->P), on = unsigned(yn * (int)lds32(&rn->pitch) + xn);
                     const float* fin = ldsP(&rn->fi);
+                    if (!zero_in) {
 #pragma unroll
-                    for (unsigned i = 0; i < 8; ++i) prefetch_l2(fin + (on + i * Pn));
+                        for (unsigned i = 0; i < 8; ++i) prefetch_l2(fin + (on + i * Pn));
+                    }
                     const float* fcn = ldsP(&rn->fc);
                     if (fcn) { prefetch_l2(fcn + on); prefetch_l2(fcn + (on + Pn)); }
                     if constexpr (RESID) {
@@ -1417,7 +1426,7 @@ batched_push4_kernel(const BatchInst<T, float>* __restrict__ inst, const XlbbBat
         double acc = 0.0;
         for (int y = (int)lds32(&r->ys) + w; y < (int)lds32(&r->ye); y += blockDim.y)
             acc += batched_push_row4<T, RESID, SUMSQ>(r, a, b, mix, sumsq_diff, y, x, lane, lane < nlan, nlan, single,
-                                                      next);
+                                                      zero_in, next);
         next();                                  // a warp without a row in this tile
         if constexpr (SUMSQ) {
             const double s = block_sum_2d(acc, red);
@@ -1449,7 +1458,7 @@ __global__ void __launch_bounds__(512, 1) grid_push4_kernel(const TileRec<float,
     const int nlan = min(32, (nx - x0) >> 2);
     const int y = blockIdx.y * 16 + threadIdx.y;
     if (y < rin.ny)
-        batched_push_row4<float, RESID, false>(&rec, a, b, mix, 0, y, x, lane, lane < nlan, nlan, nx <= 128, [] {});
+        batched_push_row4<float, RESID, false>(&rec, a, b, mix, 0, y, x, lane, lane < nlan, nlan, nx <= 128, 0, [] {});
 }
 
 // Whether an FP32 sweep can take the four-column kernel: periodic (no rules),
@@ -1994,9 +2003,27 @@ int xlbb_batch_desc_bytes(int dtype) {
 
 }  // extern "C"
 
+// Zero the input populations (8 planes) of every tile's cells: the
+// row-marching form's stand-in for zero_in (it reads its input rows).
+template <typename T, typename S>
+__global__ void batched_zero_in_kernel(const BatchInst<T, S>* __restrict__ inst, const XlbbBatchTile* __restrict__ tiles,
+                                       int ntiles) {
+    grid_dep_wait();
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const XlbbBatchTile tl = tiles[t];
+        const BatchInst<T, S>& I = inst[tl.inst];
+        S* f = const_cast<S*>(I.f_in);
+        const int x = tl.x0 + threadIdx.x;
+        if (x >= I.geom.nx) continue;
+        for (int y = tl.ys; y < tl.ye; ++y)
+            for (int i = 0; i < 8; ++i) f[(size_t)y * I.geom.pitch + x + (size_t)i * I.geom.plane] = S(0);
+    }
+}
+
 template <typename T, typename S = T>
 static int batched_sweep_t(const void* inst, const XlbbBatchTile* tiles, int ntiles, int ctas, double a, double b,
-                           int use_force, int has_resid, int sumsq_diff, double* tile_sumsq, cudaStream_t st) {
+                           int use_force, int has_resid, int sumsq_diff, double* tile_sumsq, int zero_in,
+                           cudaStream_t st) {
     const int mix = (a == 0.0 && b == 1.0) ? 0 : 1;
     const bool prev = mix || (tile_sumsq && sumsq_diff);
     const BatchInst<T, S>* I = static_cast<const BatchInst<T, S>*>(inst);
@@ -2013,13 +2040,14 @@ static int batched_sweep_t(const void* inst, const XlbbBatchTile* tiles, int nti
             resident = (per_sm > 0 ? per_sm : 1) * num_sms();                                                 \
         }                                                                                                     \
         launch_k(batched_push_kernel<T, R, Q_, S>, ctas < resident ? ctas : resident, blk, 0, st,                   \
-            I, tiles, ntiles, T(a), T(b), mix, use_force, sumsq_diff, tile_sumsq);                            \
+            I, tiles, ntiles, T(a), T(b), mix, use_force, sumsq_diff, tile_sumsq, zero_in);                   \
     } while (0)
         if (has_resid) { if (tile_sumsq) XLBB_BP(true, true); else XLBB_BP(true, false); }
         else { if (tile_sumsq) XLBB_BP(false, true); else XLBB_BP(false, false); }
 #undef XLBB_BP
         return check_launch("xlbb_batched_elast_sweep");
     }
+    if (zero_in) launch_k(batched_zero_in_kernel<T, S>, ctas, 128, 0, st, I, tiles, ntiles);
 #define XLBB_B(R, P) \
     launch_k(batched_elast_kernel<T, 128, R, P, S>, ctas, 160, 0, st, I, tiles, ntiles, T(a), T(b), mix, use_force, \
                                                                  sumsq_diff, tile_sumsq)
@@ -2033,7 +2061,8 @@ static int batched_sweep_t(const void* inst, const XlbbBatchTile* tiles, int nti
 // at most one wave of resident CTAs.
 template <typename T>
 static int batched_sweep4_t(const void* inst, const XlbbBatchTile* tiles, int ntiles, int ctas, double a, double b,
-                            int use_force, int has_resid, int sumsq_diff, double* tile_sumsq, cudaStream_t st) {
+                            int use_force, int has_resid, int sumsq_diff, double* tile_sumsq, int zero_in,
+                            cudaStream_t st) {
     const int mix = (a == 0.0 && b == 1.0) ? 0 : 1;
     const BatchInst<T, float>* I = static_cast<const BatchInst<T, float>*>(inst);
     const dim3 blk(32, 16);
@@ -2047,7 +2076,7 @@ static int batched_sweep4_t(const void* inst, const XlbbBatchTile* tiles, int nt
             resident = (per_sm > 0 ? per_sm : 1) * num_sms();                                                 \
         }                                                                                                     \
         launch_k(batched_push4_kernel<T, R, Q_>, ctas < resident ? ctas : resident, blk, 0, st,                     \
-            I, tiles, ntiles, T(a), T(b), mix, use_force, sumsq_diff, tile_sumsq);                            \
+            I, tiles, ntiles, T(a), T(b), mix, use_force, sumsq_diff, tile_sumsq, zero_in);                   \
     } while (0)
     if (has_resid) { if (tile_sumsq) XLBB_BP4(true, true); else XLBB_BP4(true, false); }
     else { if (tile_sumsq) XLBB_BP4(false, true); else XLBB_BP4(false, false); }
@@ -2059,28 +2088,28 @@ extern "C" {
 
 int xlbb_batched_elast_sweep(int dtype, const void* inst_dev, const XlbbBatchTile* tiles_dev, int ntiles, int ctas,
                              double a, double b, int use_force, int has_resid, int sumsq_diff, double* tile_sumsq,
-                             void* stream) {
+                             int zero_in, void* stream) {
     if (!inst_dev || !tiles_dev || ntiles <= 0 || ctas <= 0) return fail(XLBB_EBADARG, "xlbb_batched_elast_sweep: bad argument");
     if (dtype == XLBB_F32)
         return batched_sweep_t<float>(inst_dev, tiles_dev, ntiles, ctas, a, b, use_force, has_resid, sumsq_diff,
-                                      tile_sumsq, XLBB_STREAM(stream));
+                                      tile_sumsq, zero_in, XLBB_STREAM(stream));
     if (dtype == XLBB_F64)
         return batched_sweep_t<double>(inst_dev, tiles_dev, ntiles, ctas, a, b, use_force, has_resid, sumsq_diff,
-                                       tile_sumsq, XLBB_STREAM(stream));
+                                       tile_sumsq, zero_in, XLBB_STREAM(stream));
     if (dtype == XLBB_F32_ACC64)
         return batched_sweep_t<double, float>(inst_dev, tiles_dev, ntiles, ctas, a, b, use_force, has_resid,
-                                              sumsq_diff, tile_sumsq, XLBB_STREAM(stream));
+                                              sumsq_diff, tile_sumsq, zero_in, XLBB_STREAM(stream));
     return fail(XLBB_EUNSUPPORTED, "xlbb_batched_elast_sweep: dtype");
 }
 
 int xlbb_batched_elast_sweep4(int dtype, const void* inst_dev, const XlbbBatchTile* tiles_dev, int ntiles, int ctas,
                               double a, double b, int use_force, int has_resid, int sumsq_diff, double* tile_sumsq,
-                              void* stream) {
+                              int zero_in, void* stream) {
     if (!inst_dev || !tiles_dev || ntiles <= 0 || ctas <= 0)
         return fail(XLBB_EBADARG, "xlbb_batched_elast_sweep4: bad argument");
     if (dtype == XLBB_F32)
         return batched_sweep4_t<float>(inst_dev, tiles_dev, ntiles, ctas, a, b, use_force, has_resid, sumsq_diff,
-                                       tile_sumsq, XLBB_STREAM(stream));
+                                       tile_sumsq, zero_in, XLBB_STREAM(stream));
     return fail(XLBB_EUNSUPPORTED, "xlbb_batched_elast_sweep4: dtype (XLBB_F32 only)");
 }
 
