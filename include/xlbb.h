@@ -251,9 +251,11 @@ int xlbb_prolong_add(int dtype_fine, int dtype_coarse, const XlbbGrid* fine, con
  * owns it).  A sweep runs every tile of `tiles_dev`: tile = (instance, x0,
  * row range), CTAs of 128 owned columns looping over the list (`ctas` is an
  * upper bound: at most one wave of resident CTAs is launched); the algebra is
- * the one of xlbb_elast_sweep (out = a f + b STEP(f - resid)); tile_sumsq (one
- * double per tile, or NULL) receives sum(out^2) / sum((out - f_in)^2), reduced
- * per instance by xlbb_segment_sum over tile ranges begin[i]..begin[i+1].
+ * the one of xlbb_elast_sweep (out = a f + b STEP(f - resid)); tile_sumsq
+ * (XLBB_BATCH_PARTS_PER_TILE doubles per tile -- a partial per warp, no block
+ * barrier --, or NULL) receives sum(out^2) / sum((out - f_in)^2), reduced per
+ * instance by xlbb_segment_sum over the ranges begin[i]..begin[i+1] of
+ * partials (tile ranges times XLBB_BATCH_PARTS_PER_TILE).
  * zero_in != 0 takes every f_in as zero without reading it (the first sweep of
  * a coarse level, whose correction starts from zero): the results of a
  * zero-filled input, bit for bit, without the fill and the reads.
@@ -271,6 +273,8 @@ typedef struct {
 typedef struct {
     int inst, x0, ys, ye;
 } XlbbBatchTile;
+
+#define XLBB_BATCH_PARTS_PER_TILE 32
 
 typedef struct {
     const void* fine;        /* fine residual (restrict) / fine populations (prolong) */

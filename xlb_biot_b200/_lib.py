@@ -13,6 +13,7 @@ LIB_PATH = os.path.join(_HERE, "libxlbb.so")
 
 XLBB_F32, XLBB_F64, XLBB_F32_ACC64 = 0, 1, 2
 XLBB_PROLONG_BLOCKS = 32
+XLBB_BATCH_PARTS_PER_TILE = 32       # FP64 partials per tile of a batched sweep with sums
 ERRORS = {-1: "XLBB_EBADARG", -2: "XLBB_ELAUNCH", -3: "XLBB_ETIMEOUT", -4: "XLBB_ENONFINITE",
           -5: "XLBB_EUNSUPPORTED"}
 

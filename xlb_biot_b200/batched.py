@@ -197,8 +197,10 @@ class BatchedElasticity:
                                        code=_lib.XLBB_F32_ACC64 if acc64 else None))
         if self.deeper[0] != list(range(self.n)):
             raise AssertionError("every instance recurses below level 0")
-        self.tile_begin = self.res[0].begin
-        self.tile_sumsq = torch.zeros(self.res[0].ntiles, dtype=torch.float64, device=dev)
+        # per-instance ranges of the level-0 residual sweep's partials (a partial per warp of each tile)
+        self.tile_begin = self.res[0].begin * _lib.XLBB_BATCH_PARTS_PER_TILE
+        self.tile_sumsq = torch.zeros(self.res[0].ntiles * _lib.XLBB_BATCH_PARTS_PER_TILE, dtype=torch.float64,
+                                      device=dev)
         self.norm2 = torch.zeros(self.n, dtype=torch.float64, device=dev)
         # level-0 coarse correction: per instance [sum corr^2, sum f^2] (FP64)
         self.corr2 = torch.zeros((self.n, 2), dtype=torch.float64, device=dev)

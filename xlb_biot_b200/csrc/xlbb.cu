@@ -997,7 +997,8 @@ batched_elast_kernel(const BatchInst<T, S>* __restrict__ inst, const XlbbBatchTi
         const double acc = sweep_strip<Ph, TX, 1, PREV>(p, tl.x0, tl.ys, tl.ye, post);
         if (tile_sumsq != nullptr) {
             const double s = block_sum(acc, red);
-            if (threadIdx.x == 0) tile_sumsq[t] = s;
+            if (threadIdx.x < XLBB_BATCH_PARTS_PER_TILE)
+                tile_sumsq[(size_t)t * XLBB_BATCH_PARTS_PER_TILE + threadIdx.x] = threadIdx.x == 0 ? s : 0.0;
         }
     }
 }
@@ -1172,7 +1173,6 @@ __global__ void __launch_bounds__(1024, 1)
 batched_push_kernel(const BatchInst<T, S>* __restrict__ inst, const XlbbBatchTile* __restrict__ tiles, int ntiles,
                     T a, T b, int mix, int use_force, int sumsq_diff, double* tile_sumsq, int zero_in) {
     grid_dep_wait();
-    __shared__ double red[32];
     __shared__ TileRec<T, S> rec[2][32];
     const int tid = threadIdx.y * blockDim.x + threadIdx.x, wid = tid >> 5;
     if (blockIdx.x >= ntiles) return;          // uniform over the block
@@ -1213,9 +1213,9 @@ batched_push_kernel(const BatchInst<T, S>* __restrict__ inst, const XlbbBatchTil
             if (tn < ntiles && (tid & 31) == 0) fill_tile_rec(rn, inst, tiles, tn, use_force, RESID, false);
             __syncwarp();
         }
-        if constexpr (SUMSQ) {   // the tile's writes: every output of the instance is written once
-            const double s = block_sum_2d(acc, red);
-            if (threadIdx.x == 0 && threadIdx.y == 0) tile_sumsq[t] = s;
+        if constexpr (SUMSQ) {   // a partial per warp (no block barrier); every output is written once
+            const double s = warp_sum(acc);
+            if ((tid & 31) == 0) tile_sumsq[(size_t)t * XLBB_BATCH_PARTS_PER_TILE + wid] = s;
         }
         __syncwarp();                           // every lane is done with r before it is refilled
     }
@@ -1383,7 +1383,6 @@ __global__ void __launch_bounds__(512, 1)
 batched_push4_kernel(const BatchInst<T, float>* __restrict__ inst, const XlbbBatchTile* __restrict__ tiles, int ntiles,
                      T a, T b, int mix, int use_force, int sumsq_diff, double* tile_sumsq, int zero_in) {
     grid_dep_wait();
-    __shared__ double red[16];
     __shared__ TileRec<T, float> rec[2][16];
     const int lane = threadIdx.x, w = threadIdx.y;   // blockDim = (32, 16): a warp per tile row
     if (blockIdx.x >= ntiles) return;                 // uniform over the block
@@ -1428,9 +1427,12 @@ batched_push4_kernel(const BatchInst<T, float>* __restrict__ inst, const XlbbBat
             acc += batched_push_row4<T, RESID, SUMSQ>(r, a, b, mix, sumsq_diff, y, x, lane, lane < nlan, nlan, single,
                                                       zero_in, next);
         next();                                  // a warp without a row in this tile
-        if constexpr (SUMSQ) {
-            const double s = block_sum_2d(acc, red);
-            if (threadIdx.x == 0 && threadIdx.y == 0) tile_sumsq[t] = s;
+        if constexpr (SUMSQ) {                   // a partial per warp (no block barrier)
+            const double s = warp_sum(acc);
+            if (lane == 0) {
+                tile_sumsq[(size_t)t * XLBB_BATCH_PARTS_PER_TILE + w] = s;
+                tile_sumsq[(size_t)t * XLBB_BATCH_PARTS_PER_TILE + 16 + w] = 0.0;
+            }
         }
         __syncwarp();                            // every lane is done with r before it is refilled
     }

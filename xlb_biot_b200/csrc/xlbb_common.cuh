@@ -74,6 +74,13 @@ __device__ __forceinline__ int wrap(int v, int n) { return v < 0 ? v + n : (v >=
 // has finished and its writes are visible (a no-op for an ordinary launch).
 __device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
+// Warp-wide FP64 sum (fixed butterfly order: deterministic), in every lane.
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
 // Block-wide FP64 sum (blockDim.x multiple of 32, <= 1024).
 __device__ __forceinline__ double block_sum(double v, double* sh) {
 #pragma unroll
