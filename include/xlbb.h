@@ -314,6 +314,20 @@ int xlbb_batched_prolong_add(int dtype_fine, int dtype_coarse, const XlbbBatchTr
 #define XLBB_PROLONG_BLOCKS 32
 int xlbb_batched_prolong_add_norms(int dtype_fine, int dtype_coarse, const XlbbBatchTransfer* tr_dev, int ninst,
                                    double* parts, double* norms, void* stream);
+/*
+ * The same prolongation with a balanced block map: block b adds the coarse
+ * correction to elements [map[2 b + 1], + 1024) (cell index y * nx_f + x) of
+ * instance map[2 b] of tr_dev -- the caller gives each instance
+ * ceil(nx_f * ny_f / 1024) consecutive blocks, so every block does the same
+ * work whatever the instance sizes.  With norms != NULL (then parts, begin_dev
+ * and ninst too), norms[2 i] / norms[2 i + 1] receive the FP64 sums of the
+ * correction^2 / of the corrected populations^2 over instance i's blocks
+ * begin_dev[i] .. begin_dev[i + 1] (deterministic); parts: caller scratch of
+ * 2 * nblocks doubles.
+ */
+int xlbb_batched_prolong_add_map(int dtype_fine, int dtype_coarse, const XlbbBatchTransfer* tr_dev,
+                                 const int* map_dev, int nblocks, double* parts, const int* begin_dev, int ninst,
+                                 double* norms, void* stream);
 int xlbb_segment_sum(const double* parts, const int* begin_dev, int nseg, double* out, void* stream);
 
 /*

@@ -116,6 +116,7 @@ SIGNATURES = {
     "xlbb_batched_restrict": (I, [I, I, P, I, P]),
     "xlbb_batched_prolong_add": (I, [I, I, P, I, P]),
     "xlbb_batched_prolong_add_norms": (I, [I, I, P, I, P, P, P]),
+    "xlbb_batched_prolong_add_map": (I, [I, I, P, P, I, P, P, I, P, P]),
     "xlbb_segment_sum": (I, [P, P, I, P, P]),
     "xlbb_elast_sweep_adjoint": (I, [I, PG, ctypes.POINTER(ElastMaterial), ctypes.POINTER(ElastSweepAdjoint), P]),
     "xlbb_darcy_sweep_adjoint": (I, [I, PG, ctypes.POINTER(DarcySweepAdjoint), P]),

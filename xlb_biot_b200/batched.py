@@ -204,7 +204,7 @@ class BatchedElasticity:
         self.norm2 = torch.zeros(self.n, dtype=torch.float64, device=dev)
         # level-0 coarse correction: per instance [sum corr^2, sum f^2] (FP64)
         self.corr2 = torch.zeros((self.n, 2), dtype=torch.float64, device=dev)
-        self._corr_parts = torch.zeros(2 * _lib.XLBB_PROLONG_BLOCKS * self.n, dtype=torch.float64, device=dev)
+        self._corr_parts = None       # sized below: 2 doubles per block of the level-0 prolongation maps
 
         def transfers(l, fine, coarse_arenas, d_coarse, src_is_res):
             ids = [g for g in self.deeper[l] if dtype_of(g, l + 1) == d_coarse]
@@ -221,14 +221,26 @@ class BatchedElasticity:
             return (torch.as_tensor(np.frombuffer(raw, dtype=np.uint8).copy(), device=dev), len(ids),
                     _lib.dtype_code(dt), _lib.dtype_code(d_coarse), ids)
 
+        def prolong_map(t, l):
+            """Balanced block map of a prolongation list: ceil(cells / 1024)
+            consecutive blocks per instance, each (instance, first cell)."""
+            blocks, begin = [], [0]
+            for k, g in enumerate(t[4]):
+                nx, ny = self.shapes[l][g]
+                blocks += [(k, e) for e in range(0, nx * ny, 1024)]
+                begin.append(len(blocks))
+            m = torch.as_tensor(np.asarray(blocks, dtype=np.int32).reshape(-1), device=dev)
+            return m, len(blocks), torch.as_tensor(np.asarray(begin, dtype=np.int32), device=dev)
+
         self.t_restrict, self.t_prolong = [], []
         for l in range(self.levels - 1):
             dcs = sorted(set(dtype_of(g, l + 1) for g in self.deeper[l]), key=str)
             self.t_restrict.append([t for t in (transfers(l, self.RES[l], self.R[l + 1], d, True) for d in dcs) if t])
-            self.t_prolong.append([t for t in (transfers(l, self.X[l][dt], self.X[l + 1], d, False) for d in dcs)
-                                   if t])
+            self.t_prolong.append([t + prolong_map(t, l) for t in
+                                   (transfers(l, self.X[l][dt], self.X[l + 1], d, False) for d in dcs) if t])
         # row r of corr2 belongs to instance _corr_ids[r] (transfer-list order)
         self._corr_ids = np.asarray([g for t in self.t_prolong[0] for g in t[4]])
+        self._corr_parts = torch.zeros(2 * max(t[6] for t in self.t_prolong[0]), dtype=torch.float64, device=dev)
         self.launches_per_cycle = 0
         self.graph = None
 
@@ -265,19 +277,18 @@ class BatchedElasticity:
                                                             _lib.stream_ptr()), "xlbb_batched_restrict")
                 self.launches_per_cycle += 1
             self._level(l + 1)          # its correction starts from zero (first sweep: zero input)
-            for k, (buf, cnt, cf, cc, _) in enumerate(self.t_prolong[l]):
+            for k, (buf, cnt, cf, cc, _, bmap, nblocks, bbegin) in enumerate(self.t_prolong[l]):
                 if l == 0:   # instances of transfer list k occupy rows offset.. of corr2
                     off = sum(t[1] for t in self.t_prolong[0][:k])
-                    _lib.check(_lib.lib().xlbb_batched_prolong_add_norms(
-                        cf, cc, ctypes.c_void_p(buf.data_ptr()), cnt,
-                        ctypes.c_void_p(self._corr_parts.data_ptr() + 16 * _lib.XLBB_PROLONG_BLOCKS * off),
-                        ctypes.c_void_p(self.corr2.data_ptr() + 16 * off), _lib.stream_ptr()),
-                        "xlbb_batched_prolong_add_norms")
+                    parts, norms = ctypes.c_void_p(self._corr_parts.data_ptr()), ctypes.c_void_p(
+                        self.corr2.data_ptr() + 16 * off)
                     self.launches_per_cycle += 2
                 else:
-                    _lib.check(_lib.lib().xlbb_batched_prolong_add(cf, cc, ctypes.c_void_p(buf.data_ptr()), cnt,
-                                                                   _lib.stream_ptr()), "xlbb_batched_prolong_add")
+                    parts = norms = None
                     self.launches_per_cycle += 1
+                _lib.check(_lib.lib().xlbb_batched_prolong_add_map(
+                    cf, cc, ctypes.c_void_p(buf.data_ptr()), ctypes.c_void_p(bmap.data_ptr()), nblocks, parts,
+                    ctypes.c_void_p(bbegin.data_ptr()), cnt, norms, _lib.stream_ptr()), "xlbb_batched_prolong_add_map")
         self._smooth(l)
 
     def vcycle(self):

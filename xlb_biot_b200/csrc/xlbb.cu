@@ -1614,6 +1614,75 @@ __global__ void batched_prolong_add_kernel(const XlbbBatchTransfer* __restrict__
 
 // norms[2 i + k] = sum over the XLBB_PROLONG_BLOCKS blocks of instance i of
 // parts[2 block + k]; one warp per instance, fixed order.
+// Prolongation with a balanced block map: block b adds the coarse correction
+// to elements [e0, e0 + 1024) of instance map[b].x (e0 = map[b].y; a thread
+// takes 4 elements 256 apart), so that every block does the same work whatever
+// the instance sizes.  With parts != NULL the block writes its FP64 sums of the
+// correction^2 and of the corrected populations^2 to parts[b], parts[nb + b].
+template <typename Tf, typename Tc>
+__global__ void __launch_bounds__(256) batched_prolong_map_kernel(const XlbbBatchTransfer* __restrict__ tr,
+                                                                  const int2* __restrict__ map, int nb,
+                                                                  double* parts) {
+    grid_dep_wait();
+    __shared__ double red[8];
+    const int2 m = map[blockIdx.x];
+    const XlbbBatchTransfer T_ = tr[m.x];
+    Tf* __restrict__ ff = static_cast<Tf*>(const_cast<void*>(T_.fine));
+    const Tc* __restrict__ fc = static_cast<const Tc*>(T_.coarse);
+    const int n = T_.nx_f * T_.ny_f;
+    double cc = 0.0, nn = 0.0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int e = m.y + k * 256 + threadIdx.x;
+        if (e < n) {
+            const int x = e % T_.nx_f, y = e / T_.nx_f;
+            const size_t of = (size_t)y * T_.pitch_f + x, oc = (size_t)(y / 2) * T_.pitch_c + x / 2;
+            Tf a[8];      // every plane's loads before the first store
+            Tc c[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                a[i] = ff[of + (size_t)i * T_.plane_f];
+                c[i] = __ldg(fc + oc + (size_t)i * T_.plane_c);
+            }
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const Tf v = Tf(a[i] + c[i]);
+                ff[of + (size_t)i * T_.plane_f] = v;
+                cc += (double)c[i] * (double)c[i];
+                nn += (double)v * (double)v;
+            }
+        }
+    }
+    if (parts != nullptr) {
+        const double sa = block_sum(cc, red);
+        const double sb = block_sum(nn, red);
+        if (threadIdx.x == 0) {
+            parts[blockIdx.x] = sa;
+            parts[nb + blockIdx.x] = sb;
+        }
+    }
+}
+
+// norms[2 i] = sum of parts[begin[i] .. begin[i+1]), norms[2 i + 1] the same
+// over parts[nb + ...] (fixed order: deterministic).
+__global__ void pair_segment_sum_kernel(const double* parts, int nb, const int* begin, int nseg, double* norms) {
+    grid_dep_wait();
+    __shared__ double red[8];
+    const int i = blockIdx.x;
+    if (i >= nseg) return;
+    double a = 0.0, b = 0.0;
+    for (int t = begin[i] + threadIdx.x; t < begin[i + 1]; t += blockDim.x) {
+        a += parts[t];
+        b += parts[nb + t];
+    }
+    const double sa = block_sum(a, red);
+    const double sb = block_sum(b, red);
+    if (threadIdx.x == 0) {
+        norms[2 * i] = sa;
+        norms[2 * i + 1] = sb;
+    }
+}
+
 __global__ void prolong_norms_kernel(const double* parts, int ninst, double* norms) {
     grid_dep_wait();
     const int i = blockIdx.x;
@@ -2149,6 +2218,26 @@ int xlbb_batched_prolong_add_norms(int dtype_fine, int dtype_coarse, const XlbbB
     if (st_ != XLBB_OK) return st_;
     launch_k(prolong_norms_kernel, ninst, 32, 0, XLBB_STREAM(stream), parts, ninst, norms);
     return check_launch("xlbb_batched_prolong_add_norms");
+}
+
+int xlbb_batched_prolong_add_map(int dtype_fine, int dtype_coarse, const XlbbBatchTransfer* tr_dev,
+                                 const int* map_dev, int nblocks, double* parts, const int* begin_dev, int ninst,
+                                 double* norms, void* stream) {
+    if (!tr_dev || !map_dev || nblocks <= 0 || ((parts != nullptr) != (norms != nullptr)) ||
+        (norms && (!begin_dev || ninst <= 0)))
+        return fail(XLBB_EBADARG, "xlbb_batched_prolong_add_map: bad argument");
+    cudaStream_t st = XLBB_STREAM(stream);
+    const int2* map = reinterpret_cast<const int2*>(map_dev);
+    if (dtype_fine == XLBB_F32 && dtype_coarse == XLBB_F32)
+        launch_k(batched_prolong_map_kernel<float, float>, nblocks, 256, 0, st, tr_dev, map, nblocks, parts);
+    else if (dtype_fine == XLBB_F32 && dtype_coarse == XLBB_F64)
+        launch_k(batched_prolong_map_kernel<float, double>, nblocks, 256, 0, st, tr_dev, map, nblocks, parts);
+    else if (dtype_fine == XLBB_F64 && dtype_coarse == XLBB_F64)
+        launch_k(batched_prolong_map_kernel<double, double>, nblocks, 256, 0, st, tr_dev, map, nblocks, parts);
+    else return fail(XLBB_EUNSUPPORTED, "xlbb_batched_prolong_add_map: dtype pair");
+    if (norms) launch_k(pair_segment_sum_kernel, ninst, 256, 0, st, (const double*)parts, nblocks, begin_dev, ninst,
+                        norms);
+    return check_launch("xlbb_batched_prolong_add_map");
 }
 
 int xlbb_segment_sum(const double* parts, const int* begin_dev, int nseg, double* out, void* stream) {
