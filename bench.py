@@ -620,6 +620,29 @@ def run_c4sweep(args):
     return 0
 
 
+def run_c4vcycle(args):
+    """Whole batched V-cycles of the 512-instance batch (one CUDA-graph replay
+    each, every level and transfer): ``--steps`` timed after ``--warmup``
+    (the first captures the graph); the workload of the per-kernel launch
+    list of a V-cycle."""
+    import torch
+    from xlb_biot_b200.batched import BatchedElasticity
+    from xlb_biot_b200.workloads import batch_instances
+    sizes, lams, mus, forces = batch_instances(count=args.instances)
+    b = BatchedElasticity(sizes, lams, mus, forces, levels="auto", precision="f32/f32", coarsest_precision="f64",
+                          residual_precision="f64")
+    b.reset()
+    for _ in range(max(3, args.warmup)):
+        b.vcycle()
+    (_, t) = _timed(lambda: [b.vcycle() for _ in range(args.steps)])
+    lu = b.lattice_updates_per_cycle()
+    print(json.dumps({"workload": "c4_batched_vcycle", "metric": "ms per V-cycle", "value": t / args.steps * 1e3,
+                      "unit": "ms", "higher_is_better": False, "vcycles": args.steps,
+                      "launches_per_vcycle": b.launches_per_cycle, "levels": b.levels,
+                      "glups": lu * args.steps / t / 1e9}), flush=True)
+    return 0
+
+
 def run_c5(args):
     """Adjoint of heterogeneous Terzaghi-type consolidation: 512 x 256 cells
     (arrays 512 x 258 with the boundary rows), 200 Biot steps, each with 4
@@ -726,7 +749,7 @@ def main():
                     help="tx,depth,ctas_per_sm,min_rows,pipeline of the elasticity sweeps (all workloads)")
     ap.add_argument("--adjoint-steps", type=int, default=200)
     ap.add_argument("--fd-directions", type=int, default=32)
-    ap.add_argument("--workload", choices=["darcy", "c1", "c3", "c4", "c4sweep", "c5"], default="darcy",
+    ap.add_argument("--workload", choices=["darcy", "c1", "c3", "c4", "c4sweep", "c4vcycle", "c5"], default="darcy",
                     help="darcy: the headline line; c1/c3/c4/c5: the other configurations (one JSON line each)")
     ap.add_argument("--biot-steps", type=int, default=100)
     ap.add_argument("--instances", type=int, default=512)
@@ -748,6 +771,8 @@ def main():
         return run_c5(args)
     if args.workload == "c4sweep":
         return run_c4sweep(args)
+    if args.workload == "c4vcycle":
+        return run_c4vcycle(args)
     return run_ours(args)
 
 

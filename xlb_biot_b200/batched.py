@@ -32,6 +32,18 @@ from .fields import pitch_for
 _ALIGN = 64   # elements; keeps every instance's planes 256-byte aligned
 
 
+def balanced_block_map(cells, per_block=1024):
+    """Block map of ``xlbb_batched_prolong_add_map``: ceil(cells[k] / per_block)
+    consecutive blocks for instance k, each the pair (k, first cell index).
+    Returns (int32 array (nblocks, 2), int32 begin array (len(cells) + 1):
+    instance k's blocks are begin[k] .. begin[k + 1])."""
+    blocks, begin = [], [0]
+    for k, n in enumerate(cells):
+        blocks += [(k, e) for e in range(0, int(n), per_block)]
+        begin.append(len(blocks))
+    return np.asarray(blocks, dtype=np.int32).reshape(-1, 2), np.asarray(begin, dtype=np.int32)
+
+
 def auto_levels(nx, ny, min_side=3):
     """Levels of the factor-2 hierarchy of an ``nx x ny`` grid whose coarsest
     side is the smallest one that is still >= ``min_side``."""
@@ -222,15 +234,9 @@ class BatchedElasticity:
                     _lib.dtype_code(dt), _lib.dtype_code(d_coarse), ids)
 
         def prolong_map(t, l):
-            """Balanced block map of a prolongation list: ceil(cells / 1024)
-            consecutive blocks per instance, each (instance, first cell)."""
-            blocks, begin = [], [0]
-            for k, g in enumerate(t[4]):
-                nx, ny = self.shapes[l][g]
-                blocks += [(k, e) for e in range(0, nx * ny, 1024)]
-                begin.append(len(blocks))
-            m = torch.as_tensor(np.asarray(blocks, dtype=np.int32).reshape(-1), device=dev)
-            return m, len(blocks), torch.as_tensor(np.asarray(begin, dtype=np.int32), device=dev)
+            blocks, begin = balanced_block_map([self.shapes[l][g][0] * self.shapes[l][g][1] for g in t[4]])
+            return (torch.as_tensor(blocks.reshape(-1), device=dev), len(blocks),
+                    torch.as_tensor(begin, device=dev))
 
         self.t_restrict, self.t_prolong = [], []
         for l in range(self.levels - 1):
