@@ -643,6 +643,64 @@ def run_c4vcycle(args):
     return 0
 
 
+def run_mlups2d(args):
+    """The fluid path of ``examples/performance/MLUPS2d.py``: lid-driven cavity
+    (Re = 100, u_wall = 0.1, full-way bounce-back walls, equilibrium lid),
+    D2Q9, FP32, ``--cavity-n`` squared cells (4096^2: 1.2 GB of populations,
+    far above L2), BGK and KBC collisions, ``--steps`` calls of the public
+    ``step`` timed with CUDA events; roofline at 72 B per cell (9 populations
+    read and written, FP32).  CPU baseline: the oracle's BGK step (vectorised
+    NumPy, one process) on a 512^2 cavity."""
+    import time
+    import numpy as np
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import xlb_biot_b200.api as G
+    from problems import make_cavity
+    n = args.cavity_n
+    peak, peak_kind = measured_peak_hbm()
+    out = {}
+    for model in ("bgk", "kbc"):
+        C, om = make_cavity(G, model)
+        s = C(lattice=G.LatticeD2Q9("f32/f32"), omega=om(n), nx=n, ny=n, nz=0, precision="f32/f32")
+        f = s.assign_fields_sharded()
+        for t in range(args.warmup):
+            f, _ = s.step(f, t)
+
+        def loop(f=f):
+            for t in range(args.steps):
+                f, _ = s.step(f, t)
+            return f
+        f, t = _timed(loop)
+        mlups = n * n * args.steps / t / 1e6
+        gbs = n * n * 72 * args.steps / t / 1e9
+        out[model] = {"mlups": mlups, "ms_per_step": t / args.steps * 1e3,
+                      "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
+                                   "peak_kind": peak_kind, "frac_of_spec": gbs / SPEC_HBM_GBS,
+                                   "spec_gbs": SPEC_HBM_GBS},
+                      "finite": bool(torch.isfinite(f).all())}
+        del s, f
+        torch.cuda.empty_cache()
+    cpu = None
+    if not args.no_cpu_baseline:
+        import oracle.api as O
+        Co, omo = make_cavity(O, "bgk")
+        so = Co(lattice=O.LatticeD2Q9("f32/f32"), omega=omo(512), nx=512, ny=512, nz=0, precision="f32/f32")
+        fo = so.assign_fields_sharded()
+        fo, _ = so.step(fo, 0)
+        t0, k = time.time(), 0
+        while time.time() - t0 < 10.0:
+            fo, _ = so.step(fo, k)
+            k += 1
+        cpu = {"value": 512 * 512 * k / (time.time() - t0) / 1e6, "unit": "MLUPS", "cores": 1, "kind": "port",
+               "sample": f"oracle BGK cavity step (NumPy, FP32), 512^2 cells, {k} steps"}
+    print(json.dumps({"workload": f"mlups2d_cavity_{n}x{n}", "metric": "MLUPS", "value": out["bgk"]["mlups"],
+                      "unit": "MLUPS", "dtype": "f32", "steps": args.steps, "warmup": args.warmup,
+                      "bgk": out["bgk"], "kbc": out["kbc"], "cpu_baseline": cpu,
+                      "data": "synthetic (cavity from rest, as the example)"}), flush=True)
+    return 0
+
+
 def run_c5(args):
     """Adjoint of heterogeneous Terzaghi-type consolidation: 512 x 256 cells
     (arrays 512 x 258 with the boundary rows), 200 Biot steps, each with 4
@@ -749,7 +807,9 @@ def main():
                     help="tx,depth,ctas_per_sm,min_rows,pipeline of the elasticity sweeps (all workloads)")
     ap.add_argument("--adjoint-steps", type=int, default=200)
     ap.add_argument("--fd-directions", type=int, default=32)
-    ap.add_argument("--workload", choices=["darcy", "c1", "c3", "c4", "c4sweep", "c4vcycle", "c5"], default="darcy",
+    ap.add_argument("--cavity-n", type=int, default=4096)
+    ap.add_argument("--workload", choices=["darcy", "c1", "c3", "c4", "c4sweep", "c4vcycle", "c5", "mlups2d"],
+                    default="darcy",
                     help="darcy: the headline line; c1/c3/c4/c5: the other configurations (one JSON line each)")
     ap.add_argument("--biot-steps", type=int, default=100)
     ap.add_argument("--instances", type=int, default=512)
@@ -773,6 +833,8 @@ def main():
         return run_c4sweep(args)
     if args.workload == "c4vcycle":
         return run_c4vcycle(args)
+    if args.workload == "mlups2d":
+        return run_mlups2d(args)
     return run_ours(args)
 
 

@@ -165,6 +165,19 @@ int xlbb_darcy_sweep(int dtype, const XlbbGrid* g, const XlbbDarcySweep* s, void
 int xlbb_darcy_sweep_ctas(int dtype, const XlbbGrid* g);
 
 /*
+ * One fused D2Q9 fluid step (replaces BGKSim.collision, src/models.py:20-34, or
+ * KBCSim.collision, :48-72, inside LBMBase.step, src/base.py:809-846):
+ * collision with the second-order equilibrium of src/base.py:686-724,
+ * PostCollision rules, streaming, PostStreaming rules.  Same argument block as
+ * xlbb_darcy_sweep (omega uniform or per cell); source and ext_source must be
+ * NULL (XLBB_EBADARG otherwise).  sumsq, when set, has
+ * xlbb_darcy_sweep_ctas(dtype, g) entries.
+ */
+#define XLBB_FLUID_BGK 0
+#define XLBB_FLUID_KBC 1
+int xlbb_fluid_sweep(int dtype, const XlbbGrid* g, const XlbbDarcySweep* s, int model, void* stream);
+
+/*
  * Darcy sweep plus its FP64 convergence residual, allocating nothing.
  * No counterpart in the reference: it exists for callers that cannot allocate
  * device memory (inside a CUDA-graph capture, host runtimes that hand the

@@ -2,8 +2,8 @@
 
 This package is a plain NumPy restatement of the reference solvers of
 s-lunowa/xlb-biot (JAX 0.5.3 code in ``src/elasticity.py``, ``src/darcy.py``,
-``src/poroelasticity.py``, ``src/boundary_conditions.py``, ``src/base.py`` and
-``src/lattice.py``).  Every function cites the reference ``file:line`` it
+``src/poroelasticity.py``, ``src/models.py``, ``src/boundary_conditions.py``,
+``src/base.py`` and ``src/lattice.py``).  Every function cites the reference ``file:line`` it
 follows.  It is used as the checker by ``tests/``, by ``__graft_entry__.smoke()``
 and by the ``cpu_baseline`` / ``--impl reference`` legs of ``bench.py``.  The
 product (``xlb_biot_b200``) never imports it.

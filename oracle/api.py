@@ -6,3 +6,4 @@ from .elasticity import (LBMElasticity, ElasticityBounceBackFullway, ElasticityB
 from .darcy import (AdvectionDiffusionReactionBGK, ADR_AntiBounceBack, ADR_Neumann_BounceBack,  # noqa: F401
                     ADR_EquilibriumBC)
 from .poroelasticity import LBMPoroelasticity  # noqa: F401
+from .models import BGKSim, KBCSim, BounceBack, EquilibriumBC  # noqa: F401

@@ -292,3 +292,43 @@ def make_terzaghi(m, force_value=-1.0, ny=4):
             self.records.append({k: np.array(v) for k, v in kwargs.items()
                                  if k in ("timestep", "eta", "sigma", "pressure", "pressure_grad", "dt_div_eta")})
     return TP
+
+
+def make_cavity(m, model="bgk", u_wall=0.1, Re=100.0):
+    """``examples/performance/MLUPS2d.py``: lid-driven cavity, full-way
+    bounce-back on the left, right and bottom walls, equilibrium (rho = 1,
+    u = (u_wall, 0)) on the top row; omega from Re with clength = n - 1."""
+    base = m.BGKSim if model == "bgk" else m.KBCSim
+
+    class Cavity(base):
+        def set_boundary_conditions(self):
+            bb = self.boundingBoxIndices
+            walls = np.concatenate((bb["left"], bb["right"], bb["bottom"]))
+            self.BCs.append(m.BounceBack(tuple(walls.T), self.gridInfo, self.precisionPolicy))
+            lid = bb["top"]
+            dt = self.precisionPolicy.compute_dtype
+            rho_wall = np.ones((lid.shape[0], 1), dtype=dt)
+            vel_wall = np.zeros(lid.shape, dtype=dt)
+            vel_wall[:, 0] = u_wall
+            self.BCs.append(m.EquilibriumBC(tuple(lid.T), self.gridInfo, self.precisionPolicy, rho_wall, vel_wall))
+
+    def omega(n):
+        return 1.0 / (3.0 * (u_wall * (n - 1) / Re) + 0.5)
+    return Cavity, omega
+
+
+def make_shear_wave(m, model="bgk", amp=0.02):
+    """Periodic decaying shear wave u_x(y) = amp sin(2 pi (y + 1/2) / ny) at
+    rho = 1: the incompressible solution decays as exp(-nu k^2 t) with
+    nu = (1 / omega - 1/2) / 3 and k = 2 pi / ny."""
+    base = m.BGKSim if model == "bgk" else m.KBCSim
+
+    class ShearWave(base):
+        def initialize_macroscopic_fields(self):
+            y = (np.arange(self.ny) + 0.5) / self.ny
+            u = np.zeros((self.nx, self.ny, 2))
+            u[..., 0] = amp * np.sin(2 * np.pi * y)[None, :]
+            rho = np.ones((self.nx, self.ny, 1))
+            dt = self.precisionPolicy.compute_dtype
+            return rho.astype(dt), u.astype(dt)
+    return ShearWave

@@ -84,9 +84,18 @@ def _scenarios():
         return [BB(tuple(b["bottom"].T), gi, pp), AntiBB(tuple(b["top"].T), gi, pp),
                 m.ADR_EquilibriumBC(tuple(b["left"].T), gi, pp, rho=0.25)]
 
+    def cavity(m, lat, gi, pp, nx, ny):
+        b = bbox(nx, ny)
+        walls = np.concatenate((b["left"], b["right"], b["bottom"]))
+        vel = np.zeros(b["top"].shape)
+        vel[:, 0] = 0.1
+        return [m.BounceBack(tuple(walls.T), gi, pp),
+                m.EquilibriumBC(tuple(b["top"].T), gi, pp, np.ones((len(b["top"]), 1)), vel)]
+
     return [("dirichlet_fullway", 8, 10, 9, dirichlet_full), ("neumann_antibb", 8, 10, 9, neumann),
             ("halfway_bb", 8, 9, 8, halfway), ("terzaghi_elasticity", 8, 12, 4, terz_el),
-            ("adr_anti_rho", 9, 10, 9, adr_anti), ("adr_mixed", 9, 11, 10, adr_mixed)]
+            ("adr_anti_rho", 9, 10, 9, adr_anti), ("adr_mixed", 9, 11, 10, adr_mixed),
+            ("lid_driven_cavity", 9, 10, 9, cavity)]
 
 
 @pytest.mark.parametrize("name,q,nx,ny,builder", _scenarios(), ids=[s[0] for s in _scenarios()])

@@ -11,6 +11,7 @@ reference module                       this package
 ``src.elasticity``                     ``xlb_biot_b200.elasticity``
 ``src.darcy``                          ``xlb_biot_b200.darcy``
 ``src.poroelasticity``                 ``xlb_biot_b200.poroelasticity``
+``src.models`` (D2Q9 BGK, KBC)         ``xlb_biot_b200.models``
 ``src.utils`` (Parameters, downsample) ``xlb_biot_b200.utils``
 =====================================  ==========================================
 
@@ -23,7 +24,8 @@ import sys
 
 __version__ = "1.0.0"
 
-_MODULES = ("lattice", "boundary_conditions", "base", "elasticity", "darcy", "poroelasticity", "utils")
+_MODULES = ("lattice", "boundary_conditions", "base", "elasticity", "darcy", "poroelasticity", "models",
+            "utils")
 
 
 def install_as_src():

@@ -94,6 +94,7 @@ SIGNATURES = {
     "xlbb_elast_sweep_ctas": (I, [I, PG]),
     "xlbb_darcy_sweep": (I, [I, PG, ctypes.POINTER(DarcySweep), P]),
     "xlbb_darcy_sweep_ctas": (I, [I, PG]),
+    "xlbb_fluid_sweep": (I, [I, PG, ctypes.POINTER(DarcySweep), I, P]),
     "xlbb_darcy_sweep_residual_noalloc": (I, [I, PG, ctypes.POINTER(DarcySweep), P, P]),
     "xlbb_darcy_gradient": (I, [I, PG, P, D, ctypes.POINTER(Rules), P, P, P]),
     "xlbb_elast_divgrad": (I, [I, PG, ctypes.POINTER(ElastMaterial), D, P, D, ctypes.POINTER(Rules), P, P, P]),

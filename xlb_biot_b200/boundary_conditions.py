@@ -212,6 +212,33 @@ class BounceBackHalfway(BoundaryCondition):
         return fbd
 
 
+class BounceBack(BoundaryCondition):
+    """``src/boundary_conditions.py:351-394``: full-way bounce-back, after the
+    collision: the wall cell's output is its input reflected, fin[opp]."""
+
+    def __init__(self, indices, gridInfo, precision_policy):
+        super().__init__(indices, gridInfo, precision_policy)
+        self.name = "BounceBackFullway"
+        self.implementationStep = "PostCollision"
+
+    def apply(self, fout, fin):
+        return np.array(_take(fin, self.indices))[:, self.lattice.opp_indices]
+
+
+class EquilibriumBC(BoundaryCondition):
+    """``src/boundary_conditions.py:549-595``: the populations of the boundary
+    cells are set, after streaming, to the equilibrium of (``rho``, ``u``)."""
+
+    def __init__(self, indices, gridInfo, precision_policy, rho, u):
+        super().__init__(indices, gridInfo, precision_policy)
+        self.out = self.equilibrium(rho, u)
+        self.name = "EquilibriumBC"
+        self.implementationStep = "PostStreaming"
+
+    def apply(self, fout, fin):
+        return self.out
+
+
 def apply_in_order(bcs, fout, fin, implementation_step=None, names=None):
     """Apply an ordered BC list to full-grid arrays (in place on ``fout``), as
     ``apply_bc`` (``src/elasticity.py:1061-1091``) does for one implementation

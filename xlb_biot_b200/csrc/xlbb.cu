@@ -451,6 +451,83 @@ struct DarcyPhys {
     }
 };
 
+// ---------------------------------------------------------------------------
+// D2Q9 fluid models of src/models.py: BGK (:20-34) and KBC (:48-72).
+// rho = sum f, u = sum c f / rho (src/base.py:748-772), feq = rho w (1 + cu
+// (1 + cu / 2) - usqr) with cu = 3 c.u, usqr = 3/2 |u|^2 (src/base.py:686-724).
+// BGK: f* = f - omega (f - feq).  KBC: fneq = f - feq splits into the shear
+// part dS (fdecompose_shear_d2q9, :127-154, times rho / 4) and dH = fneq - dS;
+// with beta = omega / 2 and the entropic products <x, y> = sum x y / feq,
+// gamma = 1 / beta - (2 - 1 / beta) <dS, dH> / (1e-32 + <dH, dH>) and
+// f* = f - beta (2 dS + gamma dH).  Same planes, rules and sweep pipelines as
+// the Darcy step; only the collision differs (no source terms: the fluid entry
+// point rejects them).
+// ---------------------------------------------------------------------------
+template <typename T_, bool KBC>
+struct FluidPhys : DarcyPhys<T_> {
+    using T = T_;
+    using Args = typename DarcyPhys<T_>::Args;
+    using In = typename DarcyPhys<T_>::In;
+    __device__ static void collide(const Args&, int, int, const In& in, T (&o)[9]) {
+        T rho = in.f[0];
+#pragma unroll
+        for (int i = 1; i < 9; ++i) rho += in.f[i];
+        // momentum: D2Q9 x-velocities (+) 3, 5, 7 and (-) 4, 6, 8; y (+) 1, 4, 7 and (-) 2, 5, 8
+        const T jx = ((in.f[3] - in.f[4]) + (in.f[5] - in.f[6])) + (in.f[7] - in.f[8]);
+        const T jy = ((in.f[1] - in.f[2]) + (in.f[4] - in.f[5])) + (in.f[7] - in.f[8]);
+        const T ux = jx / rho, uy = jy / rho;
+        const T usqr = T(1.5) * (ux * ux + uy * uy);
+        const T om = in.om;
+        T feq[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            const T cu = T(3) * (T(cx9(i)) * ux + T(cy9(i)) * uy);
+            feq[i] = rho * w9<T>(i) * (T(1) + cu * (T(1) + T(0.5) * cu) - usqr);
+        }
+        if constexpr (!KBC) {
+#pragma unroll
+            for (int i = 0; i < 9; ++i) o[i] = in.f[i] - om * (in.f[i] - feq[i]);
+        } else {
+            T fneq[9];
+#pragma unroll
+            for (int i = 0; i < 9; ++i) fneq[i] = in.f[i] - feq[i];
+            // momentum flux of fneq: axis directions 1-4 / 6 carry cx^2 or cy^2,
+            // diagonals 4, 5, 7, 8 carry both and cx cy = -1 (4, 5) or +1 (7, 8)
+            const T dg = ((fneq[4] + fneq[5]) + (fneq[7] + fneq[8]));
+            const T pxx = (fneq[3] + fneq[6]) + dg;
+            const T pyy = (fneq[1] + fneq[2]) + dg;
+            const T pxy = (fneq[7] + fneq[8]) - (fneq[4] + fneq[5]);
+            const T N = pxx - pyy;
+            const T r4 = rho / T(4);
+            T dS[9];
+            dS[0] = T(0);
+            dS[1] = -N * r4;
+            dS[2] = -N * r4;
+            dS[3] = N * r4;
+            dS[6] = N * r4;
+            dS[4] = -pxy * r4;
+            dS[5] = -pxy * r4;
+            dS[7] = pxy * r4;
+            dS[8] = pxy * r4;
+            T sh = T(0), hh = T(0);
+#pragma unroll
+            for (int i = 0; i < 9; ++i) {
+                const T dH = fneq[i] - dS[i];
+                sh += dS[i] * dH / feq[i];
+                hh += dH * dH / feq[i];
+            }
+            const T beta = om * T(0.5);
+            const T ib = T(1) / beta;
+            const T gamma = ib - (T(2) - ib) * sh / (T(1e-32) + hh);
+#pragma unroll
+            for (int i = 0; i < 9; ++i) {
+                const T dH = fneq[i] - dS[i];
+                o[i] = in.f[i] - beta * (T(2) * dS[i] + gamma * dH);
+            }
+        }
+    }
+};
+
 #include "xlbb_push.cuh"
 
 // Launch geometry of the sweeps: tx owned columns per CTA, strips of rows
@@ -926,6 +1003,26 @@ static int darcy_sweep_t(const XlbbGrid* g, const XlbbDarcySweep* s, cudaStream_
     if (s->sumsq) launch_sweep<Ph, true>(c, g, st, a);
     else launch_sweep<Ph, false>(c, g, st, a);
     return check_launch("xlbb_darcy_sweep");
+}
+
+template <typename T, bool KBC>
+static int fluid_sweep_t(const XlbbGrid* g, const XlbbDarcySweep* s, cudaStream_t st) {
+    using Ph = FluidPhys<T, KBC>;
+    typename Ph::Args a;
+    a.geom = geom(g);
+    a.f_in = static_cast<const T*>(s->f_in);
+    a.f_out = static_cast<T*>(s->f_out);
+    a.omega = T(s->omega);
+    a.omega_f = static_cast<const T*>(s->omega_field);
+    a.source = nullptr;
+    a.ext = nullptr;
+    a.pc = rules_view<T, 9>(s->pc);
+    a.ps = rules_view<T, 9>(s->ps);
+    a.sumsq = s->sumsq;
+    const XlbbSweepConfig c = effective_cfg(1, sizeof(T) == 4 ? XLBB_F32 : XLBB_F64);
+    if (s->sumsq) launch_sweep<Ph, true>(c, g, st, a);
+    else launch_sweep<Ph, false>(c, g, st, a);
+    return check_launch("xlbb_fluid_sweep");
 }
 
 static inline dim3 row_grid(int nx, int ny, int bs) { return dim3((nx + bs - 1) / bs, ny); }
@@ -1808,6 +1905,21 @@ int xlbb_darcy_sweep(int dtype, const XlbbGrid* g, const XlbbDarcySweep* s, void
     if (dtype == XLBB_F32) return darcy_sweep_t<float>(g, s, XLBB_STREAM(stream));
     if (dtype == XLBB_F64) return darcy_sweep_t<double>(g, s, XLBB_STREAM(stream));
     return fail(XLBB_EUNSUPPORTED, "xlbb_darcy_sweep: dtype");
+}
+
+int xlbb_fluid_sweep(int dtype, const XlbbGrid* g, const XlbbDarcySweep* s, int model, void* stream) {
+    if (!grid_ok(g) || !s || !s->f_in || !s->f_out) return fail(XLBB_EBADARG, "xlbb_fluid_sweep: bad argument");
+    if (model != XLBB_FLUID_BGK && model != XLBB_FLUID_KBC) return fail(XLBB_EBADARG, "xlbb_fluid_sweep: model");
+    if (s->f_in == s->f_out) return fail(XLBB_EBADARG, "xlbb_fluid_sweep: f_in and f_out must differ");
+    if (s->source || s->ext_source) return fail(XLBB_EBADARG, "xlbb_fluid_sweep: source planes are not supported");
+    if (!rules_ok(s->pc, g) || !rules_ok(s->ps, g)) return fail(XLBB_EBADARG, "xlbb_fluid_sweep: incomplete rules");
+
+    const bool kbc = model == XLBB_FLUID_KBC;
+    if (dtype == XLBB_F32)
+        return kbc ? fluid_sweep_t<float, true>(g, s, XLBB_STREAM(stream)) : fluid_sweep_t<float, false>(g, s, XLBB_STREAM(stream));
+    if (dtype == XLBB_F64)
+        return kbc ? fluid_sweep_t<double, true>(g, s, XLBB_STREAM(stream)) : fluid_sweep_t<double, false>(g, s, XLBB_STREAM(stream));
+    return fail(XLBB_EUNSUPPORTED, "xlbb_fluid_sweep: dtype");
 }
 
 int xlbb_darcy_gradient(int dtype, const XlbbGrid* g, const void* q, double scale, const XlbbRules* rules,
