@@ -654,9 +654,8 @@ def run_mlups2d(args):
     import time
     import numpy as np
     import torch
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
     import xlb_biot_b200.api as G
-    from problems import make_cavity
+    from xlb_biot_b200.workloads import lid_driven_cavity as make_cavity
     n = args.cavity_n
     peak, peak_kind = measured_peak_hbm()
     out = {}

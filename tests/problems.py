@@ -295,26 +295,10 @@ def make_terzaghi(m, force_value=-1.0, ny=4):
 
 
 def make_cavity(m, model="bgk", u_wall=0.1, Re=100.0):
-    """``examples/performance/MLUPS2d.py``: lid-driven cavity, full-way
-    bounce-back on the left, right and bottom walls, equilibrium (rho = 1,
-    u = (u_wall, 0)) on the top row; omega from Re with clength = n - 1."""
-    base = m.BGKSim if model == "bgk" else m.KBCSim
-
-    class Cavity(base):
-        def set_boundary_conditions(self):
-            bb = self.boundingBoxIndices
-            walls = np.concatenate((bb["left"], bb["right"], bb["bottom"]))
-            self.BCs.append(m.BounceBack(tuple(walls.T), self.gridInfo, self.precisionPolicy))
-            lid = bb["top"]
-            dt = self.precisionPolicy.compute_dtype
-            rho_wall = np.ones((lid.shape[0], 1), dtype=dt)
-            vel_wall = np.zeros(lid.shape, dtype=dt)
-            vel_wall[:, 0] = u_wall
-            self.BCs.append(m.EquilibriumBC(tuple(lid.T), self.gridInfo, self.precisionPolicy, rho_wall, vel_wall))
-
-    def omega(n):
-        return 1.0 / (3.0 * (u_wall * (n - 1) / Re) + 0.5)
-    return Cavity, omega
+    """``examples/performance/MLUPS2d.py`` (the benchmark workload of the same
+    name): returns the cavity class and ``omega(n)``."""
+    from xlb_biot_b200.workloads import lid_driven_cavity
+    return lid_driven_cavity(m, model, u_wall, Re)
 
 
 def make_shear_wave(m, model="bgk", amp=0.02):

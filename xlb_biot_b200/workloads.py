@@ -8,6 +8,7 @@ exposes the reference's class names.
   left wall and 0 on the right wall (ADR anti-bounce-back), no flux at the
   bottom and top walls (ADR bounce-back), corner directions patched as in the
   reference's Terzaghi example.
+* ``lid_driven_cavity``: the D2Q9 fluid cavity of ``MLUPS2d.py``.
 """
 import numpy as np
 
@@ -283,3 +284,28 @@ def terzaghi_heterogeneous(m, nx=512, ny=258, levels=5, mu0=TERZAGHI_MU, lam0=TE
     if getattr(sim.darcy, "omega_field", None) is None:
         sim.darcy.omega = omega[..., None].astype(sim.darcy.precisionPolicy.compute_dtype)
     return sim, dict(log_mu=g_mu, log_k=g_k, mu=mu, lam=lam, K=K, omega=omega)
+
+
+def lid_driven_cavity(m, model="bgk", u_wall=0.1, Re=100.0):
+    """The fluid workload of ``examples/performance/MLUPS2d.py``: lid-driven
+    cavity with full-way bounce-back on the left, right and bottom walls and
+    the equilibrium of (rho = 1, u = (u_wall, 0)) on the top row.  Returns the
+    solver class (``m.BGKSim`` or ``m.KBCSim`` based) and ``omega(n)`` from
+    ``Re`` with the example's characteristic length n - 1."""
+    base = m.BGKSim if model == "bgk" else m.KBCSim
+
+    class Cavity(base):
+        def set_boundary_conditions(self):
+            bb = self.boundingBoxIndices
+            walls = np.concatenate((bb["left"], bb["right"], bb["bottom"]))
+            self.BCs.append(m.BounceBack(tuple(walls.T), self.gridInfo, self.precisionPolicy))
+            lid = bb["top"]
+            dt = self.precisionPolicy.compute_dtype
+            rho_wall = np.ones((lid.shape[0], 1), dtype=dt)
+            vel_wall = np.zeros(lid.shape, dtype=dt)
+            vel_wall[:, 0] = u_wall
+            self.BCs.append(m.EquilibriumBC(tuple(lid.T), self.gridInfo, self.precisionPolicy, rho_wall, vel_wall))
+
+    def omega(n):
+        return 1.0 / (3.0 * (u_wall * (n - 1) / Re) + 0.5)
+    return Cavity, omega
