@@ -118,8 +118,9 @@ typedef struct {
  * STEP applies force (if use_force) + fext as in collision() (:959-1000).
  * If sumsq != NULL, each CTA writes sum(out^2) (sumsq_diff = 0) or
  * sum((out - f_in)^2) (sumsq_diff = 1) over the box [bx0,bx1)x[by0,by1) into
- * sumsq[cta] (FP64; reduce with xlbb_reduce_sum); count via
- * xlbb_elast_sweep_ctas().  If div_out != NULL the divergence moment of out
+ * sumsq[cta] (FP64; reduce with xlbb_reduce_sum); the buffer needs
+ * xlbb_elast_sweep_ctas() entries, the reduction the exact count
+ * xlbb_elast_sweep_partials().  If div_out != NULL the divergence moment of out
  * (update_divergence, :1040-1058) is written as a side output.
  */
 typedef struct {
@@ -139,7 +140,15 @@ typedef struct {
 
 int xlbb_elast_sweep(int dtype, const XlbbGrid* g, const XlbbElastMaterial* mat,
                      const XlbbElastSweep* s, void* stream);
-int xlbb_elast_sweep_ctas(int dtype, const XlbbGrid* g);   /* CTAs of the next launch of this dtype */
+/* Upper bound on the FP64 partials of any elasticity sweep of this dtype on g
+ * under the current launch config (size of a partials buffer). */
+int xlbb_elast_sweep_ctas(int dtype, const XlbbGrid* g);
+/* Exactly the partials that xlbb_elast_sweep with these arguments writes when
+ * s->sumsq is set (the CTAs of the launch it takes: collide-and-push, or the
+ * row-marching shape when its post-streaming rules have no push words or it
+ * writes div_out); pass this count to xlbb_reduce_sum. */
+int xlbb_elast_sweep_partials(int dtype, const XlbbGrid* g, const XlbbElastMaterial* mat,
+                              const XlbbElastSweep* s);
 /* The pipeline (XlbbSweepConfig numbering; 0 for the row-marching kernel)
  * that xlbb_elast_sweep would run for these arguments now (diagnostic). */
 int xlbb_elast_sweep_pipeline(int dtype, const XlbbGrid* g, const XlbbElastMaterial* mat,
@@ -162,7 +171,15 @@ typedef struct {
 } XlbbDarcySweep;
 
 int xlbb_darcy_sweep(int dtype, const XlbbGrid* g, const XlbbDarcySweep* s, void* stream);
+/* Upper bound on the FP64 partials of any D2Q9 sweep of this dtype on g under
+ * the current launch config (size of a partials buffer). */
 int xlbb_darcy_sweep_ctas(int dtype, const XlbbGrid* g);
+/* Exactly the partials that xlbb_darcy_sweep / xlbb_fluid_sweep with these
+ * arguments writes when s->sumsq is set; pass this count to xlbb_reduce_sum. */
+int xlbb_darcy_sweep_partials(int dtype, const XlbbGrid* g, const XlbbDarcySweep* s);
+/* The pipeline (XlbbSweepConfig numbering) that xlbb_darcy_sweep would run
+ * for these arguments now (diagnostic). */
+int xlbb_darcy_sweep_pipeline(int dtype, const XlbbGrid* g, const XlbbDarcySweep* s);
 
 /*
  * One fused D2Q9 fluid step (replaces BGKSim.collision, src/models.py:20-34, or
@@ -171,7 +188,8 @@ int xlbb_darcy_sweep_ctas(int dtype, const XlbbGrid* g);
  * PostCollision rules, streaming, PostStreaming rules.  Same argument block as
  * xlbb_darcy_sweep (omega uniform or per cell); source and ext_source must be
  * NULL (XLBB_EBADARG otherwise).  sumsq, when set, has
- * xlbb_darcy_sweep_ctas(dtype, g) entries.
+ * xlbb_darcy_sweep_ctas(dtype, g) entries, of which it writes
+ * xlbb_darcy_sweep_partials(dtype, g, s).
  */
 #define XLBB_FLUID_BGK 0
 #define XLBB_FLUID_KBC 1
@@ -186,8 +204,11 @@ int xlbb_fluid_sweep(int dtype, const XlbbGrid* g, const XlbbDarcySweep* s, int 
  * (s->sumsq is ignored) plus sumsq_out, one device double that receives
  * sum((f_out - f_in)^2).  The per-CTA partial sums go to a scratch array built
  * into the library: XLBB_NOALLOC_MAX_PARTIALS doubles (128 KiB) held by every
- * GPU that loads the library until exit; launch shapes needing more CTAs are
- * rejected with XLBB_EBADARG.  The first call on a device looks up the
+ * GPU that loads the library until exit; a sweep whose launch has more CTAs
+ * (xlbb_darcy_sweep_partials) is rejected with XLBB_EBADARG.  Under the
+ * default collide-and-push shape that is ceil(nx / 128) * ny > 16384, e.g.
+ * every grid of 2048 x 2048 or more; row-marching shapes (pipelines 0-2) have
+ * about ctas_per_sm CTAs per SM at any size.  The first call on a device looks up the
  * array's device address (cudaGetSymbolAddress), so make that first call
  * before any stream capture.  All calls share the array, which keeps the last
  * call's contents (each used slot is rewritten before it is read, so nothing

@@ -14,6 +14,7 @@ LIB_PATH = os.path.join(_HERE, "libxlbb.so")
 XLBB_F32, XLBB_F64, XLBB_F32_ACC64 = 0, 1, 2
 XLBB_PROLONG_BLOCKS = 32
 XLBB_BATCH_PARTS_PER_TILE = 32       # FP64 partials per tile of a batched sweep with sums
+XLBB_OK, XLBB_EBADARG, XLBB_ELAUNCH, XLBB_ETIMEOUT, XLBB_ENONFINITE, XLBB_EUNSUPPORTED = 0, -1, -2, -3, -4, -5
 ERRORS = {-1: "XLBB_EBADARG", -2: "XLBB_ELAUNCH", -3: "XLBB_ETIMEOUT", -4: "XLBB_ENONFINITE",
           -5: "XLBB_EUNSUPPORTED"}
 
@@ -92,8 +93,11 @@ SIGNATURES = {
     "xlbb_elast_sweep": (I, [I, PG, ctypes.POINTER(ElastMaterial), ctypes.POINTER(ElastSweep), P]),
     "xlbb_elast_sweep_pipeline": (I, [I, PG, ctypes.POINTER(ElastMaterial), ctypes.POINTER(ElastSweep)]),
     "xlbb_elast_sweep_ctas": (I, [I, PG]),
+    "xlbb_elast_sweep_partials": (I, [I, PG, ctypes.POINTER(ElastMaterial), ctypes.POINTER(ElastSweep)]),
     "xlbb_darcy_sweep": (I, [I, PG, ctypes.POINTER(DarcySweep), P]),
     "xlbb_darcy_sweep_ctas": (I, [I, PG]),
+    "xlbb_darcy_sweep_partials": (I, [I, PG, ctypes.POINTER(DarcySweep)]),
+    "xlbb_darcy_sweep_pipeline": (I, [I, PG, ctypes.POINTER(DarcySweep)]),
     "xlbb_fluid_sweep": (I, [I, PG, ctypes.POINTER(DarcySweep), I, P]),
     "xlbb_darcy_sweep_residual_noalloc": (I, [I, PG, ctypes.POINTER(DarcySweep), P, P]),
     "xlbb_darcy_gradient": (I, [I, PG, P, D, ctypes.POINTER(Rules), P, P, P]),

@@ -35,13 +35,16 @@ def set_config(kernel, tx, depth, ctas_per_sm, min_rows, pipeline=0):
     _lib.check(_lib.lib().xlbb_sweep_set_config(kernel, c), "xlbb_sweep_set_config")
 
 
-def candidates(dtype_bytes=4):
+def candidates(dtype_bytes=4, kernel=ELASTICITY):
     """Every launch shape the library instantiates for the given element size
-    (pipelines 3 and 4 ignore depth, CTAs per SM and strip height; pipeline 4,
-    the four-column form of eligible FP32 elasticity sweeps, is pipeline 3
-    for every other sweep)."""
+    and kernel family (pipelines 3 and 4 ignore depth, CTAs per SM and strip
+    height; pipeline 4, the four-column form of eligible FP32 elasticity
+    sweeps, is pipeline 3 for every other sweep, so the D2Q9 family does not
+    list it)."""
     out = []
     for pipe, depths in DEPTH.items():
+        if pipe == 4 and kernel != ELASTICITY:
+            continue
         ctas, rows = (CTAS_PER_SM, MIN_ROWS) if pipe < 3 else ((1,), (8,))   # pipelines 3, 4: only tx matters
         for t, d, c, m in itertools.product(TX if pipe != 2 else (128,), depths, ctas, rows):
             if dtype_bytes == 8 and (t > 128 or d > 4 or pipe == 4):
@@ -103,7 +106,7 @@ def tune(kernel, run, key, reps=5, cands_override=None, use_cache=True):
         cfg = cache[full_key]["config"]
         set_config(kernel, **cfg)
         return cfg, cache[full_key]["ms"], None
-    cands = candidates() if cands_override is None else cands_override
+    cands = candidates(kernel=kernel) if cands_override is None else cands_override
     table = []
     for cfg in cands:
         set_config(kernel, **cfg)

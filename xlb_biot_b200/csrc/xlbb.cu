@@ -11,6 +11,8 @@
 #include <vector>
 #include <cstdlib>
 #include <utility>
+#include <algorithm>
+#include <climits>
 
 #include "xlbb.h"
 #include "xlbb_common.cuh"
@@ -563,6 +565,29 @@ static dim3 sweep_grid(const XlbbGrid* g, const XlbbSweepConfig& c) {
     return dim3(nbx, nby);
 }
 
+// The launch shape a sweep takes under config c: pipeline 3 collides and
+// pushes only when the sweep is push-eligible (its post-streaming rules carry
+// push words and it has no divergence side output); otherwise it runs on the
+// row-marching fallback shape.  Every launcher and every partial-count query
+// resolves the shape here, so a fused sum's partials are counted on the grid
+// that wrote them.
+static XlbbSweepConfig resolve_shape(XlbbSweepConfig c, bool push, bool f32) {
+    if (c.pipeline == 3 && !push) return push_fallback(f32);
+    return c;
+}
+
+// CTAs (= FP64 partials of a fused sum) of a launch with the resolved shape c.
+static long long launch_ctas(const XlbbGrid* g, const XlbbSweepConfig& c) {
+    if (c.pipeline == 3) return (long long)((g->nx + c.tx - 1) / c.tx) * g->ny;   // one per push block
+    const dim3 a = sweep_grid(g, c);
+    return (long long)a.x * a.y;
+}
+
+template <class Ph>
+static bool push_eligible(const typename Ph::Args& a) {
+    return Ph::push_ok(a) && (a.ps.count == 0 || a.ps.push != nullptr);
+}
+
 // Runtime (tx, depth) -> template instance.
 template <class Ph, int TX, int D, bool PREV>
 static void launch_bulk(dim3 grid, cudaStream_t st, const typename Ph::Args& a) {
@@ -603,12 +628,10 @@ template <class Ph, bool PREV>
 static void launch_sweep(XlbbSweepConfig c, const XlbbGrid* g, cudaStream_t st, typename Ph::Args& a) {
     constexpr bool F32 = sizeof(typename Ph::T) == 4;
     Ph::fill_ptrs(a);
+    c = resolve_shape(c, push_eligible<Ph>(a), F32);
     if (c.pipeline == 3) {
-        if (Ph::push_ok(a) && (a.ps.count == 0 || a.ps.push != nullptr)) {
-            launch_push<Ph>(c, g, st, a);
-            return;
-        }
-        c = push_fallback(F32);
+        launch_push<Ph>(c, g, st, a);
+        return;
     }
     const dim3 grid = sweep_grid(g, c);
     if (c.pipeline == 2) {
@@ -645,7 +668,8 @@ static void launch_sweep(XlbbSweepConfig c, const XlbbGrid* g, cudaStream_t st, 
     launch_k(sweep_kernel<Ph, 128, 1, PREV>, grid, 128 + 32, 0, st, a);
 }
 
-// FP32 storage / FP64 arithmetic: the register-prefetch kernel at tx = 128.
+// FP32 storage / FP64 arithmetic: the register-prefetch kernel at tx = 128
+// (c is a resolved row-marching shape).
 template <class Ph, bool PREV>
 static void launch_sweep_regs(const XlbbSweepConfig& c, const XlbbGrid* g, cudaStream_t st,
                               typename Ph::Args& a) {
@@ -985,9 +1009,11 @@ static ElastMat<T, S> make_mat(const XlbbElastMaterial* m) {
 }
 
 
-template <typename T>
-static int darcy_sweep_t(const XlbbGrid* g, const XlbbDarcySweep* s, cudaStream_t st) {
-    using Ph = DarcyPhys<T>;
+// Kernel arguments of a D2Q9 sweep (Darcy or fluid policy; the fluid entry
+// point rejects source planes before this is built).
+template <class Ph>
+static typename Ph::Args darcy_args(const XlbbGrid* g, const XlbbDarcySweep* s) {
+    using T = typename Ph::T;
     typename Ph::Args a;
     a.geom = geom(g);
     a.f_in = static_cast<const T*>(s->f_in);
@@ -999,6 +1025,23 @@ static int darcy_sweep_t(const XlbbGrid* g, const XlbbDarcySweep* s, cudaStream_
     a.pc = rules_view<T, 9>(s->pc);
     a.ps = rules_view<T, 9>(s->ps);
     a.sumsq = s->sumsq;
+    return a;
+}
+
+// FP64 partials that a D2Q9 sweep with these arguments writes when it fuses
+// its residual sum (the CTAs of the launch it takes).
+template <typename T>
+static long long darcy_partials_t(const XlbbGrid* g, const XlbbDarcySweep* s) {
+    using Ph = DarcyPhys<T>;
+    const typename Ph::Args a = darcy_args<Ph>(g, s);
+    const XlbbSweepConfig c = effective_cfg(1, sizeof(T) == 4 ? XLBB_F32 : XLBB_F64);
+    return launch_ctas(g, resolve_shape(c, push_eligible<Ph>(a), sizeof(T) == 4));
+}
+
+template <typename T>
+static int darcy_sweep_t(const XlbbGrid* g, const XlbbDarcySweep* s, cudaStream_t st) {
+    using Ph = DarcyPhys<T>;
+    typename Ph::Args a = darcy_args<Ph>(g, s);
     const XlbbSweepConfig c = effective_cfg(1, sizeof(T) == 4 ? XLBB_F32 : XLBB_F64);
     if (s->sumsq) launch_sweep<Ph, true>(c, g, st, a);
     else launch_sweep<Ph, false>(c, g, st, a);
@@ -1008,17 +1051,7 @@ static int darcy_sweep_t(const XlbbGrid* g, const XlbbDarcySweep* s, cudaStream_
 template <typename T, bool KBC>
 static int fluid_sweep_t(const XlbbGrid* g, const XlbbDarcySweep* s, cudaStream_t st) {
     using Ph = FluidPhys<T, KBC>;
-    typename Ph::Args a;
-    a.geom = geom(g);
-    a.f_in = static_cast<const T*>(s->f_in);
-    a.f_out = static_cast<T*>(s->f_out);
-    a.omega = T(s->omega);
-    a.omega_f = static_cast<const T*>(s->omega_field);
-    a.source = nullptr;
-    a.ext = nullptr;
-    a.pc = rules_view<T, 9>(s->pc);
-    a.ps = rules_view<T, 9>(s->ps);
-    a.sumsq = s->sumsq;
+    typename Ph::Args a = darcy_args<Ph>(g, s);
     const XlbbSweepConfig c = effective_cfg(1, sizeof(T) == 4 ? XLBB_F32 : XLBB_F64);
     if (s->sumsq) launch_sweep<Ph, true>(c, g, st, a);
     else launch_sweep<Ph, false>(c, g, st, a);
@@ -1602,8 +1635,8 @@ static int launch_elast(const XlbbGrid* g, const XlbbElastMaterial* mat, const X
     using Ph = ElastPhys<T, RESID, S>;
     typename Ph::Args a = elast_args<T, RESID, S>(g, mat, s);
     if constexpr (sizeof(T) != sizeof(S)) {
-        const XlbbSweepConfig c = effective_cfg(0, XLBB_F32_ACC64);
-        if (c.pipeline == 3 && Ph::push_ok(a) && (a.ps.count == 0 || a.ps.push != nullptr)) {
+        const XlbbSweepConfig c = resolve_shape(effective_cfg(0, XLBB_F32_ACC64), push_eligible<Ph>(a), false);
+        if (c.pipeline == 3) {
             Ph::fill_ptrs(a);
             launch_push<Ph>(c, g, st, a);
         } else {
@@ -1643,6 +1676,17 @@ static int elast_sweep_t(const XlbbGrid* g, const XlbbElastMaterial* mat, const 
     if (s->resid)
         return mix ? launch_elast<T, true, true, S>(g, mat, s, st) : launch_elast<T, true, false, S>(g, mat, s, st);
     return mix ? launch_elast<T, false, true, S>(g, mat, s, st) : launch_elast<T, false, false, S>(g, mat, s, st);
+}
+
+// FP64 partials that an elasticity sweep with these arguments writes with a
+// fused sum (the four-column kernel never takes a fused sum).
+template <typename T, typename S>
+static long long elast_partials_t(const XlbbGrid* g, const XlbbElastMaterial* mat, const XlbbElastSweep* s,
+                                  int dtype) {
+    using Ph = ElastPhys<T, false, S>;
+    const typename Ph::Args a = elast_args<T, false, S>(g, mat, s);
+    const XlbbSweepConfig c = effective_cfg(0, dtype);
+    return launch_ctas(g, resolve_shape(c, push_eligible<Ph>(a), sizeof(T) == 4));
 }
 
 // Restriction (2x2 block sums) and prolongation (injection, added) of every
@@ -1823,24 +1867,46 @@ int xlbb_version(void) { return 100; }
 
 const char* xlbb_last_error(void) { return g_last_error.c_str(); }
 
-// Exactly the CTAs (= FP64 partials) of the next sweep launch of this dtype:
-// the reductions read exactly that many partials.
+// Upper bound on the FP64 partials of a sweep of this dtype on g under the
+// current launch config (the larger of its collide-and-push and row-marching
+// shapes): enough to size a partials buffer for any sweep.
 int xlbb_elast_sweep_ctas(int dtype, const XlbbGrid* g) {
     if (!grid_ok(g) || (dtype != XLBB_F32 && dtype != XLBB_F64 && dtype != XLBB_F32_ACC64))
         return fail(XLBB_EBADARG, "xlbb_elast_sweep_ctas: bad argument");
     const XlbbSweepConfig c = effective_cfg(0, dtype);
-    if (c.pipeline == 3) return ((g->nx + c.tx - 1) / c.tx) * g->ny;   // one partial per push block
-    const dim3 a = sweep_grid(g, c);
-    return (int)(a.x * a.y);
+    const bool f32 = dtype == XLBB_F32;
+    const long long n = std::max(launch_ctas(g, resolve_shape(c, true, f32)), launch_ctas(g, resolve_shape(c, false, f32)));
+    return n > INT_MAX ? fail(XLBB_EBADARG, "xlbb_elast_sweep_ctas: grid too large") : (int)n;
 }
 
 int xlbb_darcy_sweep_ctas(int dtype, const XlbbGrid* g) {
     if (!grid_ok(g) || (dtype != XLBB_F32 && dtype != XLBB_F64))
         return fail(XLBB_EBADARG, "xlbb_darcy_sweep_ctas: bad argument");
     const XlbbSweepConfig c = effective_cfg(1, dtype);
-    if (c.pipeline == 3) return ((g->nx + c.tx - 1) / c.tx) * g->ny;   // one partial per push block
-    const dim3 a = sweep_grid(g, c);
-    return (int)(a.x * a.y);
+    const bool f32 = dtype == XLBB_F32;
+    const long long n = std::max(launch_ctas(g, resolve_shape(c, true, f32)), launch_ctas(g, resolve_shape(c, false, f32)));
+    return n > INT_MAX ? fail(XLBB_EBADARG, "xlbb_darcy_sweep_ctas: grid too large") : (int)n;
+}
+
+// Exactly the FP64 partials that a sweep with these arguments writes with a
+// fused sum: the count to hand to xlbb_reduce_sum.
+int xlbb_darcy_sweep_partials(int dtype, const XlbbGrid* g, const XlbbDarcySweep* s) {
+    if (!grid_ok(g) || !s) return fail(XLBB_EBADARG, "xlbb_darcy_sweep_partials: bad argument");
+    long long n;
+    if (dtype == XLBB_F32) n = darcy_partials_t<float>(g, s);
+    else if (dtype == XLBB_F64) n = darcy_partials_t<double>(g, s);
+    else return fail(XLBB_EBADARG, "xlbb_darcy_sweep_partials: dtype");
+    return n > INT_MAX ? fail(XLBB_EBADARG, "xlbb_darcy_sweep_partials: grid too large") : (int)n;
+}
+
+int xlbb_elast_sweep_partials(int dtype, const XlbbGrid* g, const XlbbElastMaterial* mat, const XlbbElastSweep* s) {
+    if (!grid_ok(g) || !mat || !s) return fail(XLBB_EBADARG, "xlbb_elast_sweep_partials: bad argument");
+    long long n;
+    if (dtype == XLBB_F32) n = elast_partials_t<float, float>(g, mat, s, dtype);
+    else if (dtype == XLBB_F64) n = elast_partials_t<double, double>(g, mat, s, dtype);
+    else if (dtype == XLBB_F32_ACC64) n = elast_partials_t<double, float>(g, mat, s, dtype);
+    else return fail(XLBB_EBADARG, "xlbb_elast_sweep_partials: dtype");
+    return n > INT_MAX ? fail(XLBB_EBADARG, "xlbb_elast_sweep_partials: grid too large") : (int)n;
 }
 
 int xlbb_sweep_set_config(int kernel, const XlbbSweepConfig* cfg) {
@@ -1890,11 +1956,16 @@ int xlbb_elast_sweep_pipeline(int dtype, const XlbbGrid* g, const XlbbElastMater
         if (ok) return 4;
     }
     const XlbbSweepConfig c = effective_cfg(0, dtype);
-    if (c.pipeline == 3) {
-        const bool push = s->div_out == nullptr && (s->ps.count <= 0 || s->ps.row_ptr == nullptr || s->ps.push != nullptr);
-        return push ? 3 : 0;
-    }
-    return dtype == XLBB_F32_ACC64 && (c.pipeline == 1 || c.pipeline == 2) ? 0 : c.pipeline;
+    const bool push = push_eligible<ElastPhys<double, false>>(elast_args<double, false>(g, mat, s));
+    return resolve_shape(c, push, dtype == XLBB_F32).pipeline;
+}
+
+int xlbb_darcy_sweep_pipeline(int dtype, const XlbbGrid* g, const XlbbDarcySweep* s) {
+    if (!grid_ok(g) || !s || (dtype != XLBB_F32 && dtype != XLBB_F64))
+        return fail(XLBB_EBADARG, "xlbb_darcy_sweep_pipeline: bad argument");
+    const XlbbSweepConfig c = effective_cfg(1, dtype);
+    const bool push = push_eligible<DarcyPhys<double>>(darcy_args<DarcyPhys<double>>(g, s));
+    return resolve_shape(c, push, dtype == XLBB_F32).pipeline;
 }
 
 int xlbb_darcy_sweep(int dtype, const XlbbGrid* g, const XlbbDarcySweep* s, void* stream) {
@@ -2110,16 +2181,21 @@ extern "C" {
 int xlbb_darcy_sweep_residual_noalloc(int dtype, const XlbbGrid* g, const XlbbDarcySweep* s, double* sumsq_out,
                                       void* stream) {
     if (!grid_ok(g) || !s || !sumsq_out) return fail(XLBB_EBADARG, "xlbb_darcy_sweep_residual_noalloc: bad argument");
-    const int n = xlbb_darcy_sweep_ctas(dtype, g);
+    // the partials of the launch this sweep actually takes (push or row-marching shape)
+    const int n = xlbb_darcy_sweep_partials(dtype, g, s);
     if (n < 0) return n;
-    if (n > XLBB_NOALLOC_MAX_PARTIALS)
-        return fail(XLBB_EBADARG, "xlbb_darcy_sweep_residual_noalloc: the launch shape needs more CTA partials than "
-                                  "the 16384 of the built-in scratch (lower ctas_per_sm)");
+    if (n > XLBB_NOALLOC_MAX_PARTIALS) {
+        g_last_error = "xlbb_darcy_sweep_residual_noalloc: this sweep's launch has " + std::to_string(n) +
+                       " CTAs, more than the " + std::to_string(XLBB_NOALLOC_MAX_PARTIALS) +
+                       " partials of the built-in scratch (the collide-and-push shape has ceil(nx/tx)*ny CTAs; "
+                       "a row-marching shape, xlbb_sweep_set_config pipeline 0-2, has about ctas_per_sm per SM)";
+        return XLBB_EBADARG;
+    }
     double* scratch = nullptr;
     const int rc = noalloc_scratch(&scratch);
     if (rc != XLBB_OK) return rc;
     XlbbDarcySweep local = *s;
-    local.sumsq = scratch;      // every used slot is written by its CTA before the reduction reads it
+    local.sumsq = scratch;      // the launch's n CTAs write slots 0..n-1 before the reduction reads them
     const int st = xlbb_darcy_sweep(dtype, g, &local, stream);
     if (st != XLBB_OK) return st;
     return xlbb_reduce_sum(scratch, n, sumsq_out, stream);

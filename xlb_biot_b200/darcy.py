@@ -131,17 +131,33 @@ class AdvectionDiffusionReactionBGK(LBMBase):
         L = self._layout
         out = L.empty(9) if out is None else out
         if sumsq:
-            # one FP64 partial per CTA of the current launch shape
-            self._n_partials = _lib.check(_lib.lib().xlbb_darcy_sweep_ctas(self._dcode, L.grid()), "xlbb_darcy_sweep_ctas")
-            if self._partials.numel() < self._n_partials:
-                self._partials = torch.empty(self._n_partials, dtype=torch.float64, device=L.device)
-        s = _lib.DarcySweep(f.data_ptr(), out.data_ptr(), float(self.omega),
-                            self.omega_field.data_ptr() if self.omega_field is not None else None,
-                            self.source.data_ptr() if self.source is not None else None,
-                            external_source.data_ptr() if external_source is not None else None,
-                            self._pc.struct(), self._ps.struct(), self._partials.data_ptr() if sumsq else None)
+            # a buffer for the largest launch shape; the reduction reads the
+            # partials of the launch this sweep takes
+            n_max = _lib.check(_lib.lib().xlbb_darcy_sweep_ctas(self._dcode, L.grid()), "xlbb_darcy_sweep_ctas")
+            if self._partials.numel() < n_max:
+                self._partials = torch.empty(n_max, dtype=torch.float64, device=L.device)
+        s = self._sweep_args(f, out, external_source, sumsq)
+        if sumsq:
+            self._n_partials = _lib.check(_lib.lib().xlbb_darcy_sweep_partials(self._dcode, L.grid(), s),
+                                          "xlbb_darcy_sweep_partials")
         _lib.check(_lib.lib().xlbb_darcy_sweep(self._dcode, L.grid(), s, _lib.stream_ptr()), "xlbb_darcy_sweep")
         return out
+
+    def _sweep_args(self, f, out, external_source=None, sumsq=False):
+        return _lib.DarcySweep(f.data_ptr(), out.data_ptr(), float(self.omega),
+                               self.omega_field.data_ptr() if self.omega_field is not None else None,
+                               self.source.data_ptr() if self.source is not None else None,
+                               external_source.data_ptr() if external_source is not None else None,
+                               self._pc.struct(), self._ps.struct(), self._partials.data_ptr() if sumsq else None)
+
+    def sweep_pipeline(self, f=None, out=None):
+        """The launch pipeline a sweep of this solver runs now (3: collide and
+        push; 0-2: row-marching kernels), as the library resolves it."""
+        L = self._layout
+        f = L.empty(9) if f is None else f
+        out = L.empty(9) if out is None else out
+        return _lib.check(_lib.lib().xlbb_darcy_sweep_pipeline(self._dcode, L.grid(), self._sweep_args(f, out)),
+                          "xlbb_darcy_sweep_pipeline")
 
     def step(self, f_poststreaming, timestep, return_fpost=False, external_source=None):
         """``src/darcy.py:131-171``: one fused sweep."""

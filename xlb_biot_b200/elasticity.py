@@ -572,10 +572,11 @@ class LBMElasticity:
             fext = L.field(fext, 2)      # e.g. a coupling force computed in another precision
         code = _lib.XLBB_F32_ACC64 if acc64 else _lib.dtype_code(L.dtype)
         if sumsq:
-            # one FP64 partial per CTA of the current launch shape
-            self._n_partials = _lib.check(_lib.lib().xlbb_elast_sweep_ctas(code, L.grid()), "xlbb_elast_sweep_ctas")
-            if self._partials.numel() < self._n_partials:
-                self._partials = torch.empty(self._n_partials, dtype=torch.float64, device=L.device)
+            # a buffer for the largest launch shape; the reduction reads the
+            # partials of the launch this sweep takes
+            n_max = _lib.check(_lib.lib().xlbb_elast_sweep_ctas(code, L.grid()), "xlbb_elast_sweep_ctas")
+            if self._partials.numel() < n_max:
+                self._partials = torch.empty(n_max, dtype=torch.float64, device=L.device)
         pc, ps = self._rules_acc64 if acc64 else self._rules[level]
         bx0, bx1, by0, by1 = self._box(level)
         s = _lib.ElastSweep(f.data_ptr(), out.data_ptr(), self.force.data_ptr() if self.force is not None else None,
@@ -587,6 +588,9 @@ class LBMElasticity:
         if query:
             return _lib.check(_lib.lib().xlbb_elast_sweep_pipeline(code, L.grid(), self._mats[level], s),
                               "xlbb_elast_sweep_pipeline")
+        if sumsq:
+            self._n_partials = _lib.check(_lib.lib().xlbb_elast_sweep_partials(code, L.grid(), self._mats[level], s),
+                                          "xlbb_elast_sweep_partials")
         _lib.check(_lib.lib().xlbb_elast_sweep(code, L.grid(), self._mats[level], s, _lib.stream_ptr()),
                    "xlbb_elast_sweep")
         return out

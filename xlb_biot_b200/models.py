@@ -64,12 +64,14 @@ class _FluidSim(LBMBase):
         L = self._layout
         out = L.empty(9) if out is None else out
         if sumsq:
-            self._n_partials = _lib.check(_lib.lib().xlbb_darcy_sweep_ctas(self._dcode, L.grid()),
-                                          "xlbb_darcy_sweep_ctas")
-            if self._partials.numel() < self._n_partials:
-                self._partials = torch.empty(self._n_partials, dtype=torch.float64, device=L.device)
+            n_max = _lib.check(_lib.lib().xlbb_darcy_sweep_ctas(self._dcode, L.grid()), "xlbb_darcy_sweep_ctas")
+            if self._partials.numel() < n_max:
+                self._partials = torch.empty(n_max, dtype=torch.float64, device=L.device)
         s = _lib.DarcySweep(f.data_ptr(), out.data_ptr(), float(self.omega), None, None, None,
                             self._pc.struct(), self._ps.struct(), self._partials.data_ptr() if sumsq else None)
+        if sumsq:
+            self._n_partials = _lib.check(_lib.lib().xlbb_darcy_sweep_partials(self._dcode, L.grid(), s),
+                                          "xlbb_darcy_sweep_partials")
         _lib.check(_lib.lib().xlbb_fluid_sweep(self._dcode, L.grid(), s, self._model, _lib.stream_ptr()),
                    "xlbb_fluid_sweep")
         return out
