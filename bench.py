@@ -700,6 +700,122 @@ def run_mlups2d(args):
     return 0
 
 
+def run_c2solve(args):
+    """The Darcy configuration as stated: 1024^2, log-normal k, run to steady
+    state at a relative residual ||f^{n+1} - f^n|| / ||f^1 - f^0|| < 1e-8
+    (FP64 norms reduced on the device every ``check`` sweeps; the sweeps of one
+    check interval are one CUDA-graph replay).  Three runs from the same start:
+    all FP64; FP32 populations until the residual stops falling (the FP32
+    rounding floor); FP32 until that floor, then FP64 to 1e-8 of the FP32
+    run's first residual.  Reports sweeps and time to solution and the relative
+    L2 pressure error of each run against the FP64 run."""
+    import torch
+    import xlb_biot_b200.api as G
+    from xlb_biot_b200 import autotune
+    from xlb_biot_b200.workloads import darcy_lognormal
+    autotune.set_config(autotune.DARCY, 128, 1, 1, 8, 3)
+    check, tol = 2000, 1e-8
+    out = {}
+
+    def run(prec, f=None, r0=None, max_sweeps=10 ** 8):
+        solver, _ = darcy_lognormal(G, n=N, precision=prec)
+        solver.solve(solver.assign_fields_sharded(), tol=1.0, check_every=check)     # capture + warm-up
+        clocks = ClockSampler(torch.cuda.current_device())
+        clocks.start()
+        (fs, sweeps, rel), t = _timed(lambda: solver.solve(f, tol=tol, check_every=check, r0=r0,
+                                                           max_sweeps=max_sweeps))
+        clk = clocks.stop()
+        p = solver.update_macroscopic(fs).double()
+        return solver, fs, p, {"sweeps": int(sweeps), "seconds": t, "relative_residual": rel,
+                               "stalled": bool(solver.stalled), "glups": N * N * sweeps / t / 1e9, "clocks": clk}
+    _, _, p64, out["f64"] = run("f64/f64")
+    s32, f32, p32, out["f32"] = run("f32/f32")
+    # the FP32 run's reference norm: its own first sweep from the same start
+    loop = s32._sweep_loop(check, None)
+    r0 = loop.first(s32.assign_fields_sharded())
+    _, _, ph, hyb = run("f64/f64", f=f32.double(), r0=r0)
+    hyb["sweeps_f32"] = out["f32"]["sweeps"]
+    hyb["sweeps_f64"] = hyb.pop("sweeps")
+    hyb["seconds"] += out["f32"]["seconds"]
+    out["f32_then_f64"] = hyb
+
+    def err(p):
+        return float(torch.linalg.vector_norm(p - p64) / torch.linalg.vector_norm(p64))
+    out["f32"]["pressure_rel_err_vs_f64"] = err(p32)
+    out["f32_then_f64"]["pressure_rel_err_vs_f64"] = err(ph)
+    print(json.dumps({"workload": "c2_darcy_1024x1024_lognormal_steady_state", "metric": "time_to_solution",
+                      "unit": "s", "higher_is_better": False, "value": out["f32_then_f64"]["seconds"],
+                      "tolerance": tol, "check_every": check, "runs": out, "data": "synthetic"}), flush=True)
+    return 0
+
+
+def run_darcy_hbm(args):
+    """The headline Darcy sweep measured out of L2: (a) 4096^2 cells (1.27 GB
+    of populations and omega, ten times L2), CUDA-graph replays of 20 sweeps;
+    (b) 1024^2 with a 256 MiB L2 flush before every single sweep (each sweep
+    timed alone with CUDA events).  Same kernel, launch shape and bytes per
+    lattice update (76 B) as the headline."""
+    import torch
+    import xlb_biot_b200.api as G
+    from xlb_biot_b200 import autotune
+    from xlb_biot_b200.workloads import darcy_lognormal
+    peak, peak_kind = measured_peak_hbm()
+    stream = torch.cuda.current_stream()
+    out = {}
+    shape = [int(v) for v in args.launch_shape.split(",")] if args.launch_shape else [128, 1, 1, 8, 3]
+    autotune.set_config(autotune.DARCY, *shape)
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    # (a) 4096^2 in the sweep graph
+    n = 4096
+    solver, _ = darcy_lognormal(G, n=n)
+    loop = solver.sweep_graph(20)
+    loop.state.copy_(solver.assign_fields_sharded())
+    for _ in range(3):
+        loop.replay()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(args.steps):
+        loop.replay()
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / (args.steps * 20)
+    gbs = n * n * BYTES_PER_LU_F32 / (ms * 1e-3) / 1e9
+    out["4096x4096_graph"] = {"us_per_sweep": ms * 1e3, "glups": n * n / (ms * 1e-3) / 1e9, "achieved_gbs": gbs,
+                              "frac": gbs / peak, "pipeline": solver.sweep_pipeline()}
+    del solver, loop
+    torch.cuda.empty_cache()
+    # (b) 1024^2, L2 flushed before every sweep
+    solver, _ = darcy_lognormal(G, n=N)
+    L = solver._layout
+    x, y = L.empty(9), L.empty(9)
+    x.copy_(solver.assign_fields_sharded())
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    reps = max(50, args.steps * 10)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+    for i in range(reps + 5):
+        flush.fill_(float(i))
+        if i >= 5:
+            ev[i - 5][0].record(stream)
+        solver._sweep(x, None, out=y)
+        if i >= 5:
+            ev[i - 5][1].record(stream)
+        x, y = y, x
+    torch.cuda.synchronize()
+    ts = sorted(e0.elapsed_time(e1) for e0, e1 in ev)
+    ms = float(np.median(ts))
+    gbs = N * N * BYTES_PER_LU_F32 / (ms * 1e-3) / 1e9
+    out["1024x1024_l2_flushed_each_sweep"] = {"us_per_sweep_median": ms * 1e3, "us_min": ts[0] * 1e3,
+                                              "achieved_gbs": gbs, "frac": gbs / peak,
+                                              "pipeline": solver.sweep_pipeline()}
+    clk = clocks.stop()
+    print(json.dumps({"workload": "darcy_sweep_out_of_l2", "metric": "GB/s", "unit": "GB/s",
+                      "value": out["4096x4096_graph"]["achieved_gbs"], "peak": peak, "peak_kind": peak_kind,
+                      "bytes_per_lu": BYTES_PER_LU_F32, "launch_shape": shape, "runs": out, "clocks": clk}),
+          flush=True)
+    return 0
+
+
 def run_c5(args):
     """Adjoint of heterogeneous Terzaghi-type consolidation: 512 x 256 cells
     (arrays 512 x 258 with the boundary rows), 200 Biot steps, each with 4
@@ -807,7 +923,8 @@ def main():
     ap.add_argument("--adjoint-steps", type=int, default=200)
     ap.add_argument("--fd-directions", type=int, default=32)
     ap.add_argument("--cavity-n", type=int, default=4096)
-    ap.add_argument("--workload", choices=["darcy", "c1", "c3", "c4", "c4sweep", "c4vcycle", "c5", "mlups2d"],
+    ap.add_argument("--workload", choices=["darcy", "c1", "c2solve", "c3", "c4", "c4sweep", "c4vcycle", "c5",
+                                           "mlups2d", "darcy_hbm"],
                     default="darcy",
                     help="darcy: the headline line; c1/c3/c4/c5: the other configurations (one JSON line each)")
     ap.add_argument("--biot-steps", type=int, default=100)
@@ -834,6 +951,10 @@ def main():
         return run_c4vcycle(args)
     if args.workload == "mlups2d":
         return run_mlups2d(args)
+    if args.workload == "c2solve":
+        return run_c2solve(args)
+    if args.workload == "darcy_hbm":
+        return run_darcy_hbm(args)
     return run_ours(args)
 
 

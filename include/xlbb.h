@@ -96,10 +96,18 @@ typedef struct {
 int xlbb_sweep_set_config(int kernel, const XlbbSweepConfig* cfg);
 int xlbb_sweep_get_config(int kernel, XlbbSweepConfig* cfg);
 
-/* Device status word of the kernels' bounded waits (0, or XLBB_ETIMEOUT if a
- * wait gave up; XLBB_EBADARG if xlbb_batched_elast_sweep4 skipped an instance
- * that does not qualify); synchronous; reset != 0 clears it. */
+/* Device status word: 0, or the first error a kernel recorded since the last
+ * reset -- XLBB_ETIMEOUT if a bounded wait gave up, XLBB_ENONFINITE if
+ * xlbb_reduce_sum produced NaN or Inf (a diverged or corrupted field),
+ * XLBB_EBADARG if xlbb_batched_elast_sweep4 skipped an instance that does not
+ * qualify.  Synchronous; reset != 0 clears it. */
 int xlbb_device_status(int* status, int reset);
+/* Self-test of the bounded waits (no counterpart in the reference): one
+ * kernel waits on an mbarrier that nothing completes, with a limit of `polls`
+ * (1 .. 2^22), gives up, records XLBB_ETIMEOUT in the status word, writes 1
+ * to the device int *gave_up and returns.  No copy is in flight, so nothing
+ * hangs; the context stays usable. */
+int xlbb_wait_selftest(unsigned polls, int* gave_up, void* stream);
 
 typedef struct {
     double lam, mu;          /* uniform Lame parameters (lattice units)       */

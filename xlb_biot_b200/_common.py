@@ -3,6 +3,7 @@ host copies for the ``output_data`` hooks."""
 import numpy as np
 import torch
 
+from . import _lib
 from .boundary_conditions import PrecisionPolicy
 
 _PRECISIONS = {
@@ -54,3 +55,39 @@ def gathered(x):
     """``process_allgather`` of one process: a leading axis of length 1."""
     h = host(x)
     return None if h is None else h[None]
+
+
+def require_finite(value, what, iteration):
+    """Raise ``NonFiniteError`` (XLBB_ENONFINITE) when a convergence measure
+    (scalar or per-instance array) holds NaN or Inf."""
+    v = np.asarray(value, dtype=np.float64)
+    if not np.all(np.isfinite(v)):
+        where = "" if v.ndim == 0 else f" (instances {np.flatnonzero(~np.isfinite(v))[:8].tolist()})"
+        raise _lib.NonFiniteError(f"XLBB_ENONFINITE: {what} is not finite after {iteration} iterations{where}: "
+                                  "the iteration diverged or a field holds NaN/Inf")
+
+
+def iterate_to_tolerance(advance, tol, max_iters, stall_checks=None, what="relative residual"):
+    """Host driver of the pseudo-time and V-cycle loops.  ``advance()`` runs the
+    next batch of iterations on the device and returns ``(iterations run,
+    relative residual)``.  Stops when the residual is below ``tol``, when
+    ``max_iters`` iterations have run, or -- with ``stall_checks`` -- when the
+    residual has not fallen by 1 % for that many checks (the rounding floor of
+    the storage precision).  A NaN or Inf residual raises ``NonFiniteError``
+    at once.  Returns ``(iterations, relative residual, stalled)``."""
+    it, rel = 0, 1.0
+    best, since_best = np.inf, 0
+    while it < max_iters:
+        n, rel = advance()
+        it += n
+        require_finite(rel, what, it)
+        if rel < tol:
+            return it, rel, False
+        if stall_checks:
+            if rel < 0.99 * best:
+                best, since_best = rel, 0
+            else:
+                since_best += 1
+                if since_best >= stall_checks:
+                    return it, rel, True
+    return it, rel, False

@@ -22,6 +22,15 @@ ERRORS = {-1: "XLBB_EBADARG", -2: "XLBB_ELAUNCH", -3: "XLBB_ETIMEOUT", -4: "XLBB
 class XlbbError(RuntimeError):
     """A negative status returned by the C ABI."""
 
+    code = None
+
+
+class NonFiniteError(XlbbError):
+    """XLBB_ENONFINITE: a convergence norm became NaN or Inf (the iteration
+    diverged, or a field or parameter holds non-finite values)."""
+
+    code = XLBB_ENONFINITE
+
 
 class Grid(ctypes.Structure):
     _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("pitch", ctypes.c_int), ("plane", ctypes.c_longlong)]
@@ -108,6 +117,7 @@ SIGNATURES = {
     "xlbb_restrict": (I, [I, I, PG, PG, I, I, I, I, I, P, P, P]),
     "xlbb_prolong_add": (I, [I, I, PG, PG, I, I, I, I, I, P, P, P]),
     "xlbb_reduce_sum": (I, [P, I, P, P]),
+    "xlbb_wait_selftest": (I, [ctypes.c_uint, P, P]),
     "xlbb_sumsq": (I, [I, PG, I, P, I, I, I, I, P, P]),
     "xlbb_sumsq_ctas": (I, [PG]),
     "xlbb_axpby": (I, [I, ctypes.c_longlong, D, P, D, P, P, P]),
@@ -162,7 +172,10 @@ def require_cuda():
 def check(status, what):
     if status < 0:
         msg = lib().xlbb_last_error().decode()
-        raise XlbbError(f"{what} failed with {ERRORS.get(status, status)}: {msg}")
+        cls = NonFiniteError if status == XLBB_ENONFINITE else XlbbError
+        err = cls(f"{what} failed with {ERRORS.get(status, status)}: {msg}")
+        err.code = status
+        raise err
     return status
 
 

@@ -27,6 +27,7 @@ import numpy as np
 import torch
 
 from . import _lib
+from ._common import require_finite
 from .fields import pitch_for
 
 _ALIGN = 64   # elements; keeps every instance's planes 256-byte aligned
@@ -341,11 +342,13 @@ class BatchedElasticity:
         cycles = 1
         if criterion == "residual":
             r0 = torch.sqrt(self.norm2).cpu().numpy()
+            require_finite(r0, "level-0 residual norm of the first V-cycle", cycles)
             rel = np.ones(self.n)
             while cycles < max_cycles:
                 self.vcycle()
                 cycles += 1
                 rel = torch.sqrt(self.norm2).cpu().numpy() / np.where(r0 > 0, r0, 1.0)
+                require_finite(rel, "relative V-cycle residual", cycles)
                 self.converged_at[(self.converged_at < 0) & (rel < tol)] = cycles
                 if np.all(rel < tol):
                     break
@@ -359,12 +362,14 @@ class BatchedElasticity:
             out[self._corr_ids] = np.sqrt(c[:, 0] / np.where(c[:, 1] > 0, c[:, 1], 1.0))
             return out
         prev = corr()
+        require_finite(prev, "relative coarse-grid correction", cycles)
         est = np.full(self.n, np.inf)
         flat = np.zeros(self.n, dtype=int)
         while cycles < max_cycles:
             self.vcycle()
             cycles += 1
             c = corr()
+            require_finite(c, "relative coarse-grid correction", cycles)
             ratio = c / np.where(prev > 0, prev, 1.0)
             rho = np.minimum(ratio, 0.95)
             est = c * rho / (1.0 - rho)

@@ -987,7 +987,22 @@ __global__ void reduce_sum_kernel(const double* p, int n, double* out) {
     double acc = 0.0;
     for (int i = threadIdx.x; i < n; i += blockDim.x) acc += p[i];
     const double s = block_sum(acc, red);
-    if (threadIdx.x == 0) *out = s;
+    if (threadIdx.x == 0) {
+        *out = s;
+        if (!isfinite(s)) note_status(XLBB_ENONFINITE);
+    }
+}
+
+// Self-test of the bounded mbarrier wait: one thread waits on a barrier that
+// nothing arrives at, with a limit of `polls`; the wait gives up, records
+// XLBB_ETIMEOUT and the kernel returns (no copy is in flight, nothing hangs).
+__global__ void wait_selftest_kernel(uint32_t polls, int* gave_up) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        *gave_up = mbar_wait(&bar, 0, polls) ? 0 : 1;
+    }
 }
 
 template <typename T>
@@ -1193,7 +1208,7 @@ __device__ __forceinline__ void fill_tile_rec(TileRec<T, S>* d, const BatchInst<
     d->cd = I.cd;
     d->h = I.h;
     d->n = I.n;
-    if (!ok) atomicExch(&g_xlbb_status, XLBB_EBADARG);
+    if (!ok) note_status(XLBB_EBADARG);
 }
 
 __device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
@@ -2199,6 +2214,12 @@ int xlbb_darcy_sweep_residual_noalloc(int dtype, const XlbbGrid* g, const XlbbDa
     const int st = xlbb_darcy_sweep(dtype, g, &local, stream);
     if (st != XLBB_OK) return st;
     return xlbb_reduce_sum(scratch, n, sumsq_out, stream);
+}
+
+int xlbb_wait_selftest(unsigned polls, int* gave_up, void* stream) {
+    if (!gave_up || polls == 0 || polls > (1u << 22)) return fail(XLBB_EBADARG, "xlbb_wait_selftest: bad argument");
+    wait_selftest_kernel<<<1, 32, 0, XLBB_STREAM(stream)>>>(polls, gave_up);
+    return check_launch("xlbb_wait_selftest");
 }
 
 int xlbb_reduce_sum(const double* partials, int n, double* out, void* stream) {

@@ -189,11 +189,16 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
                  : "memory");
 }
 
-// Bounded wait on an mbarrier phase: gives up after ~2^22 polls (seconds),
-// records XLBB_ETIMEOUT in g_xlbb_status and lets the kernel run to its end.
-__device__ __forceinline__ void mbar_wait(uint64_t* bar, uint32_t parity) {
+// Records a device error in g_xlbb_status unless an earlier one is there
+// (the first error of a run is the one reported).
+__device__ __forceinline__ void note_status(int code) { atomicCAS(&g_xlbb_status, 0, code); }
+
+// Bounded wait on an mbarrier phase: gives up after `limit` polls (by default
+// ~2^22, seconds), records XLBB_ETIMEOUT in g_xlbb_status and returns false;
+// the caller runs on to its end.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t limit = 1u << 22) {
     const uint32_t a = smem_u32(bar);
-    for (uint32_t it = 0; it < (1u << 22); ++it) {
+    for (uint32_t it = 0; it < limit; ++it) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -202,9 +207,10 @@ __device__ __forceinline__ void mbar_wait(uint64_t* bar, uint32_t parity) {
             : "=r"(done)
             : "r"(a), "r"(parity)
             : "memory");
-        if (done) return;
+        if (done) return true;
     }
-    atomicExch(&g_xlbb_status, -3);
+    note_status(-3);
+    return false;
 }
 
 // 1D bulk copy global -> shared completing on an mbarrier (no multicast).

@@ -16,7 +16,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._common import gathered
+from ._common import gathered, iterate_to_tolerance, require_finite
 from .base import LBMBase
 from .bc_compile import compile_rules
 from .boundary_conditions import BoundaryCondition, BounceBackHalfway, _at_add, _at_set, _take
@@ -175,6 +175,43 @@ class AdvectionDiffusionReactionBGK(LBMBase):
         sum((f_new - f_old)^2).  Returns a ``SweepLoop``."""
         return SweepLoop(self, n_sweeps, external_source)
 
+    def solve(self, f=None, tol=1e-8, check_every=1000, max_sweeps=10 ** 8, external_source=None,
+              stall_checks=20, r0=None):
+        """Pseudo-time iteration of the Darcy step (``src/darcy.py:131-171``) to
+        steady state: until the relative residual ``||f^{n+1} - f^n|| /
+        ||f^1 - f^0||`` (FP64 norms, reduced on the device) is below ``tol``.
+        Sweeps run as one CUDA-graph replay of ``check_every`` sweeps between
+        host checks; a residual that stops falling for ``stall_checks`` checks
+        (the rounding floor of the storage precision) ends the loop with
+        ``self.stalled = True``; a NaN or Inf residual raises
+        ``NonFiniteError``.  ``r0``: the reference norm of the relative
+        residual when continuing an earlier solve (default: this solve's
+        first sweep).  Returns ``(f, sweeps, relative_residual)``."""
+        L = self._layout
+        f = self.assign_fields_sharded() if f is None else L.field(f, 9)
+        loop = self._sweep_loop(check_every, external_source)
+        first = loop.first(f)
+        require_finite(first, "first sweep's residual norm", 1)
+        r0 = first if r0 is None else float(r0)
+
+        def replay():
+            loop.replay()
+            return loop.n, ((float(loop.sumsq[0]) ** 0.5) / r0 if r0 > 0 else 0.0)
+        it, rel, self.stalled = iterate_to_tolerance(replay, tol, max_sweeps - 1, stall_checks)
+        return loop.result, it + 1, rel
+
+    def _sweep_loop(self, n, external_source):
+        """The ``SweepLoop`` of ``n`` sweeps (rounded up to even, so that its
+        result lands in its input buffer); without an external source it is
+        captured once per solver and reused."""
+        n = int(n) + (int(n) % 2)
+        if external_source is not None:
+            return SweepLoop(self, n, external_source)
+        cache = self.__dict__.setdefault("_loops", {})
+        if n not in cache:
+            cache[n] = SweepLoop(self, n)
+        return cache[n]
+
     def residual_sumsq(self, out_scalar):
         """FP64 sum of (f_new - f_old)^2 of the last sweep run with ``sumsq=True``
         (deterministic two-pass reduction), written into a device scalar."""
@@ -317,6 +354,12 @@ class SweepLoop:
             self.solver._sweep(a, self.ext, out=b, sumsq=(k == self.n - 1))
             a, b = b, a
         self.solver.residual_sumsq(self.sumsq)
+
+    def first(self, f0):
+        """One sweep from ``f0`` into ``state``; returns ||f^1 - f^0|| (FP64)."""
+        self.solver._sweep(self.solver._layout.field(f0, 9), self.ext, out=self.state, sumsq=True)
+        self.solver.residual_sumsq(self.sumsq)
+        return float(self.sumsq[0]) ** 0.5
 
     def replay(self):
         self.graph.replay()

@@ -15,7 +15,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._common import make_policy, print_parameters, set_precisions, gathered
+from ._common import gathered, iterate_to_tolerance, make_policy, print_parameters, require_finite, set_precisions
 from .bc_compile import apply_rules_device, compile_rules
 from .boundary_conditions import (BoundaryCondition, _at_add, _at_set, _take, grid_mask, solid_halo_voxels)
 from .fields import Layout, torch_dtype
@@ -608,37 +608,28 @@ class LBMElasticity:
         Multigrid: V-cycles until the level-0 residual norm drops by ``tol``.
         Returns ``(f, iterations, relative_residual)``."""
         f = self.assign_fields_sharded() if f is None else self._f(f)
+        self.stalled = False
         if self.levels > 1:
             f, r0 = self.step(f, 0, external_force=external_force)
             r0 = float(r0)
-            it, rel = 1, 1.0
-            while it < max_sweeps:
-                f, r = self.step(f, it, external_force=external_force)
-                it += 1
-                rel = float(r) / r0 if r0 > 0 else 0.0
-                if rel < tol:
-                    break
-            return f, it, rel
+            require_finite(r0, "level-0 residual norm of the first V-cycle", 1)
+            state = {"f": f, "it": 1}
+
+            def vcycle():
+                state["f"], r = self.step(state["f"], state["it"], external_force=external_force)
+                state["it"] += 1
+                return 1, (float(r) / r0 if r0 > 0 else 0.0)
+            it, rel, _ = iterate_to_tolerance(vcycle, tol, max_sweeps - 1, what="relative V-cycle residual")
+            return state["f"], it + 1, rel
         loop = self._elastic_loop(check_every, external_force)
         r0 = loop.first(f)
-        it, rel = 1, 1.0
-        best, since_best = np.inf, 0
-        self.stalled = False
-        while it < max_sweeps:
+        require_finite(r0, "first sweep's residual norm", 1)
+
+        def replay():
             loop.replay()
-            it += loop.n
-            rel = (float(loop.sumsq[0]) ** 0.5) / r0 if r0 > 0 else 0.0
-            if rel < tol or not np.isfinite(rel):
-                break
-            # stop when the residual no longer falls (rounding floor of the precision)
-            if rel < 0.99 * best:
-                best, since_best = rel, 0
-            else:
-                since_best += 1
-                if since_best >= stall_checks:
-                    self.stalled = True
-                    break
-        return loop.result, it, rel
+            return loop.n, ((float(loop.sumsq[0]) ** 0.5) / r0 if r0 > 0 else 0.0)
+        it, rel, self.stalled = iterate_to_tolerance(replay, tol, max_sweeps - 1, stall_checks)
+        return loop.result, it + 1, rel
 
     def _elastic_loop(self, n, external_force):
         """The ``ElasticLoop`` of ``n`` sweeps, captured once per solver and
