@@ -1,0 +1,1 @@
+"""Plotting is not used by the fixtures."""
