@@ -141,6 +141,10 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
+TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch, cold caches, read from "
+                  "profiles/darcy_sweep_1024x1024_lognormal.md (not measured in this run)")
+
+
 def ncu_traffic_per_launch():
     """DRAM bytes per launch of the Darcy sweep from the committed ncu summary."""
     path = os.path.join(ROOT, "profiles", "darcy_sweep_1024x1024_lognormal.md")
@@ -336,6 +340,8 @@ def run_ours(args):
     torch.cuda.synchronize()
     per_sweep_ms = kev[0].elapsed_time(kev[1]) / (reps * SWEEPS_PER_STEP)
 
+    pipeline = solver.sweep_pipeline()          # the launch the library resolved for this sweep
+    out_of_l2 = None if args.no_out_of_l2 else darcy_out_of_l2(measured_peak_hbm()[0])
     dev_ms, e2e_ms = replica_totals(dev_ms, e2e_ms, ws, "cuda")
     value = replica_glups(N * N * SWEEPS_PER_STEP * args.steps, ws, dev_ms)
     e2e = replica_glups(N * N * SWEEPS_PER_STEP * args.steps, ws, e2e_ms)
@@ -363,10 +369,10 @@ def run_ours(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "frac_of_spec": achieved / SPEC_HBM_GBS, "spec_gbs": SPEC_HBM_GBS,
-                         "traffic": traffic, "algorithmic_bytes_per_launch": N * N * BYTES_PER_LU_F32,
-                         "kernel": ("xlbb::push_kernel<DarcyPhys<float>>"
-                                    if tuned.get("pipeline") == 3 else "xlbb::sweep_kernel<DarcyPhys<float>>"),
-                         "kernel_ms": per_sweep_ms},
+                         "traffic": traffic, "traffic_source": TRAFFIC_SOURCE,
+                         "algorithmic_bytes_per_launch": N * N * BYTES_PER_LU_F32,
+                         "kernel": PIPELINE_KERNELS[pipeline], "kernel_ms": per_sweep_ms,
+                         "out_of_l2": out_of_l2},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": "GLUPS", "h2d_bytes_per_step": host_f.numel() * host_f.element_size(),
                     "d2h_bytes_per_step": 8},
@@ -749,24 +755,21 @@ def run_c2solve(args):
     return 0
 
 
-def run_darcy_hbm(args):
-    """The headline Darcy sweep measured out of L2: (a) 4096^2 cells (1.27 GB
-    of populations and omega, ten times L2), CUDA-graph replays of 20 sweeps;
-    (b) 1024^2 with a 256 MiB L2 flush before every single sweep (each sweep
-    timed alone with CUDA events).  Same kernel, launch shape and bytes per
-    lattice update (76 B) as the headline."""
+PIPELINE_KERNELS = {0: "xlbb::sweep_kernel<DarcyPhys<float>>", 1: "xlbb::sweep_bulk_kernel<DarcyPhys<float>>",
+                    2: "xlbb::sweep_warp_kernel<DarcyPhys<float>>", 3: "xlbb::push_kernel<DarcyPhys<float>>"}
+
+
+def darcy_out_of_l2(peak, replays=5):
+    """The headline Darcy sweep (same kernel, launch shape and 76 B per lattice
+    update) measured out of L2: (a) 4096^2 cells (1.27 GB of populations and
+    omega, ten times L2) in CUDA-graph replays of 20 sweeps; (b) 1024^2 with a
+    256 MiB L2 flush before every single sweep, each sweep timed alone with
+    CUDA events (median of 50)."""
     import torch
     import xlb_biot_b200.api as G
-    from xlb_biot_b200 import autotune
     from xlb_biot_b200.workloads import darcy_lognormal
-    peak, peak_kind = measured_peak_hbm()
     stream = torch.cuda.current_stream()
     out = {}
-    shape = [int(v) for v in args.launch_shape.split(",")] if args.launch_shape else [128, 1, 1, 8, 3]
-    autotune.set_config(autotune.DARCY, *shape)
-    clocks = ClockSampler(torch.cuda.current_device())
-    clocks.start()
-    # (a) 4096^2 in the sweep graph
     n = 4096
     solver, _ = darcy_lognormal(G, n=n)
     loop = solver.sweep_graph(20)
@@ -775,23 +778,22 @@ def run_darcy_hbm(args):
         loop.replay()
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     a.record(stream)
-    for _ in range(args.steps):
+    for _ in range(replays):
         loop.replay()
     b.record(stream)
     torch.cuda.synchronize()
-    ms = a.elapsed_time(b) / (args.steps * 20)
+    ms = a.elapsed_time(b) / (replays * 20)
     gbs = n * n * BYTES_PER_LU_F32 / (ms * 1e-3) / 1e9
     out["4096x4096_graph"] = {"us_per_sweep": ms * 1e3, "glups": n * n / (ms * 1e-3) / 1e9, "achieved_gbs": gbs,
-                              "frac": gbs / peak, "pipeline": solver.sweep_pipeline()}
+                              "frac": gbs / peak, "kernel": PIPELINE_KERNELS[solver.sweep_pipeline()]}
     del solver, loop
     torch.cuda.empty_cache()
-    # (b) 1024^2, L2 flushed before every sweep
     solver, _ = darcy_lognormal(G, n=N)
     L = solver._layout
     x, y = L.empty(9), L.empty(9)
     x.copy_(solver.assign_fields_sharded())
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
-    reps = max(50, args.steps * 10)
+    reps = 50
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
     for i in range(reps + 5):
         flush.fill_(float(i))
@@ -807,7 +809,22 @@ def run_darcy_hbm(args):
     gbs = N * N * BYTES_PER_LU_F32 / (ms * 1e-3) / 1e9
     out["1024x1024_l2_flushed_each_sweep"] = {"us_per_sweep_median": ms * 1e3, "us_min": ts[0] * 1e3,
                                               "achieved_gbs": gbs, "frac": gbs / peak,
-                                              "pipeline": solver.sweep_pipeline()}
+                                              "kernel": PIPELINE_KERNELS[solver.sweep_pipeline()]}
+    del solver, x, y, flush
+    torch.cuda.empty_cache()
+    return out
+
+
+def run_darcy_hbm(args):
+    """The out-of-L2 measurements of the headline sweep alone (one JSON line)."""
+    import torch
+    from xlb_biot_b200 import autotune
+    peak, peak_kind = measured_peak_hbm()
+    shape = [int(v) for v in args.launch_shape.split(",")] if args.launch_shape else [128, 1, 1, 8, 3]
+    autotune.set_config(autotune.DARCY, *shape)
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    out = darcy_out_of_l2(peak, replays=args.steps)
     clk = clocks.stop()
     print(json.dumps({"workload": "darcy_sweep_out_of_l2", "metric": "GB/s", "unit": "GB/s",
                       "value": out["4096x4096_graph"]["achieved_gbs"], "peak": peak, "peak_kind": peak_kind,
@@ -916,6 +933,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-out-of-l2", action="store_true",
+                    help="skip the out-of-L2 measurements of the headline sweep (4096^2; 1024^2 L2-flushed)")
     ap.add_argument("--launch-shape", default="",
                     help="tx,depth,ctas_per_sm,min_rows,pipeline of the Darcy sweep (skips the autotuner)")
     ap.add_argument("--elast-shape", default="",

@@ -8,13 +8,14 @@ follows.  It is used as the checker by ``tests/``, by ``__graft_entry__.smoke()`
 and by the ``cpu_baseline`` / ``--impl reference`` legs of ``bench.py``.  The
 product (``xlb_biot_b200``) never imports it.
 
-Parity status: the reference needs JAX, which is not installable offline, so no
-output of the reference itself could be produced.  The restatement is pinned by
-the reference's own verification data instead: the analytic and manufactured
-solutions of ``examples/elasticity/*.py``, ``examples/darcy/*.py`` and
-``examples/poroelasticity/periodic.py`` (error levels and convergence orders),
-see ``tests/test_oracle_pins.py``.  Bitwise-level parity with the JAX code is
-therefore "pinned by analytic fixtures", not by golden vectors of the reference.
+Parity status: pinned to the reference's own source.  JAX is not installable
+offline, so ``tests/golden/make_golden.py`` runs the unmodified reference
+modules under a NumPy stand-in for the JAX array API (``tests/golden/jaxshim``)
+and stores their FP64 outputs on seeded cases (``tests/golden/
+reference_fixtures.npz``); ``tests/test_golden_reference.py`` holds this
+restatement to them at 1e-12 (measured: <= 1e-14).  The analytic and
+manufactured solutions of the reference's examples pin it as well
+(``tests/test_oracle_pins.py``).
 
 JAX semantics reproduced explicitly (``oracle/jaxsem.py``):
   * ``x.at[idx].set(v)`` with duplicate indices: the last update wins (XLA CPU

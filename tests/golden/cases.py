@@ -191,6 +191,49 @@ def mg_transfers(m):
             "equilibrium": to_np(s.equilibrium(_in(m, eta), _in(m, sig), external_force=_in(m, ext)))}
 
 
+PARAMETER_KEYS = ("L_tot", "E", "nu", "c0", "alpha", "lambda", "mu", "force", "Kpm", "p0", "eta0", "etaInf",
+                  "kappa", "c_f", "T_tot")
+
+
+def parameters_terzaghi(m, alpha=0.8):
+    """``Parameters`` (``src/utils.py:17-76``) driven as the Terzaghi example
+    does (``examples/poroelasticity/Terzaghi.py:247-280``): SI units, derived
+    2-D Lame parameters, load, pressures and times, then the non-dimensional
+    units L_tot, eta0, T_tot, p0; every parameter's dimensional and
+    non-dimensional value, and the type checks of the setters."""
+    params = m.Parameters()
+    params.add_units(L=1.0, H=1.0, T=1.0, P=1.0)
+    params.add_parameters(L_tot=(1e0, {'L': 1}), E=(1.0, {'P': 1}), nu=(0.8, {}), c0=(1e0, {'P': -1}),
+                          alpha=(alpha, {}))
+    g = params.get
+    params.set_parameter('lambda', g('E') * g('nu') / (1 - g('nu') ** 2), {'P': 1})
+    params.set_parameter('mu', 0.5 * g('E') / (1 + g('nu')), {'P': 1})
+    params.add_parameters(
+        force=(g('alpha') / g('c0') + (g('lambda') + 2 * g('mu')) / g('alpha'), {'L': -1, 'H': 1, 'P': 1}),
+        Kpm=(g('lambda') + 2 * g('mu') + g('alpha') ** 2 / g('c0'), {'P': 1}))
+    params.add_parameters(
+        p0=(g('alpha') * g('force') / g('c0') / g('Kpm'), {'P': 1}),
+        eta0=(g('force') * g('L_tot') / g('Kpm'), {'H': 1}),
+        etaInf=(g('force') * g('L_tot') / (g('lambda') + 2 * g('mu')), {'H': 1}),
+        kappa=(g('Kpm') / (g('lambda') + 2 * g('mu')), {'L': 2, 'T': -1, 'P': -1}))
+    params.set_parameter('c_f', g('kappa') * (g('lambda') + 2 * g('mu')) / g('c0') / g('Kpm'), {'L': 2, 'T': -1})
+    params.set_parameter('T_tot', g('L_tot') ** 2 / g('c_f'), {'T': 1})
+    dimensional = [g(k) for k in PARAMETER_KEYS]
+    params.add_units(L=g('L_tot'), H=g('eta0'), T=g('T_tot'), P=g('p0'))
+    rejected = []
+    for bad in (lambda: params.set_unit('L', 1), lambda: params.set_unit('L', -1.0),
+                lambda: params.set_parameter('x', 1, {}), lambda: params.set_parameter('x', 1.0, {'Q': 1}),
+                lambda: params.set_parameter('x', 1.0, {'L': 1.0}), lambda: params.set_parameter('x', 1.0, [])):
+        try:
+            bad()
+            rejected.append(0.0)
+        except TypeError:
+            rejected.append(1.0)
+    return {"dimensional": np.array(dimensional),
+            "nondimensional": np.array([params.get_nondimensional(k) for k in PARAMETER_KEYS]),
+            "units": np.array([params.get_unit(k) for k in "LHTP"]), "rejected": np.array(rejected)}
+
+
 CASES = {
     "elast_plain_16x16": lambda m: elast_plain(m, 16, 16),
     "elast_plain_37x22": lambda m: elast_plain(m, 37, 22),
@@ -207,4 +250,5 @@ CASES = {
     "biot_periodic_l2": lambda m: biot_periodic(m, 2),
     "biot_terzaghi_l3": biot_terzaghi,
     "mg_transfers": mg_transfers,
+    "parameters_terzaghi": parameters_terzaghi,
 }

@@ -31,8 +31,10 @@ def load(name):
 
 def oracle_namespace():
     import oracle.api as O
+    from xlb_biot_b200.utils import Parameters     # host-only class of the product (no oracle copy)
     m = SimpleNamespace(**{k: getattr(O, k) for k in dir(O) if not k.startswith("_")})
     m.golden_set_omega = lambda solver, om: setattr(solver, "omega", om)
+    m.Parameters = Parameters
     return m
 
 

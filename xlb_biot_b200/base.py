@@ -226,14 +226,20 @@ class LBMBase:
         pass
 
     def save_checkpoint(self, timestep, f):
+        """The populations after ``timestep`` (the reference's orbax manager with
+        ``max_to_keep=1``, ``src/base.py:82-87``: older checkpoints are removed)."""
         os.makedirs(self.checkpointDir, exist_ok=True)
-        torch.save({"timestep": timestep, "f": f.detach().cpu()},
-                   os.path.join(self.checkpointDir, f"checkpoint_{timestep:08d}.pt"))
+        name = f"checkpoint_{timestep:08d}.pt"
+        torch.save({"timestep": timestep, "f": f.detach().cpu()}, os.path.join(self.checkpointDir, name + ".tmp"))
+        os.replace(os.path.join(self.checkpointDir, name + ".tmp"), os.path.join(self.checkpointDir, name))
+        for old in os.listdir(self.checkpointDir):
+            if old.startswith("checkpoint_") and old.endswith(".pt") and old != name:
+                os.remove(os.path.join(self.checkpointDir, old))
 
     def load_latest_checkpoint(self):
         if not os.path.isdir(self.checkpointDir):
             return None
-        names = sorted(n for n in os.listdir(self.checkpointDir) if n.startswith("checkpoint_"))
+        names = sorted(n for n in os.listdir(self.checkpointDir) if n.startswith("checkpoint_") and n.endswith(".pt"))
         if not names:
             return None
         return torch.load(os.path.join(self.checkpointDir, names[-1]))

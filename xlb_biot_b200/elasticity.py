@@ -557,6 +557,8 @@ class LBMElasticity:
 
     def _prolong(self, f):
         """``:878-894``: injection of the coarse interior to twice its size."""
+        if not isinstance(f, torch.Tensor):
+            f = torch.as_tensor(np.asarray(f), device=self._L(0).device)
         s = f[self._interior(f.shape)]
         return s.repeat_interleave(2, dim=0).repeat_interleave(2, dim=1)
 

@@ -70,6 +70,29 @@ class Parameters:
             print(f"{k:>20} | {unit: ^20} | {v}")
 
 
+def results_filename(output_dir, E, nu, K, alpha, nx, ne, levels, coupling, alternative_gradient=False):
+    """Result file of one run of the convergence sweeps, named as
+    ``examples/poroelasticity/periodic.py:217`` names it."""
+    return os.path.join(output_dir, f"error_E{E:.3f}_nu{nu:.3f}_K{K:.3f}_a{alpha:.3f}_nx{nx:03d}_ne{ne:03d}"
+                                    f"_l{levels:03d}_{coupling}{'_altgrad' if alternative_gradient else ''}.npz")
+
+
+def cached_results(filename, compute):
+    """``examples/poroelasticity/periodic.py:218-259``: the arrays of an earlier
+    run loaded from ``filename`` (``.npz``), or -- when the file is missing or
+    unreadable -- ``compute()`` (a dict of arrays) run and saved compressed.
+    Returns a dict of NumPy arrays either way."""
+    try:
+        with np.load(filename) as data:
+            return {k: data[k] for k in data.files}
+    except Exception:
+        pass
+    data = {k: np.asarray(v) for k, v in compute().items()}
+    os.makedirs(os.path.dirname(os.path.abspath(filename)), exist_ok=True)
+    np.savez_compressed(filename, **data)
+    return data
+
+
 def _keys_cubic(x, a=-0.5):
     x = np.abs(x)
     return np.where(x <= 1, ((a + 2) * x - (a + 3)) * x * x + 1,
