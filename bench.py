@@ -414,17 +414,29 @@ def run_c1(args):
         res[prec] = (eta.double().cpu().numpy(), it, rel, t, s.stalled)
     e32, it, rel, t, stalled = res["f32/f32"]
     e64, it64, rel64, t64, _ = res["f64/f64"]
-    _, u = plain_elasticity_128(G, precision="f64/f64")
+    # FP32 bulk sweeps to the FP64 tolerance: mixed-precision iterative refinement
+    s, u = plain_elasticity_128(G, precision="f32/f32")
+    s.solve_refined(tol=1e-8, check_every=200)           # warm-up: FP64 twin, graph capture
+    (fr, itr, relr), tr = _timed(lambda: s.solve_refined(tol=1e-8, check_every=200))
+    er, _ = s._twin.update_macroscopic(fr)
+    er = er.double().cpu().numpy()
+    st = s.refine_stats
     line = {"workload": "c1_plain_elasticity_128x128_periodic", "metric": "GLUPS",
-            "value": 128 * 128 * it64 / t64 / 1e9, "unit": "GLUPS", "dtype": "f64 (reaches 1e-8)",
-            "time_to_solution_s": t64, "sweeps": it64, "relative_residual": rel64,
-            "rel_err_vs_exact": float(np.linalg.norm(e64 - u) / np.linalg.norm(u)),
-            "fp32": {"glups": 128 * 128 * it / t / 1e9, "seconds": t, "sweeps": it, "relative_residual": rel,
-                     "stalled_at_rounding_floor": bool(stalled),
-                     "rel_err_vs_exact": float(np.linalg.norm(e32 - u) / np.linalg.norm(u)),
-                     "rel_err_vs_fp64": float(np.linalg.norm(e32 - e64) / np.linalg.norm(e64))},
+            "value": 128 * 128 * itr / tr / 1e9, "unit": "GLUPS",
+            "dtype": "f32 sweeps with f64 defects and master state (iterative refinement; reaches 1e-8)",
+            "time_to_solution_s": tr, "sweeps": itr, "sweeps_f32": st["sweeps_f32"], "sweeps_f64": st["sweeps_f64"],
+            "outer_steps": st["outer"], "relative_residual": relr,
+            "rel_err_vs_exact": float(np.linalg.norm(er - u) / np.linalg.norm(u)),
+            "rel_err_vs_fp64": float(np.linalg.norm(er - e64) / np.linalg.norm(e64)),
+            "fp64": {"glups": 128 * 128 * it64 / t64 / 1e9, "seconds": t64, "sweeps": it64,
+                     "relative_residual": rel64,
+                     "rel_err_vs_exact": float(np.linalg.norm(e64 - u) / np.linalg.norm(u))},
+            "fp32_plain": {"glups": 128 * 128 * it / t / 1e9, "seconds": t, "sweeps": it, "relative_residual": rel,
+                           "stalled_at_rounding_floor": bool(stalled),
+                           "rel_err_vs_exact": float(np.linalg.norm(e32 - u) / np.linalg.norm(u)),
+                           "rel_err_vs_fp64": float(np.linalg.norm(e32 - e64) / np.linalg.norm(e64))},
             "note": "L2-resident 0.5 MB problem: launch/latency bound, sweeps replayed as CUDA graphs; "
-                    "FP32 residuals cannot fall below ~1e-5 of the first update"}
+                    "plain FP32 residuals cannot fall below ~1e-5 of the first update"}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -712,9 +724,10 @@ def run_c2solve(args):
     (FP64 norms reduced on the device every ``check`` sweeps; the sweeps of one
     check interval are one CUDA-graph replay).  Three runs from the same start:
     all FP64; FP32 populations until the residual stops falling (the FP32
-    rounding floor); FP32 until that floor, then FP64 to 1e-8 of the FP32
-    run's first residual.  Reports sweeps and time to solution and the relative
-    L2 pressure error of each run against the FP64 run."""
+    rounding floor); FP32 correction sweeps under FP64 defects and master
+    state (mixed-precision iterative refinement) to 1e-8.  Reports sweeps and
+    time to solution and the relative L2 pressure error of each run against
+    the FP64 run."""
     import torch
     import xlb_biot_b200.api as G
     from xlb_biot_b200 import autotune
@@ -734,23 +747,26 @@ def run_c2solve(args):
         p = solver.update_macroscopic(fs).double()
         return solver, fs, p, {"sweeps": int(sweeps), "seconds": t, "relative_residual": rel,
                                "stalled": bool(solver.stalled), "glups": N * N * sweeps / t / 1e9, "clocks": clk}
-    _, _, p64, out["f64"] = run("f64/f64")
+    s64, _, p64, out["f64"] = run("f64/f64")
     s32, f32, p32, out["f32"] = run("f32/f32")
-    # the FP32 run's reference norm: its own first sweep from the same start
-    loop = s32._sweep_loop(check, None)
-    r0 = loop.first(s32.assign_fields_sharded())
-    _, _, ph, hyb = run("f64/f64", f=f32.double(), r0=r0)
-    hyb["sweeps_f32"] = out["f32"]["sweeps"]
-    hyb["sweeps_f64"] = hyb.pop("sweeps")
-    hyb["seconds"] += out["f32"]["seconds"]
-    out["f32_then_f64"] = hyb
+    # FP32 bulk sweeps to the FP64 tolerance: mixed-precision iterative refinement
+    s32.solve_refined(tol=1e-3, check_every=check)        # warm-up: FP64 twin, graph capture
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    (fr, sweeps, rel), t = _timed(lambda: s32.solve_refined(tol=tol, check_every=check))
+    st = s32.refine_stats
+    out["f32_refined"] = {"seconds": t, "sweeps_f32": st["sweeps_f32"], "sweeps_f64": st["sweeps_f64"],
+                          "outer_steps": st["outer"], "relative_residual": rel,
+                          "inner": [{k: v for k, v in d.items()} for d in st["inner"]],
+                          "glups": N * N * sweeps / t / 1e9, "clocks": clocks.stop()}
+    pr = s64.update_macroscopic(fr).double()
 
     def err(p):
         return float(torch.linalg.vector_norm(p - p64) / torch.linalg.vector_norm(p64))
     out["f32"]["pressure_rel_err_vs_f64"] = err(p32)
-    out["f32_then_f64"]["pressure_rel_err_vs_f64"] = err(ph)
+    out["f32_refined"]["pressure_rel_err_vs_f64"] = err(pr)
     print(json.dumps({"workload": "c2_darcy_1024x1024_lognormal_steady_state", "metric": "time_to_solution",
-                      "unit": "s", "higher_is_better": False, "value": out["f32_then_f64"]["seconds"],
+                      "unit": "s", "higher_is_better": False, "value": out["f32_refined"]["seconds"],
                       "tolerance": tol, "check_every": check, "runs": out, "data": "synthetic"}), flush=True)
     return 0
 

@@ -176,6 +176,9 @@ typedef struct {
     const void* ext_source;  /* external source (1 plane) or NULL */
     XlbbRules pc, ps;
     double* sumsq;
+    const void* resid;       /* 9 planes r or NULL: the sweep collides f - r (a
+                                refinement step's correction equation); not
+                                with post-collision rules (XLBB_EUNSUPPORTED) */
 } XlbbDarcySweep;
 
 int xlbb_darcy_sweep(int dtype, const XlbbGrid* g, const XlbbDarcySweep* s, void* stream);
@@ -194,8 +197,8 @@ int xlbb_darcy_sweep_pipeline(int dtype, const XlbbGrid* g, const XlbbDarcySweep
  * KBCSim.collision, :48-72, inside LBMBase.step, src/base.py:809-846):
  * collision with the second-order equilibrium of src/base.py:686-724,
  * PostCollision rules, streaming, PostStreaming rules.  Same argument block as
- * xlbb_darcy_sweep (omega uniform or per cell); source and ext_source must be
- * NULL (XLBB_EBADARG otherwise).  sumsq, when set, has
+ * xlbb_darcy_sweep (omega uniform or per cell); source, ext_source and resid
+ * must be NULL (XLBB_EBADARG otherwise).  sumsq, when set, has
  * xlbb_darcy_sweep_ctas(dtype, g) entries, of which it writes
  * xlbb_darcy_sweep_partials(dtype, g, s).
  */

@@ -64,7 +64,7 @@ class ElastSweep(ctypes.Structure):
 class DarcySweep(ctypes.Structure):
     _fields_ = [("f_in", ctypes.c_void_p), ("f_out", ctypes.c_void_p), ("omega", ctypes.c_double),
                 ("omega_field", ctypes.c_void_p), ("source", ctypes.c_void_p), ("ext_source", ctypes.c_void_p),
-                ("pc", Rules), ("ps", Rules), ("sumsq", ctypes.c_void_p)]
+                ("pc", Rules), ("ps", Rules), ("sumsq", ctypes.c_void_p), ("resid", ctypes.c_void_p)]
 
 
 class BatchInstance(ctypes.Structure):

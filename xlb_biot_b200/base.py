@@ -22,6 +22,7 @@ class LBMBase:
     """``src/base.py:30-146``."""
 
     def __init__(self, **kwargs):
+        self._init_kwargs = dict(kwargs)       # an FP64 twin is built from them (refine.py)
         self.omega = kwargs.get("omega")
         self.nx = kwargs.get("nx")
         self.ny = kwargs.get("ny")

@@ -353,6 +353,7 @@ struct DarcyPhys {
         const T* omega_f;
         const T* source;
         const T* ext;
+        const T* resid;          // 9 planes subtracted from the input before the collision, or NULL
         RulesView<T, 9> pc, ps;
         double* sumsq;
         static constexpr int PMAX = 12;
@@ -421,18 +422,26 @@ struct DarcyPhys {
     }
     static bool push_ok(const Args&) { return true; }
     __device__ static T f_in(const In& in, int i) { return in.f[i]; }
-    __device__ static void collide(const Args& p, int, int, const In& in, T (&o)[9]) {
+    __device__ static void collide(const Args& p, int y, int x, const In& in, T (&o)[9]) {
         const bool hasS = p.source != nullptr || p.ext != nullptr;
-        T rho = in.f[0];
+        T f[9];
 #pragma unroll
-        for (int i = 1; i < 9; ++i) rho += in.f[i];
+        for (int i = 0; i < 9; ++i) f[i] = in.f[i];
+        if (p.resid) {      // the sweep of f - resid (the correction equation of a refinement step)
+            const size_t o = (size_t)y * p.geom.pitch + x;
+#pragma unroll
+            for (int i = 0; i < 9; ++i) f[i] = f[i] - __ldg(p.resid + (o + (size_t)i * p.geom.plane));
+        }
+        T rho = f[0];
+#pragma unroll
+        for (int i = 1; i < 9; ++i) rho += f[i];
         if (hasS) rho = rho + T(0.5) * in.S;
         const T om = in.om;
         const T sf = T(1) - T(0.5) * om;
 #pragma unroll
         for (int i = 0; i < 9; ++i) {
             const T feq = rho * w9<T>(i);
-            T v = in.f[i] - om * (in.f[i] - feq);
+            T v = f[i] - om * (f[i] - feq);
             if (hasS) v = v + in.S * (sf * w9<T>(i));
             o[i] = v;
         }
@@ -477,7 +486,9 @@ struct FluidPhys : DarcyPhys<T_> {
         // momentum: D2Q9 x-velocities (+) 3, 5, 7 and (-) 4, 6, 8; y (+) 1, 4, 7 and (-) 2, 5, 8
         const T jx = ((in.f[3] - in.f[4]) + (in.f[5] - in.f[6])) + (in.f[7] - in.f[8]);
         const T jy = ((in.f[1] - in.f[2]) + (in.f[4] - in.f[5])) + (in.f[7] - in.f[8]);
-        const T ux = jx / rho, uy = jy / rho;
+        // one reciprocal of rho instead of two divisions (u = j / rho)
+        const T irho = T(1) / rho;
+        const T ux = jx * irho, uy = jy * irho;
         const T usqr = T(1.5) * (ux * ux + uy * uy);
         const T om = in.om;
         T feq[9];
@@ -500,7 +511,7 @@ struct FluidPhys : DarcyPhys<T_> {
             const T pyy = (fneq[1] + fneq[2]) + dg;
             const T pxy = (fneq[7] + fneq[8]) - (fneq[4] + fneq[5]);
             const T N = pxx - pyy;
-            const T r4 = rho / T(4);
+            const T r4 = rho * T(0.25);
             T dS[9];
             dS[0] = T(0);
             dS[1] = -N * r4;
@@ -511,12 +522,15 @@ struct FluidPhys : DarcyPhys<T_> {
             dS[5] = -pxy * r4;
             dS[7] = pxy * r4;
             dS[8] = pxy * r4;
+            // entropic products <x, y> = sum x y / feq with one reciprocal of
+            // feq per direction shared by both products
             T sh = T(0), hh = T(0);
 #pragma unroll
             for (int i = 0; i < 9; ++i) {
                 const T dH = fneq[i] - dS[i];
-                sh += dS[i] * dH / feq[i];
-                hh += dH * dH / feq[i];
+                const T ife = T(1) / feq[i];
+                sh += (dS[i] * dH) * ife;
+                hh += (dH * dH) * ife;
             }
             const T beta = om * T(0.5);
             const T ib = T(1) / beta;
@@ -1037,6 +1051,7 @@ static typename Ph::Args darcy_args(const XlbbGrid* g, const XlbbDarcySweep* s) 
     a.omega_f = static_cast<const T*>(s->omega_field);
     a.source = static_cast<const T*>(s->source);
     a.ext = static_cast<const T*>(s->ext_source);
+    a.resid = static_cast<const T*>(s->resid);
     a.pc = rules_view<T, 9>(s->pc);
     a.ps = rules_view<T, 9>(s->ps);
     a.sumsq = s->sumsq;
@@ -1987,6 +2002,8 @@ int xlbb_darcy_sweep(int dtype, const XlbbGrid* g, const XlbbDarcySweep* s, void
     if (!grid_ok(g) || !s || !s->f_in || !s->f_out) return fail(XLBB_EBADARG, "xlbb_darcy_sweep: bad argument");
     if (s->f_in == s->f_out) return fail(XLBB_EBADARG, "xlbb_darcy_sweep: f_in and f_out must differ");
     if (!rules_ok(s->pc, g) || !rules_ok(s->ps, g)) return fail(XLBB_EBADARG, "xlbb_darcy_sweep: incomplete rules");
+    if (s->resid && s->pc.count > 0 && s->pc.row_ptr)
+        return fail(XLBB_EUNSUPPORTED, "xlbb_darcy_sweep: resid with post-collision rules");
 
     if (dtype == XLBB_F32) return darcy_sweep_t<float>(g, s, XLBB_STREAM(stream));
     if (dtype == XLBB_F64) return darcy_sweep_t<double>(g, s, XLBB_STREAM(stream));
@@ -1997,7 +2014,8 @@ int xlbb_fluid_sweep(int dtype, const XlbbGrid* g, const XlbbDarcySweep* s, int 
     if (!grid_ok(g) || !s || !s->f_in || !s->f_out) return fail(XLBB_EBADARG, "xlbb_fluid_sweep: bad argument");
     if (model != XLBB_FLUID_BGK && model != XLBB_FLUID_KBC) return fail(XLBB_EBADARG, "xlbb_fluid_sweep: model");
     if (s->f_in == s->f_out) return fail(XLBB_EBADARG, "xlbb_fluid_sweep: f_in and f_out must differ");
-    if (s->source || s->ext_source) return fail(XLBB_EBADARG, "xlbb_fluid_sweep: source planes are not supported");
+    if (s->source || s->ext_source || s->resid)
+        return fail(XLBB_EBADARG, "xlbb_fluid_sweep: source and resid planes are not supported");
     if (!rules_ok(s->pc, g) || !rules_ok(s->ps, g)) return fail(XLBB_EBADARG, "xlbb_fluid_sweep: incomplete rules");
 
     const bool kbc = model == XLBB_FLUID_KBC;

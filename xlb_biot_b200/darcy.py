@@ -127,7 +127,7 @@ class AdvectionDiffusionReactionBGK(LBMBase):
         from .bc_compile import apply_rules_device
         return apply_rules_device(self._pc if implementation_step == "PostCollision" else self._ps, fout, fin)
 
-    def _sweep(self, f, external_source=None, out=None, sumsq=False):
+    def _sweep(self, f, external_source=None, out=None, sumsq=False, resid=None, homogeneous=False):
         L = self._layout
         out = L.empty(9) if out is None else out
         if sumsq:
@@ -136,19 +136,33 @@ class AdvectionDiffusionReactionBGK(LBMBase):
             n_max = _lib.check(_lib.lib().xlbb_darcy_sweep_ctas(self._dcode, L.grid()), "xlbb_darcy_sweep_ctas")
             if self._partials.numel() < n_max:
                 self._partials = torch.empty(n_max, dtype=torch.float64, device=L.device)
-        s = self._sweep_args(f, out, external_source, sumsq)
+        s = self._sweep_args(f, out, external_source, sumsq, resid, homogeneous)
         if sumsq:
             self._n_partials = _lib.check(_lib.lib().xlbb_darcy_sweep_partials(self._dcode, L.grid(), s),
                                           "xlbb_darcy_sweep_partials")
         _lib.check(_lib.lib().xlbb_darcy_sweep(self._dcode, L.grid(), s, _lib.stream_ptr()), "xlbb_darcy_sweep")
         return out
 
-    def _sweep_args(self, f, out, external_source=None, sumsq=False):
+    def _sweep_args(self, f, out, external_source=None, sumsq=False, resid=None, homogeneous=False):
+        """Kernel arguments; ``homogeneous``: the linear part of the sweep (no
+        sources, boundary constants zero), ``resid``: collide f - resid."""
+        pc, ps = self._homogeneous_rules() if homogeneous else (self._pc, self._ps)
+        source = None if homogeneous else self.source
+        ext = None if homogeneous else external_source
         return _lib.DarcySweep(f.data_ptr(), out.data_ptr(), float(self.omega),
                                self.omega_field.data_ptr() if self.omega_field is not None else None,
-                               self.source.data_ptr() if self.source is not None else None,
-                               external_source.data_ptr() if external_source is not None else None,
-                               self._pc.struct(), self._ps.struct(), self._partials.data_ptr() if sumsq else None)
+                               source.data_ptr() if source is not None else None,
+                               ext.data_ptr() if ext is not None else None,
+                               pc.struct(), ps.struct(), self._partials.data_ptr() if sumsq else None,
+                               resid.data_ptr() if resid is not None else None)
+
+    def _homogeneous_rules(self):
+        if "_hom_rules" not in self.__dict__:
+            from .refine import homogeneous_rules
+            L = self._layout
+            self._hom_rules = (homogeneous_rules(self._pc, L.ny, L.dtype, L.device),
+                               homogeneous_rules(self._ps, L.ny, L.dtype, L.device))
+        return self._hom_rules
 
     def sweep_pipeline(self, f=None, out=None):
         """The launch pipeline a sweep of this solver runs now (3: collide and
@@ -199,6 +213,43 @@ class AdvectionDiffusionReactionBGK(LBMBase):
             return loop.n, ((float(loop.sumsq[0]) ** 0.5) / r0 if r0 > 0 else 0.0)
         it, rel, self.stalled = iterate_to_tolerance(replay, tol, max_sweeps - 1, stall_checks)
         return loop.result, it + 1, rel
+
+    def solve_refined(self, f=None, tol=1e-8, inner_tol=1e-5, check_every=1000, max_sweeps=10 ** 8, max_outer=30,
+                      stall_checks=20):
+        """Steady state to an FP64 relative residual ``tol`` with the bulk of the
+        sweeps in FP32 (mixed-precision iterative refinement, ``refine.py``):
+        FP64 master state and defect sweeps, FP32 correction sweeps.  The
+        solver must be FP32 ('f32/f32') without post-collision rules; an FP64
+        twin of it (same class and keywords) computes the defects.  Returns
+        ``(F, sweeps, relative_residual)`` with F the FP64 populations;
+        ``self.refine_stats`` holds the outer/inner breakdown."""
+        from .refine import CorrectionLoop, refine, twin64
+        L = self._layout
+        if L.dtype != torch.float32:
+            raise _lib.XlbbError("solve_refined runs its bulk sweeps in FP32: use precision 'f32/f32'")
+        if self._pc.count:
+            raise NotImplementedError("solve_refined: post-collision rules are not supported")
+        if "_twin" not in self.__dict__:
+            self._twin = twin64(self)
+        twin = self._twin
+        F = twin.assign_fields_sharded() if f is None else twin._layout.field(f, 9).clone()
+        key = ("refine", int(check_every))
+        cache = self.__dict__.setdefault("_loops", {})
+        if key not in cache:
+            cache[key] = CorrectionLoop(self, check_every, 9, lambda a, b, sq, r: self._sweep(
+                a, out=b, sumsq=sq, resid=r, homogeneous=True))
+        loop = cache[key]
+        G = twin._layout.empty(9)
+        sc = torch.zeros(1, dtype=torch.float64, device=L.device)
+
+        def defect(F):
+            twin._sweep(F, out=G, sumsq=True)
+            twin.residual_sumsq(sc)
+            return F - G, float(sc[0]) ** 0.5
+        F, stats = refine(defect, loop, F, tol, inner_tol, max_sweeps, max_outer, stall_checks,
+                          lambda x: twin._layout.field(x, 9))
+        self.refine_stats = stats
+        return F, stats["sweeps_f32"] + stats["sweeps_f64"], stats["relative_residual"]
 
     def _sweep_loop(self, n, external_source):
         """The ``SweepLoop`` of ``n`` sweeps (rounded up to even, so that its

@@ -62,6 +62,7 @@ class LBMElasticity:
     """``src/elasticity.py:30-1501``."""
 
     def __init__(self, **kwargs):
+        self._init_kwargs = dict(kwargs)       # an FP64 twin is built from them (refine.py)
         self.lamda = kwargs.get("lambda")
         self.mu = kwargs.get("mu")
         self.nx = kwargs.get("nx")
@@ -564,10 +565,12 @@ class LBMElasticity:
 
     # ------------------------------------------------------------------ kernels
     def _sweep(self, f, level, a=0.0, b=1.0, resid=None, fext=None, out=None, sumsq=False, div_out=None,
-               sumsq_diff=False, acc64=False, query=False):
+               sumsq_diff=False, acc64=False, query=False, homogeneous=False):
         """One fused sweep on ``level``; ``acc64``: FP64 arithmetic on the FP32
         level-0 fields (``residual_precision="f64"``).  ``query``: launch
-        nothing, return the pipeline the library would run (diagnostic)."""
+        nothing, return the pipeline the library would run (diagnostic).
+        ``homogeneous``: the linear part of the sweep (no static force,
+        boundary constants zero; a refinement step's correction)."""
         L = self._L(level)
         out = L.empty(8) if out is None else out
         if fext is not None and not L.conforms(fext, 2):
@@ -580,9 +583,13 @@ class LBMElasticity:
             if self._partials.numel() < n_max:
                 self._partials = torch.empty(n_max, dtype=torch.float64, device=L.device)
         pc, ps = self._rules_acc64 if acc64 else self._rules[level]
+        force = self.force
+        if homogeneous:
+            pc, ps = self._homogeneous_rules(level)
+            force = None
         bx0, bx1, by0, by1 = self._box(level)
-        s = _lib.ElastSweep(f.data_ptr(), out.data_ptr(), self.force.data_ptr() if self.force is not None else None,
-                            1 if level == 0 else 0, fext.data_ptr() if fext is not None else None,
+        s = _lib.ElastSweep(f.data_ptr(), out.data_ptr(), force.data_ptr() if force is not None else None,
+                            1 if level == 0 and force is not None else 0, fext.data_ptr() if fext is not None else None,
                             resid.data_ptr() if resid is not None else None, float(a), float(b),
                             pc.struct(), ps.struct(), self._partials.data_ptr() if sumsq else None,
                             bx0, bx1, by0, by1, div_out.data_ptr() if div_out is not None else None,
@@ -596,6 +603,53 @@ class LBMElasticity:
         _lib.check(_lib.lib().xlbb_elast_sweep(code, L.grid(), self._mats[level], s, _lib.stream_ptr()),
                    "xlbb_elast_sweep")
         return out
+
+    def _homogeneous_rules(self, level):
+        cache = self.__dict__.setdefault("_hom_rules", {})
+        if level not in cache:
+            from .refine import homogeneous_rules
+            L = self._L(level)
+            cache[level] = tuple(homogeneous_rules(r, L.ny, L.dtype, L.device) for r in self._rules[level])
+        return cache[level]
+
+    def solve_refined(self, f=None, tol=1e-8, inner_tol=1e-5, check_every=200, max_sweeps=10 ** 7, max_outer=30,
+                      external_force=None, stall_checks=20):
+        """Pseudo-time iteration to an FP64 relative residual ``tol`` with the
+        bulk of the sweeps in FP32 (mixed-precision iterative refinement,
+        ``refine.py``): FP64 master state and defect sweeps, FP32 correction
+        sweeps.  Single-level FP32 solvers ('f32/f32'); an FP64 twin of the
+        solver (same class and keywords) computes the defects.  Returns
+        ``(F, sweeps, relative_residual)`` with F the FP64 populations;
+        ``self.refine_stats`` holds the outer/inner breakdown."""
+        from .refine import CorrectionLoop, refine, twin64
+        L = self._L(0)
+        if L.dtype != torch.float32:
+            raise _lib.XlbbError("solve_refined runs its bulk sweeps in FP32: use precision 'f32/f32'")
+        if self.levels != 1:
+            raise NotImplementedError("solve_refined: single-level solvers (MG_levels=1)")
+        if "_twin" not in self.__dict__:
+            self._twin = twin64(self)
+        twin = self._twin
+        T = twin._L(0)
+        F = twin.assign_fields_sharded() if f is None else T.field(f, 8).clone()
+        ext = T.field(external_force, 2)
+        key = ("refine", int(check_every))
+        cache = self.__dict__.setdefault("_loops", {})
+        if key not in cache:
+            cache[key] = CorrectionLoop(self, check_every, 8, lambda a, b, sq, r: self._sweep(
+                a, 0, 0.0, 1.0, resid=r, out=b, sumsq=sq, sumsq_diff=True, homogeneous=True))
+        loop = cache[key]
+        D = T.empty(8)
+        sc = torch.zeros(1, dtype=torch.float64, device=L.device)
+
+        def defect(F):
+            twin._sweep(F, 0, 1.0, -1.0, fext=ext, out=D, sumsq=True)     # F - S(F)
+            twin._reduce_partials(sc)
+            return D.clone(), float(sc[0]) ** 0.5
+        F, stats = refine(defect, loop, F, tol, inner_tol, max_sweeps, max_outer, stall_checks,
+                          lambda x: T.field(x, 8))
+        self.refine_stats = stats
+        return F, stats["sweeps_f32"] + stats["sweeps_f64"], stats["relative_residual"]
 
     def _reduce_partials(self, out_scalar):
         _lib.check(_lib.lib().xlbb_reduce_sum(self._partials.data_ptr(), self._n_partials, out_scalar.data_ptr(),
