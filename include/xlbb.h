@@ -33,7 +33,8 @@ extern "C" {
 
 #define XLBB_F32 0
 #define XLBB_F64 1
-#define XLBB_F32_ACC64 2   /* FP32 storage, FP64 arithmetic (elasticity sweeps only) */
+#define XLBB_F32_ACC64 2   /* FP32 storage, FP64 arithmetic and rule constants (elasticity
+                              and Darcy sweeps: the "f64/f32" precision policy) */
 
 typedef struct {
     int nx, ny;        /* logical grid size (cells)                        */

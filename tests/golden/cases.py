@@ -39,17 +39,17 @@ def _in(m, x):
     return conv(x) if conv is not None else x
 
 
-def _el(m, cls, **kw):
-    return cls(lattice=m.LatticeD2Q8(PREC), **{"lambda": LAM}, mu=MU, nz=0, precision=PREC, print_info_rate=0, **kw)
+def _el(m, cls, prec=PREC, **kw):
+    return cls(lattice=m.LatticeD2Q8(prec), **{"lambda": LAM}, mu=MU, nz=0, precision=prec, print_info_rate=0, **kw)
 
 
-def elast_plain(m, nx, ny, sweeps=20):
+def elast_plain(m, nx, ny, sweeps=20, prec=PREC):
     """Periodic elasticity from a seeded random equilibrium, plain sweeps, then
     the macroscopic fields and the divergence (``src/elasticity.py:1128-1219``,
     ``:1003-1058``)."""
     P = make_periodic_elasticity(m)
     P.init_seed = 3
-    s = _el(m, P, nx=nx, ny=ny)
+    s = _el(m, P, prec, nx=nx, ny=ny)
     f = s.assign_fields_sharded()
     out = {"f0": to_np(f)}
     for t in range(sweeps):
@@ -72,10 +72,10 @@ def elast_periodic_mg(m, n=32, levels=3, cycles=3):
     return {"f": to_np(f), "norms": np.array(norms)}
 
 
-def elast_walled_mg(m, kind, cycles=4):
+def elast_walled_mg(m, kind, cycles=4, prec=PREC):
     """``dirichlet_MG.py`` / ``neumann_MG.py``: BC rules on every level, 3 levels."""
     kw = dict(nx=18, ny=18, MG_levels=3, MG_BCs={"top": True, "bottom": True, "left": True, "right": True})
-    s = _el(m, make_walled_elasticity(m, kind), **kw)
+    s = _el(m, make_walled_elasticity(m, kind), prec, **kw)
     f = 1e-3 * np.random.default_rng(7).standard_normal((18, 18, 8))
     out = {"f0": f.copy()}
     norms = []
@@ -107,13 +107,13 @@ def elast_halfway(m):
     return out
 
 
-def darcy(m, kind, sweeps=30):
+def darcy(m, kind, sweeps=30, prec=PREC):
     """``examples/darcy/*.py`` set-ups: sweeps with an alternating external
     source, then pressure, pressure gradient and the isotropic gradient
     (``src/darcy.py:36-171``, BCs ``:298-466``)."""
     nx = 24 if kind == "periodic" else 26
-    s = make_darcy(m, kind)(lattice=m.LatticeD2Q9(PREC), omega=1.0 / (3 * 0.1 + 0.5), nx=nx, ny=nx - 4, nz=0,
-                            precision=PREC, print_info_rate=0)
+    s = make_darcy(m, kind)(lattice=m.LatticeD2Q9(prec), omega=1.0 / (3 * 0.1 + 0.5), nx=nx, ny=nx - 4, nz=0,
+                            precision=prec, print_info_rate=0)
     f = s.assign_fields_sharded()
     out = {"f0": to_np(f)}
     ext = _in(m, 1e-3 * np.random.default_rng(2).standard_normal((nx, nx - 4, 1)))
@@ -251,4 +251,11 @@ CASES = {
     "biot_terzaghi_l3": biot_terzaghi,
     "mg_transfers": mg_transfers,
     "parameters_terzaghi": parameters_terzaghi,
+    # the 'f64/f32' policy: FP64 arithmetic on FP32 storage (held to the FP32 bar)
+    "elast_plain_16x16_f64f32": lambda m: elast_plain(m, 16, 16, prec="f64/f32"),
+    "elast_dirichlet_mg3_f64f32": lambda m: elast_walled_mg(m, "dirichlet", prec="f64/f32"),
+    "darcy_anti_f64f32": lambda m: darcy(m, "anti", prec="f64/f32"),
 }
+
+# relative tolerance of each case (FP64 runs: 1e-12; FP32 storage: 1e-5)
+TOLERANCE = {name: (1e-5 if name.endswith("_f64f32") else 1e-12) for name in CASES}

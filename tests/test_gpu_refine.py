@@ -71,3 +71,32 @@ def test_correction_sweep_is_the_homogeneous_sweep_of_f_minus_r():
     ref = s._sweep(d, out=L.empty(9)) - s._sweep(z, out=L.empty(9))
     torch.cuda.synchronize()
     assert float((got - ref).abs().max()) <= 1e-13
+
+
+@pytest.mark.parametrize("kind", ["darcy", "elasticity"])
+def test_f64_f32_policy_is_closer_to_fp64_than_f32(kind):
+    """'f64/f32' (FP64 arithmetic on FP32 storage) against 'f32/f32' and the
+    all-FP64 run on the same problem: both within the FP32 bar of FP64, the
+    FP64-arithmetic sweeps no worse."""
+    import xlb_biot_b200.api as G
+    from xlb_biot_b200.workloads import darcy_lognormal
+    out = {}
+    for prec in ("f64/f64", "f64/f32", "f32/f32"):
+        if kind == "darcy":
+            s, _ = darcy_lognormal(G, n=96, ell=8.0, precision=prec)
+            f = s.assign_fields_sharded()
+            for t in range(200):
+                f, _ = s.step(f, t)
+        else:
+            lam, mu = elastic_material()
+            P = make_periodic_elasticity(G)
+            P.init_seed = 3
+            s = P(lattice=G.LatticeD2Q8(prec), **{"lambda": lam}, mu=mu, nx=48, ny=48, nz=0, precision=prec,
+                  MG_levels=3, print_info_rate=0)
+            f = s.assign_fields_sharded()
+            for t in range(6):
+                f, _ = s.step(f, t)
+        out[prec] = f.double()
+    e32, e6432 = _rel(out["f32/f32"], out["f64/f64"]), _rel(out["f64/f32"], out["f64/f64"])
+    assert out["f64/f32"].dtype == torch.float64
+    assert e6432 < 1e-5 and e32 < 1e-5 and e6432 <= 1.5 * e32, (e6432, e32)

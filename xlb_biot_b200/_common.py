@@ -22,14 +22,23 @@ def set_precisions(precision):
 
 
 def make_policy(precision):
+    """The precision policy of ``precision`` (``src/elasticity.py:606-629``).
+    Supported: 'f64/f64', 'f32/f32' and 'f64/f32' (FP32 storage, FP64
+    arithmetic in every collide-and-stream sweep with FP64 boundary constants;
+    the auxiliary kernels -- moments, gradients, transfers -- compute in the
+    FP32 storage type).  Half-precision storage is not provided."""
     compute, stored = set_precisions(precision)
-    if compute != stored:
-        raise NotImplementedError(
-            f"precision {precision!r}: the CUDA kernels compute in their storage type; "
-            "use 'f32/f32' or 'f64/f64'")
-    if compute == np.float16:
-        raise NotImplementedError("precision 'f16/f16' is not supported by the CUDA kernels")
+    if stored == np.float16 or compute == np.float16:
+        raise NotImplementedError(f"precision {precision!r}: half-precision storage is not supported by the "
+                                  "CUDA kernels; use 'f32/f32', 'f64/f32' or 'f64/f64'")
     return PrecisionPolicy(compute, stored)
+
+
+def storage_and_sweep_dtypes(policy):
+    """(storage torch dtype, whether sweeps compute in FP64 on FP32 storage)."""
+    storage = torch.float64 if np.dtype(policy.output_dtype) == np.float64 else torch.float32
+    acc64 = np.dtype(policy.compute_dtype) == np.float64 and storage == torch.float32
+    return storage, acc64
 
 
 def print_parameters(obj, attrs, names):

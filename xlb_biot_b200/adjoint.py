@@ -51,6 +51,8 @@ def elast_sweep_adjoint(el, level, lam_out, a=0.0, b=1.0, f_in=None, resid=None,
     lam_force = L.empty(2) if want_force else None
     if fext is not None and not L.conforms(fext, 2):
         fext = L.field(fext, 2)
+    if getattr(el, "_acc64_all", False):
+        raise NotImplementedError("the adjoint kernels compute in their storage type: use 'f32/f32' or 'f64/f64'")
     pc, ps = el._rules[level]
     force = el.force if level == 0 else None
     s = _lib.ElastSweepAdjoint(

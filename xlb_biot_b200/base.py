@@ -13,7 +13,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._common import make_policy, print_parameters, set_precisions
+from ._common import make_policy, print_parameters, set_precisions, storage_and_sweep_dtypes
 from .boundary_conditions import grid_mask, solid_halo_voxels
 from .fields import Layout, torch_dtype
 
@@ -51,8 +51,11 @@ class LBMBase:
         self.show_simulation_parameters()
         self.gridInfo = {"nx": self.nx, "ny": self.ny, "nz": self.nz, "dim": self.lattice.d, "lattice": self.lattice}
         self.sharding = None
-        self._dtype = torch_dtype(self.precisionPolicy.compute_dtype)
+        # storage type of the fields; 'f64/f32' sweeps compute in FP64 on them
+        self._dtype, self._acc64 = storage_and_sweep_dtypes(self.precisionPolicy)
         self._dcode = _lib.dtype_code(self._dtype)
+        self._sweep_code = _lib.XLBB_F32_ACC64 if self._acc64 else self._dcode
+        self._rule_dtype = torch.float64 if self._acc64 else self._dtype
         self._layout = Layout(self.nx, self.ny, self._dtype)
         self.boundingBoxIndices = self.bounding_box_indices()
         self._create_boundary_data()

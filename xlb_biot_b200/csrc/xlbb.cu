@@ -339,29 +339,33 @@ struct ElastPhys {
 // ---------------------------------------------------------------------------
 // D2Q9 advection-diffusion-reaction BGK (src/darcy.py:106-129).
 // ---------------------------------------------------------------------------
-template <typename T_>
+// T_: arithmetic type; St_: storage type of the fields (St_ = float with
+// T_ = double is FP32 storage with FP64 arithmetic, the 'f64/f32' policy).
+template <typename T_, typename St_ = T_>
 struct DarcyPhys {
     using T = T_;
+    using St = St_;
+    using Storage = St_;
     static constexpr int Q = 9;
     __host__ __device__ static constexpr int cx(int i) { return cx9(i); }
     __host__ __device__ static constexpr int cy(int i) { return cy9(i); }
     struct Args {
         SweepGeom geom;
-        const T* f_in;
-        T* f_out;
+        const St* f_in;
+        St* f_out;
         T omega;
-        const T* omega_f;
-        const T* source;
-        const T* ext;
-        const T* resid;          // 9 planes subtracted from the input before the collision, or NULL
+        const St* omega_f;
+        const St* source;
+        const St* ext;
+        const St* resid;         // 9 planes subtracted from the input before the collision, or NULL
         RulesView<T, 9> pc, ps;
         double* sumsq;
         static constexpr int PMAX = 12;
-        const T* planes[PMAX];   // input planes in from_smem order (bulk-copy kernel)
+        const St* planes[PMAX];  // input planes in from_smem order (bulk-copy kernel, St = T only)
         int np;
         // Plane pointers in fixed slots (f 0-8, omega 9, source 10, ext 11)
-        const T* ip[12];
-        T* op[9];
+        const St* ip[12];
+        St* op[9];
     };
     __host__ __device__ static void fill_ptrs(Args& a) {
         for (int i = 0; i < 9; ++i) {
@@ -400,12 +404,12 @@ struct DarcyPhys {
     __device__ static void load(const Args& p, int y, int x, In& in) {
         const int o = y * p.geom.pitch + x;
 #pragma unroll
-        for (int i = 0; i < 9; ++i) in.f[i] = __ldg(p.ip[i] + o);
+        for (int i = 0; i < 9; ++i) in.f[i] = T(__ldg(p.ip[i] + o));
         T S = T(0);
-        if (p.source) S = __ldg(p.ip[10] + o);
-        if (p.ext) S = p.source ? S + __ldg(p.ip[11] + o) : __ldg(p.ip[11] + o);
+        if (p.source) S = T(__ldg(p.ip[10] + o));
+        if (p.ext) S = p.source ? S + T(__ldg(p.ip[11] + o)) : T(__ldg(p.ip[11] + o));
         in.S = S;
-        in.om = p.omega_f ? __ldg(p.ip[9] + o) : p.omega;
+        in.om = p.omega_f ? T(__ldg(p.ip[9] + o)) : p.omega;
     }
     __device__ static void fin(const In& in, T (&g)[9]) {
 #pragma unroll
@@ -413,9 +417,10 @@ struct DarcyPhys {
     }
     template <bool SUMSQ>
     __device__ static double put(const Args& p, int i, int o, int, int, T s) {
-        p.op[i][o] = s;
+        const St sv = St(s);
+        p.op[i][o] = sv;
         if constexpr (SUMSQ) {
-            const double d = (double)s - (double)__ldg(p.ip[i] + o);
+            const double d = (double)sv - (double)__ldg(p.ip[i] + o);
             return d * d;
         }
         return 0.0;
@@ -430,7 +435,7 @@ struct DarcyPhys {
         if (p.resid) {      // the sweep of f - resid (the correction equation of a refinement step)
             const size_t o = (size_t)y * p.geom.pitch + x;
 #pragma unroll
-            for (int i = 0; i < 9; ++i) f[i] = f[i] - __ldg(p.resid + (o + (size_t)i * p.geom.plane));
+            for (int i = 0; i < 9; ++i) f[i] = f[i] - T(__ldg(p.resid + (o + (size_t)i * p.geom.plane)));
         }
         T rho = f[0];
 #pragma unroll
@@ -452,9 +457,10 @@ struct DarcyPhys {
         double acc = 0.0;
 #pragma unroll
         for (int i = 0; i < 9; ++i) {
-            p.op[i][o] = S[i];
+            const St sv = St(S[i]);
+            p.op[i][o] = sv;
             if constexpr (PREV) {
-                const double d = (double)S[i] - (double)fprev[i];
+                const double d = (double)sv - (double)St(fprev[i]);
                 acc += d * d;
             }
         }
@@ -654,12 +660,13 @@ static void launch_sweep(XlbbSweepConfig c, const XlbbGrid* g, cudaStream_t st, 
         else launch_k(sweep_warp_kernel<Ph, 1, PREV>, wg.ctas, 128, 0, st, a, wg.nbx, wg.nstrips);
         return;
     }
-    Ph::make_planes(a);
-    if (c.pipeline == 1 && !bulk_aligned<Ph>(a)) {
+    constexpr bool SAME = std::is_same<typename Ph::T, typename Ph::Storage>::value;
+    if constexpr (SAME) Ph::make_planes(a);
+    if (c.pipeline == 1 && (!SAME || !bulk_aligned<Ph>(a))) {     // the bulk ring holds the arithmetic type
         c.pipeline = 0;
         c.depth = c.depth > 2 ? 2 : c.depth;
     }
-    if (c.pipeline == 1) {
+    if constexpr (SAME) if (c.pipeline == 1) {
 #define XLBB_BULK(TX_, D_)                                              \
     if (c.tx == TX_ && c.depth == D_) {                                  \
         launch_bulk<Ph, TX_, D_, PREV>(grid, st, a);                     \
@@ -1043,15 +1050,16 @@ static ElastMat<T, S> make_mat(const XlbbElastMaterial* m) {
 template <class Ph>
 static typename Ph::Args darcy_args(const XlbbGrid* g, const XlbbDarcySweep* s) {
     using T = typename Ph::T;
+    using St = typename Ph::Storage;
     typename Ph::Args a;
     a.geom = geom(g);
-    a.f_in = static_cast<const T*>(s->f_in);
-    a.f_out = static_cast<T*>(s->f_out);
+    a.f_in = static_cast<const St*>(s->f_in);
+    a.f_out = static_cast<St*>(s->f_out);
     a.omega = T(s->omega);
-    a.omega_f = static_cast<const T*>(s->omega_field);
-    a.source = static_cast<const T*>(s->source);
-    a.ext = static_cast<const T*>(s->ext_source);
-    a.resid = static_cast<const T*>(s->resid);
+    a.omega_f = static_cast<const St*>(s->omega_field);
+    a.source = static_cast<const St*>(s->source);
+    a.ext = static_cast<const St*>(s->ext_source);
+    a.resid = static_cast<const St*>(s->resid);
     a.pc = rules_view<T, 9>(s->pc);
     a.ps = rules_view<T, 9>(s->ps);
     a.sumsq = s->sumsq;
@@ -1060,19 +1068,24 @@ static typename Ph::Args darcy_args(const XlbbGrid* g, const XlbbDarcySweep* s) 
 
 // FP64 partials that a D2Q9 sweep with these arguments writes when it fuses
 // its residual sum (the CTAs of the launch it takes).
-template <typename T>
+template <typename T, typename St = T>
+static constexpr int darcy_dtype() {
+    return sizeof(T) == sizeof(St) ? (sizeof(T) == 4 ? XLBB_F32 : XLBB_F64) : XLBB_F32_ACC64;
+}
+
+template <typename T, typename St = T>
 static long long darcy_partials_t(const XlbbGrid* g, const XlbbDarcySweep* s) {
-    using Ph = DarcyPhys<T>;
+    using Ph = DarcyPhys<T, St>;
     const typename Ph::Args a = darcy_args<Ph>(g, s);
-    const XlbbSweepConfig c = effective_cfg(1, sizeof(T) == 4 ? XLBB_F32 : XLBB_F64);
+    const XlbbSweepConfig c = effective_cfg(1, darcy_dtype<T, St>());
     return launch_ctas(g, resolve_shape(c, push_eligible<Ph>(a), sizeof(T) == 4));
 }
 
-template <typename T>
+template <typename T, typename St = T>
 static int darcy_sweep_t(const XlbbGrid* g, const XlbbDarcySweep* s, cudaStream_t st) {
-    using Ph = DarcyPhys<T>;
+    using Ph = DarcyPhys<T, St>;
     typename Ph::Args a = darcy_args<Ph>(g, s);
-    const XlbbSweepConfig c = effective_cfg(1, sizeof(T) == 4 ? XLBB_F32 : XLBB_F64);
+    const XlbbSweepConfig c = effective_cfg(1, darcy_dtype<T, St>());
     if (s->sumsq) launch_sweep<Ph, true>(c, g, st, a);
     else launch_sweep<Ph, false>(c, g, st, a);
     return check_launch("xlbb_darcy_sweep");
@@ -1910,7 +1923,7 @@ int xlbb_elast_sweep_ctas(int dtype, const XlbbGrid* g) {
 }
 
 int xlbb_darcy_sweep_ctas(int dtype, const XlbbGrid* g) {
-    if (!grid_ok(g) || (dtype != XLBB_F32 && dtype != XLBB_F64))
+    if (!grid_ok(g) || (dtype != XLBB_F32 && dtype != XLBB_F64 && dtype != XLBB_F32_ACC64))
         return fail(XLBB_EBADARG, "xlbb_darcy_sweep_ctas: bad argument");
     const XlbbSweepConfig c = effective_cfg(1, dtype);
     const bool f32 = dtype == XLBB_F32;
@@ -1925,6 +1938,7 @@ int xlbb_darcy_sweep_partials(int dtype, const XlbbGrid* g, const XlbbDarcySweep
     long long n;
     if (dtype == XLBB_F32) n = darcy_partials_t<float>(g, s);
     else if (dtype == XLBB_F64) n = darcy_partials_t<double>(g, s);
+    else if (dtype == XLBB_F32_ACC64) n = darcy_partials_t<double, float>(g, s);
     else return fail(XLBB_EBADARG, "xlbb_darcy_sweep_partials: dtype");
     return n > INT_MAX ? fail(XLBB_EBADARG, "xlbb_darcy_sweep_partials: grid too large") : (int)n;
 }
@@ -1991,7 +2005,7 @@ int xlbb_elast_sweep_pipeline(int dtype, const XlbbGrid* g, const XlbbElastMater
 }
 
 int xlbb_darcy_sweep_pipeline(int dtype, const XlbbGrid* g, const XlbbDarcySweep* s) {
-    if (!grid_ok(g) || !s || (dtype != XLBB_F32 && dtype != XLBB_F64))
+    if (!grid_ok(g) || !s || (dtype != XLBB_F32 && dtype != XLBB_F64 && dtype != XLBB_F32_ACC64))
         return fail(XLBB_EBADARG, "xlbb_darcy_sweep_pipeline: bad argument");
     const XlbbSweepConfig c = effective_cfg(1, dtype);
     const bool push = push_eligible<DarcyPhys<double>>(darcy_args<DarcyPhys<double>>(g, s));
@@ -2007,6 +2021,7 @@ int xlbb_darcy_sweep(int dtype, const XlbbGrid* g, const XlbbDarcySweep* s, void
 
     if (dtype == XLBB_F32) return darcy_sweep_t<float>(g, s, XLBB_STREAM(stream));
     if (dtype == XLBB_F64) return darcy_sweep_t<double>(g, s, XLBB_STREAM(stream));
+    if (dtype == XLBB_F32_ACC64) return darcy_sweep_t<double, float>(g, s, XLBB_STREAM(stream));
     return fail(XLBB_EUNSUPPORTED, "xlbb_darcy_sweep: dtype");
 }
 

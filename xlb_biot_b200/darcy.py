@@ -44,8 +44,8 @@ class AdvectionDiffusionReactionBGK(LBMBase):
 
     def _compile_rules(self):
         L = self._layout
-        self._pc = compile_rules(self.BCs, L.nx, L.ny, 9, self._dtype, L.device, step="PostCollision")
-        self._ps = compile_rules(self.BCs, L.nx, L.ny, 9, self._dtype, L.device, step="PostStreaming")
+        self._pc = compile_rules(self.BCs, L.nx, L.ny, 9, self._rule_dtype, L.device, step="PostCollision")
+        self._ps = compile_rules(self.BCs, L.nx, L.ny, 9, self._rule_dtype, L.device, step="PostStreaming")
         self._grad_rules = compile_rules(self.BCs, L.nx, L.ny, 9, self._dtype, L.device, names=GRADIENT_BC_NAMES)
 
     def gradient_rules(self, nx, ny, dtype=None):
@@ -133,14 +133,14 @@ class AdvectionDiffusionReactionBGK(LBMBase):
         if sumsq:
             # a buffer for the largest launch shape; the reduction reads the
             # partials of the launch this sweep takes
-            n_max = _lib.check(_lib.lib().xlbb_darcy_sweep_ctas(self._dcode, L.grid()), "xlbb_darcy_sweep_ctas")
+            n_max = _lib.check(_lib.lib().xlbb_darcy_sweep_ctas(self._sweep_code, L.grid()), "xlbb_darcy_sweep_ctas")
             if self._partials.numel() < n_max:
                 self._partials = torch.empty(n_max, dtype=torch.float64, device=L.device)
         s = self._sweep_args(f, out, external_source, sumsq, resid, homogeneous)
         if sumsq:
-            self._n_partials = _lib.check(_lib.lib().xlbb_darcy_sweep_partials(self._dcode, L.grid(), s),
+            self._n_partials = _lib.check(_lib.lib().xlbb_darcy_sweep_partials(self._sweep_code, L.grid(), s),
                                           "xlbb_darcy_sweep_partials")
-        _lib.check(_lib.lib().xlbb_darcy_sweep(self._dcode, L.grid(), s, _lib.stream_ptr()), "xlbb_darcy_sweep")
+        _lib.check(_lib.lib().xlbb_darcy_sweep(self._sweep_code, L.grid(), s, _lib.stream_ptr()), "xlbb_darcy_sweep")
         return out
 
     def _sweep_args(self, f, out, external_source=None, sumsq=False, resid=None, homogeneous=False):
@@ -160,8 +160,8 @@ class AdvectionDiffusionReactionBGK(LBMBase):
         if "_hom_rules" not in self.__dict__:
             from .refine import homogeneous_rules
             L = self._layout
-            self._hom_rules = (homogeneous_rules(self._pc, L.ny, L.dtype, L.device),
-                               homogeneous_rules(self._ps, L.ny, L.dtype, L.device))
+            self._hom_rules = (homogeneous_rules(self._pc, L.ny, self._rule_dtype, L.device),
+                               homogeneous_rules(self._ps, L.ny, self._rule_dtype, L.device))
         return self._hom_rules
 
     def sweep_pipeline(self, f=None, out=None):
@@ -170,7 +170,7 @@ class AdvectionDiffusionReactionBGK(LBMBase):
         L = self._layout
         f = L.empty(9) if f is None else f
         out = L.empty(9) if out is None else out
-        return _lib.check(_lib.lib().xlbb_darcy_sweep_pipeline(self._dcode, L.grid(), self._sweep_args(f, out)),
+        return _lib.check(_lib.lib().xlbb_darcy_sweep_pipeline(self._sweep_code, L.grid(), self._sweep_args(f, out)),
                           "xlbb_darcy_sweep_pipeline")
 
     def step(self, f_poststreaming, timestep, return_fpost=False, external_source=None):

@@ -15,7 +15,8 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._common import gathered, iterate_to_tolerance, make_policy, print_parameters, require_finite, set_precisions
+from ._common import (gathered, iterate_to_tolerance, make_policy, print_parameters, require_finite,
+                      set_precisions, storage_and_sweep_dtypes)
 from .bc_compile import apply_rules_device, compile_rules
 from .boundary_conditions import (BoundaryCondition, _at_add, _at_set, _take, grid_mask, solid_halo_voxels)
 from .fields import Layout, torch_dtype
@@ -92,7 +93,9 @@ class LBMElasticity:
         self.show_simulation_parameters()
         self.gridInfo = {"nx": self.nx, "ny": self.ny, "nz": self.nz, "dim": self.lattice.d, "lattice": self.lattice}
         self.sharding = None
-        self._dtype = torch_dtype(self.precisionPolicy.compute_dtype)
+        # storage type of the fields; under 'f64/f32' every sweep computes in
+        # FP64 (dtype code XLBB_F32_ACC64, FP64 rule constants) on FP32 fields
+        self._dtype, self._acc64_all = storage_and_sweep_dtypes(self.precisionPolicy)
         self._dcode = _lib.dtype_code(self._dtype)
         # Extension: ``coarsest_precision="f64"`` runs the coarsest multigrid level
         # in FP64 under FP32 levels (transfers convert in the kernels).
@@ -348,13 +351,21 @@ class LBMElasticity:
         for level in range(self.levels):
             bcs = self.BCs if level == 0 else self.BCs_MG[level]
             L = self._layouts[level]
-            pc = compile_rules(bcs, L.nx, L.ny, 8, L.dtype, L.device, step="PostCollision")
-            ps = compile_rules(bcs, L.nx, L.ny, 8, L.dtype, L.device, step="PostStreaming")
+            rd = self._sweep_rule_dtype(L)
+            pc = compile_rules(bcs, L.nx, L.ny, 8, rd, L.device, step="PostCollision")
+            ps = compile_rules(bcs, L.nx, L.ny, 8, rd, L.device, step="PostStreaming")
             self._rules.append((pc, ps))
         if self._res64:      # FP64 rule constants of the FP64-arithmetic residual sweep
             L = self._layouts[0]
             self._rules_acc64 = (compile_rules(self.BCs, L.nx, L.ny, 8, torch.float64, L.device, step="PostCollision"),
                                  compile_rules(self.BCs, L.nx, L.ny, 8, torch.float64, L.device, step="PostStreaming"))
+
+    def _sweep_acc64(self, L):
+        """Whether sweeps on a level of layout L compute in FP64 on FP32 storage."""
+        return self._acc64_all and L.dtype == torch.float32
+
+    def _sweep_rule_dtype(self, L):
+        return torch.float64 if self._sweep_acc64(L) else L.dtype
 
     def distributed_array_init(self, shape, type, init_val=0, sharding=None):
         """A device field of ``shape`` filled with ``init_val`` (``:438-458``)."""
@@ -575,14 +586,15 @@ class LBMElasticity:
         out = L.empty(8) if out is None else out
         if fext is not None and not L.conforms(fext, 2):
             fext = L.field(fext, 2)      # e.g. a coupling force computed in another precision
-        code = _lib.XLBB_F32_ACC64 if acc64 else _lib.dtype_code(L.dtype)
+        acc64_all = self._sweep_acc64(L)
+        code = _lib.XLBB_F32_ACC64 if (acc64 or acc64_all) else _lib.dtype_code(L.dtype)
         if sumsq:
             # a buffer for the largest launch shape; the reduction reads the
             # partials of the launch this sweep takes
             n_max = _lib.check(_lib.lib().xlbb_elast_sweep_ctas(code, L.grid()), "xlbb_elast_sweep_ctas")
             if self._partials.numel() < n_max:
                 self._partials = torch.empty(n_max, dtype=torch.float64, device=L.device)
-        pc, ps = self._rules_acc64 if acc64 else self._rules[level]
+        pc, ps = self._rules_acc64 if (acc64 and not acc64_all) else self._rules[level]
         force = self.force
         if homogeneous:
             pc, ps = self._homogeneous_rules(level)
@@ -609,7 +621,8 @@ class LBMElasticity:
         if level not in cache:
             from .refine import homogeneous_rules
             L = self._L(level)
-            cache[level] = tuple(homogeneous_rules(r, L.ny, L.dtype, L.device) for r in self._rules[level])
+            cache[level] = tuple(homogeneous_rules(r, L.ny, self._sweep_rule_dtype(L), L.device)
+                                 for r in self._rules[level])
         return cache[level]
 
     def solve_refined(self, f=None, tol=1e-8, inner_tol=1e-5, check_every=200, max_sweeps=10 ** 7, max_outer=30,

@@ -29,6 +29,8 @@ class _FluidSim(LBMBase):
 
     def __init__(self, **kwargs):
         super().__init__(**kwargs)
+        if self._acc64:
+            raise NotImplementedError("the fluid models compute in their storage type: use 'f32/f32' or 'f64/f64'")
         if self.lattice.q != 9 or self.lattice.d != 2:
             raise NotImplementedError("the fluid models run on the D2Q9 lattice")
         if self.force is not None:
