@@ -532,10 +532,12 @@ def run_c4(args):
     import xlb_biot_b200.api as G
     from xlb_biot_b200.batched import BatchedElasticity
     from xlb_biot_b200.workloads import batch_instances
-    tol, max_cycles = 1e-6, 200
+    target, max_cycles = 1e-6, 200
+    tol = 0.5 * target            # the estimate tracks the error within ~10 %: stop a factor 2 below the target
     sizes, lams, mus, forces = batch_instances(count=args.instances)
     b = BatchedElasticity(sizes, lams, mus, forces, levels="auto", precision="f32/f32", coarsest_precision="f64",
-                          residual_precision="f64")
+                          residual_precision="f64", persistent_tail=args.tail_smem > 0,
+                          tail_smem=max(args.tail_smem, 1))
     b.solve(tol=1e-2, max_cycles=3)                                   # warm-up + graph capture
     (cycles, est), secs = _timed(lambda: b.solve(tol=tol, max_cycles=max_cycles, criterion="error"))
     lu = b.lattice_updates_per_cycle() * cycles
@@ -580,12 +582,18 @@ def run_c4(args):
     single_sps = len(sample) / t_single
     line = {"workload": "c4_batched_mg_512_instances", "metric": "solves/s", "value": args.instances / secs,
             "unit": "solves/s", "instances": args.instances, "vcycles": cycles, "seconds": secs,
-            "criterion": "estimated relative error < 1e-6 (coarse-correction norm x rho / (1 - rho))",
+            "criterion": "estimated relative error < 5e-7 (coarse-correction norm x rho / (1 - rho)), "
+                         "for a measured error <= 1e-6",
+            "persistent_tail": {"tail_smem_bytes": args.tail_smem, "batched_levels": b.batched_depth,
+                                "tail_start_level_counts": {str(k): int(v) for k, v in
+                                                            zip(*np.unique(b.tail_start, return_counts=True))}},
             "instances_at_rounding_floor": int(b.stalled.sum()),
             "vcycles_per_instance": {"min": int(b.converged_at.min()), "median": float(np.median(b.converged_at)),
                                      "max": int(b.converged_at.max())},
             "displacement_rel_err_vs_fp64": {"max": float(err.max()), "median": float(np.median(err)),
-                                             "count_above_1e-6": int((err > 1e-6).sum())},
+                                             "count_above_1e-6": int((err > target).sum()),
+                                             "count_above_1e-6_at_rounding_floor":
+                                                 int(((err > target) & b.stalled).sum())},
             "fp64_oracle_vcycles": cyc64, "glups": lu / secs / 1e9,
             "single_instance_loop": {"solves_per_s": single_sps, "sample": len(sample),
                                      "mean_vcycles": cyc_single / len(sample)},
@@ -648,7 +656,8 @@ def run_c4vcycle(args):
     from xlb_biot_b200.workloads import batch_instances
     sizes, lams, mus, forces = batch_instances(count=args.instances)
     b = BatchedElasticity(sizes, lams, mus, forces, levels="auto", precision="f32/f32", coarsest_precision="f64",
-                          residual_precision="f64")
+                          residual_precision="f64", persistent_tail=args.tail_smem > 0,
+                          tail_smem=max(args.tail_smem, 1))
     b.reset()
     for _ in range(max(3, args.warmup)):
         b.vcycle()
@@ -657,6 +666,7 @@ def run_c4vcycle(args):
     print(json.dumps({"workload": "c4_batched_vcycle", "metric": "ms per V-cycle", "value": t / args.steps * 1e3,
                       "unit": "ms", "higher_is_better": False, "vcycles": args.steps,
                       "launches_per_vcycle": b.launches_per_cycle, "levels": b.levels,
+                      "tail_smem_bytes": args.tail_smem, "batched_levels": b.batched_depth,
                       "glups": lu * args.steps / t / 1e9}), flush=True)
     return 0
 
@@ -964,6 +974,8 @@ def main():
                     help="darcy: the headline line; c1/c3/c4/c5: the other configurations (one JSON line each)")
     ap.add_argument("--biot-steps", type=int, default=100)
     ap.add_argument("--instances", type=int, default=512)
+    ap.add_argument("--tail-smem", type=int, default=100 * 1024,
+                    help="shared-memory budget (bytes) of the batched persistent multigrid tail; 0: no tail")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -377,6 +377,37 @@ int xlbb_batched_prolong_add_map(int dtype_fine, int dtype_coarse, const XlbbBat
 int xlbb_segment_sum(const double* parts, const int* begin_dev, int nseg, double* out, void* stream);
 
 /*
+ * Persistent multigrid tail of a periodic batch (the recursion of
+ * LBMElasticity._mg_step, src/elasticity.py:1221-1312, below a level): one
+ * launch finishes the V-cycle of every listed instance from its tail's top
+ * level down to its coarsest level and back, one CTA per instance with all of
+ * the tail's levels in shared memory (CTA barriers only).  Per level above the
+ * last: k_smooth damped sweeps (1 - gamma, gamma) from zero, the residual
+ * sweep, 2 x 2 block-sum restriction, the level below, injection of its
+ * correction, k_smooth damped sweeps; the last level: 2 k_smooth damped
+ * sweeps, the first from zero.  Reads each record's top-level right-hand
+ * side `resid` and writes its correction `f_out` (both in the top level's
+ * dtype: dtype_coarse when the tail has one level, else dtype); the results
+ * equal the level-by-level batched launches'.  dtype / dtype_coarse:
+ * (XLBB_F32, XLBB_F32), (XLBB_F32, XLBB_F64) or (XLBB_F64, XLBB_F64).
+ * smem_bytes: the largest xlbb_batched_tail_smem of the records (at most the
+ * device's opt-in shared memory per block); a record that needs more, or
+ * whose grid is not divisible by 2^(levels - 1), is skipped and the device
+ * status word set to XLBB_EBADARG.  k_smooth even, >= 2.
+ */
+typedef struct {
+    const void* resid;       /* top level's right-hand side (8 planes)             */
+    void* f_out;             /* top level's correction (8 planes)                  */
+    int nx, ny, pitch;       /* top level grid and row pitch (elements)            */
+    long long plane;         /* plane stride (elements)                            */
+    int levels;              /* levels of the tail, 1 .. 12 (the last: the coarsest) */
+    double lam, mu;          /* Lame parameters (lattice units)                    */
+} XlbbBatchTail;
+int xlbb_batched_tail_smem(int dtype, int dtype_coarse, int nx, int ny, int levels);
+int xlbb_batched_tail(int dtype, int dtype_coarse, const XlbbBatchTail* tails_dev, int count, int smem_bytes,
+                      double gamma, int k_smooth, void* stream);
+
+/*
  * Adjoints (transposed linear maps) for gradients of a misfit with respect to
  * per-cell material fields.  No counterpart in the reference (which has no
  * adjoint).  Each call takes the adjoint of a forward kernel's output and

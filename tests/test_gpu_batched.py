@@ -185,3 +185,32 @@ def test_four_column_kernel_skips_instances_that_do_not_qualify():
     torch.cuda.synchronize()
     assert autotune.device_status(reset=True) == -1        # XLBB_EBADARG
     assert bool((dst == 7.0).all())
+
+
+@pytest.mark.parametrize("prec,coarse", [("f64/f64", None), ("f32/f32", None), ("f32/f32", "f64")])
+@pytest.mark.parametrize("budget", [40 * 1024, 128 * 1024])
+def test_persistent_tail_equals_level_by_level(prec, coarse, budget):
+    """The coarse levels finished by one launch (a CTA per instance, levels in
+    shared memory) give the level-by-level launches' populations and residual
+    norms bit for bit, with fewer launches per V-cycle."""
+    from xlb_biot_b200 import autotune
+    from xlb_biot_b200.batched import BatchedElasticity
+    from xlb_biot_b200.workloads import batch_instances
+    sizes, lams, mus, forces = batch_instances(count=7, sizes=(32, 48, 64, 96, 128), seed=5)
+    kw = dict(levels="auto", precision=prec, coarsest_precision=coarse)
+    a = BatchedElasticity(sizes, lams, mus, forces, persistent_tail=True, tail_smem=budget, **kw)
+    b = BatchedElasticity(sizes, lams, mus, forces, persistent_tail=False, **kw)
+    assert a.tail is not None and b.tail is None
+    assert all(1 <= t <= lv for t, lv in zip(a.tail_start, a.instance_levels))
+    autotune.device_status(reset=True)
+    a.reset()
+    b.reset()
+    for _ in range(3):
+        a.vcycle()
+        b.vcycle()
+    torch.cuda.synchronize()
+    assert autotune.device_status(reset=True) == 0
+    assert a.launches_per_cycle < b.launches_per_cycle
+    assert torch.equal(a.norm2, b.norm2)
+    for i in range(len(sizes)):
+        assert torch.equal(a.populations(i), b.populations(i)), i

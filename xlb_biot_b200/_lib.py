@@ -87,6 +87,12 @@ class ElastSweepAdjoint(ctypes.Structure):
                 ("b", ctypes.c_double), ("pc", Rules), ("ps", Rules)]
 
 
+class BatchTail(ctypes.Structure):
+    _fields_ = [("resid", ctypes.c_void_p), ("f_out", ctypes.c_void_p), ("nx", ctypes.c_int), ("ny", ctypes.c_int),
+                ("pitch", ctypes.c_int), ("plane", ctypes.c_longlong), ("levels", ctypes.c_int),
+                ("lam", ctypes.c_double), ("mu", ctypes.c_double)]
+
+
 class DarcySweepAdjoint(ctypes.Structure):
     _fields_ = [("lam_out", ctypes.c_void_p), ("lam_f", ctypes.c_void_p), ("lam_source", ctypes.c_void_p),
                 ("g_omega", ctypes.c_void_p), ("f_in", ctypes.c_void_p), ("omega", ctypes.c_double),
@@ -117,6 +123,8 @@ SIGNATURES = {
     "xlbb_restrict": (I, [I, I, PG, PG, I, I, I, I, I, P, P, P]),
     "xlbb_prolong_add": (I, [I, I, PG, PG, I, I, I, I, I, P, P, P]),
     "xlbb_reduce_sum": (I, [P, I, P, P]),
+    "xlbb_batched_tail_smem": (I, [I, I, I, I, I]),
+    "xlbb_batched_tail": (I, [I, I, P, I, I, D, I, P]),
     "xlbb_wait_selftest": (I, [ctypes.c_uint, P, P]),
     "xlbb_sumsq": (I, [I, PG, I, P, I, I, I, I, P, P]),
     "xlbb_sumsq_ctas": (I, [PG]),

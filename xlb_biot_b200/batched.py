@@ -105,10 +105,15 @@ class BatchedElasticity:
     ``residual_precision="f64"`` computes the level-0 residual sweep of an FP32
     batch in FP64 arithmetic (FP32 storage).  ``vectorized``: FP32 launches
     whose instances all have widths divisible by 4 use the four-column kernel
-    (``xlbb_batched_elast_sweep4``; same results)."""
+    (``xlbb_batched_elast_sweep4``; same results).  ``persistent_tail``: from
+    the top-most level where an instance's remaining levels fit in
+    ``tail_smem`` bytes of shared memory, its V-cycle is finished by one
+    launch for all instances (``xlbb_batched_tail``: a CTA per instance, the
+    levels in shared memory; same results as the level-by-level launches)."""
 
     def __init__(self, sizes, lams, mus, forces, levels=5, gamma=0.75, k_smooth=2, precision="f32/f32",
-                 coarsest_precision=None, residual_precision=None, strip_rows=16, ctas_per_sm=4, vectorized=True):
+                 coarsest_precision=None, residual_precision=None, strip_rows=16, ctas_per_sm=4, vectorized=True,
+                 persistent_tail=True, tail_smem=100 * 1024):
         _lib.require_cuda()
         lib = _lib.lib()
         if k_smooth % 2:
@@ -140,6 +145,22 @@ class BatchedElasticity:
 
         def dtype_of(g, l):
             return coarse_dt if l == lv[g] - 1 else dt
+
+        # tail_start[g]: the first level of instance g handled by the persistent
+        # tail (lv[g]: none); the level-by-level launches stop above it
+        self.tail_start = list(lv)
+        if persistent_tail:
+            for g, (nx, ny) in enumerate(sizes):
+                for l in range(1, lv[g]):
+                    b = lib.xlbb_batched_tail_smem(_lib.dtype_code(dt), _lib.dtype_code(coarse_dt), nx >> l, ny >> l,
+                                                   lv[g] - l)
+                    if 0 < b <= tail_smem:
+                        self.tail_start[g] = l
+                        break
+        self.batched_depth = max(self.tail_start)
+
+        def act(g, l):
+            return self.tail_start[g] > l
 
         # groups[l]: dtype -> instance ids at level l;  deeper[l]: ids that recurse below l
         self.groups, self.deeper, self.shapes = [], [], []
@@ -197,6 +218,9 @@ class BatchedElasticity:
         for l in range(self.levels):
             parts = []
             for d, ids in self.groups[l].items():
+                ids = [g for g in ids if act(g, l)]
+                if not ids:
+                    continue
                 if vectorized and d == torch.float32:
                     q4 = [g for g in ids if self.shapes[l][g][0] % 4 == 0]
                     parts += [(d, p) for p in (q4, [g for g in ids if g not in set(q4)]) if p]
@@ -206,8 +230,9 @@ class BatchedElasticity:
             self.smooth_yx.append([launch(l, ids, d, self.Y[l][d], self.X[l][d]) for d, ids in parts])
             if l < self.levels - 1:
                 acc64 = l == 0 and residual_precision == "f64" and dt == torch.float32
-                self.res.append(launch(l, self.deeper[l], dt, self.X[l][dt], self.RES[l], want_begin=(l == 0),
-                                       code=_lib.XLBB_F32_ACC64 if acc64 else None))
+                rids = [g for g in self.deeper[l] if act(g, l)]
+                self.res.append(launch(l, rids, dt, self.X[l][dt], self.RES[l], want_begin=(l == 0),
+                                       code=_lib.XLBB_F32_ACC64 if acc64 else None) if rids else None)
         if self.deeper[0] != list(range(self.n)):
             raise AssertionError("every instance recurses below level 0")
         # per-instance ranges of the level-0 residual sweep's partials (a partial per warp of each tile)
@@ -220,7 +245,7 @@ class BatchedElasticity:
         self._corr_parts = None       # sized below: 2 doubles per block of the level-0 prolongation maps
 
         def transfers(l, fine, coarse_arenas, d_coarse, src_is_res):
-            ids = [g for g in self.deeper[l] if dtype_of(g, l + 1) == d_coarse]
+            ids = [g for g in self.deeper[l] if dtype_of(g, l + 1) == d_coarse and act(g, l)]
             if not ids:
                 return None
             recs = (_lib.BatchTransfer * len(ids))()
@@ -248,6 +273,25 @@ class BatchedElasticity:
         # row r of corr2 belongs to instance _corr_ids[r] (transfer-list order)
         self._corr_ids = np.asarray([g for t in self.t_prolong[0] for g in t[4]])
         self._corr_parts = torch.zeros(2 * max(t[6] for t in self.t_prolong[0]), dtype=torch.float64, device=dev)
+        # the persistent tail's records: top-level right-hand side and correction of every tail instance
+        self.tail = None
+        tail_ids = [g for g in range(self.n) if self.tail_start[g] < lv[g]]
+        if tail_ids:
+            recs = (_lib.BatchTail * len(tail_ids))()
+            smem = 0
+            for k, g in enumerate(tail_ids):
+                t = self.tail_start[g]
+                d = dtype_of(g, t)
+                R, X = self.R[t][d], self.X[t][d]
+                nx, ny = self.shapes[t][g]
+                recs[k] = _lib.BatchTail(R.ptr(g), X.ptr(g), nx, ny, X.pitch[X.pos[g]], X.plane[X.pos[g]],
+                                         lv[g] - t, self.lams[g], self.mus[g])
+                if R.pitch[R.pos[g]] != X.pitch[X.pos[g]] or R.plane[R.pos[g]] != X.plane[X.pos[g]]:
+                    raise AssertionError("tail right-hand side and correction differ in layout")
+                smem = max(smem, lib.xlbb_batched_tail_smem(_lib.dtype_code(dt), _lib.dtype_code(coarse_dt),
+                                                            nx, ny, lv[g] - t))
+            buf = torch.as_tensor(np.frombuffer(bytes(recs), dtype=np.uint8).copy(), device=dev)
+            self.tail = (buf, len(tail_ids), smem, _lib.dtype_code(dt), _lib.dtype_code(coarse_dt))
         self.launches_per_cycle = 0
         self.graph = None
 
@@ -270,9 +314,17 @@ class BatchedElasticity:
             for ln in (self.smooth_xy[l] if k % 2 == 0 else self.smooth_yx[l]):
                 self._sweep(l, ln, 1.0 - g, g, zero_in=from_zero and k == 0)
 
+    def _tail(self):
+        buf, count, smem, dcode, ccode = self.tail
+        _lib.check(_lib.lib().xlbb_batched_tail(dcode, ccode, ctypes.c_void_p(buf.data_ptr()), count, smem,
+                                                self.gamma, self.k_smooth, _lib.stream_ptr()), "xlbb_batched_tail")
+        self.launches_per_cycle += 1
+
     def _level(self, l):
+        """Level l of every instance still on the level-by-level launches; at
+        the deepest such level the persistent tail runs the rest."""
         self._smooth(l, from_zero=l > 0)
-        if l < self.levels - 1:
+        if l < self.levels - 1 and self.res[l] is not None:
             self._sweep(l, self.res[l], 1.0, -1.0, sumsq=(l == 0))
             if l == 0:
                 _lib.check(_lib.lib().xlbb_segment_sum(
@@ -283,7 +335,11 @@ class BatchedElasticity:
                 _lib.check(_lib.lib().xlbb_batched_restrict(cf, cc, ctypes.c_void_p(buf.data_ptr()), cnt,
                                                             _lib.stream_ptr()), "xlbb_batched_restrict")
                 self.launches_per_cycle += 1
+        if l + 1 < self.batched_depth:
             self._level(l + 1)          # its correction starts from zero (first sweep: zero input)
+        elif self.tail is not None:
+            self._tail()
+        if l < self.levels - 1 and self.res[l] is not None:
             for k, (buf, cnt, cf, cc, _, bmap, nblocks, bbegin) in enumerate(self.t_prolong[l]):
                 if l == 0:   # instances of transfer list k occupy rows offset.. of corr2
                     off = sum(t[1] for t in self.t_prolong[0][:k])

@@ -1900,6 +1900,8 @@ __global__ void segment_sum_kernel(const double* parts, const int* begin, int ni
 
 }  // namespace xlbb
 
+#include "xlbb_tail.cuh"
+
 using namespace xlbb;
 
 #define XLBB_STREAM(s) (static_cast<cudaStream_t>(s))
@@ -2480,6 +2482,50 @@ int xlbb_batched_prolong_add_map(int dtype_fine, int dtype_coarse, const XlbbBat
     if (norms) launch_k(pair_segment_sum_kernel, ninst, 256, 0, st, (const double*)parts, nblocks, begin_dev, ninst,
                         norms);
     return check_launch("xlbb_batched_prolong_add_map");
+}
+
+int xlbb_batched_tail_smem(int dtype, int dtype_coarse, int nx, int ny, int levels) {
+    if (nx < 1 || ny < 1 || levels < 1 || levels > TAIL_MAX_LEVELS || (nx >> (levels - 1)) < 1 ||
+        (ny >> (levels - 1)) < 1)
+        return fail(XLBB_EBADARG, "xlbb_batched_tail_smem: bad argument");
+    size_t b;
+    if (dtype == XLBB_F32 && dtype_coarse == XLBB_F32) b = tail_smem_bytes<float, float>(nx, ny, levels);
+    else if (dtype == XLBB_F32 && dtype_coarse == XLBB_F64) b = tail_smem_bytes<float, double>(nx, ny, levels);
+    else if (dtype == XLBB_F64 && dtype_coarse == XLBB_F64) b = tail_smem_bytes<double, double>(nx, ny, levels);
+    else return fail(XLBB_EUNSUPPORTED, "xlbb_batched_tail_smem: dtype pair");
+    return b > (size_t)INT_MAX ? fail(XLBB_EBADARG, "xlbb_batched_tail_smem: too large") : (int)b;
+}
+
+int xlbb_batched_tail(int dtype, int dtype_coarse, const XlbbBatchTail* tails_dev, int count, int smem_bytes,
+                      double gamma, int k_smooth, void* stream) {
+    if (!tails_dev || count <= 0 || smem_bytes <= 0 || k_smooth < 2 || k_smooth % 2)
+        return fail(XLBB_EBADARG, "xlbb_batched_tail: bad argument");
+    static int optin = 0;
+    if (optin == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) optin = 0;
+    }
+    if (smem_bytes > optin)
+        return fail(XLBB_EBADARG, "xlbb_batched_tail: smem_bytes above the device's shared memory per block");
+#define XLBB_TAIL(T_, TC_)                                                                                    \
+    {                                                                                                         \
+        static int configured = 0;                                                                            \
+        auto k = batched_tail_kernel<T_, TC_>;                                                                \
+        if (smem_bytes > configured) {                                                                        \
+            if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes) != cudaSuccess) \
+                return fail(XLBB_ELAUNCH, "xlbb_batched_tail: shared memory attribute");                      \
+            configured = smem_bytes;                                                                          \
+        }                                                                                                     \
+        launch_k(k, count, TAIL_THREADS, (size_t)smem_bytes, XLBB_STREAM(stream), tails_dev, gamma, k_smooth,  \
+                 (size_t)smem_bytes);                                                                         \
+    }
+    if (dtype == XLBB_F32 && dtype_coarse == XLBB_F32) XLBB_TAIL(float, float)
+    else if (dtype == XLBB_F32 && dtype_coarse == XLBB_F64) XLBB_TAIL(float, double)
+    else if (dtype == XLBB_F64 && dtype_coarse == XLBB_F64) XLBB_TAIL(double, double)
+    else return fail(XLBB_EUNSUPPORTED, "xlbb_batched_tail: dtype pair");
+#undef XLBB_TAIL
+    return check_launch("xlbb_batched_tail");
 }
 
 int xlbb_segment_sum(const double* parts, const int* begin_dev, int nseg, double* out, void* stream) {
