@@ -12,7 +12,7 @@ import time
 
 import torch
 
-from ._common import gathered
+from ._common import gathered, require_finite
 
 
 class DivGradForce:
@@ -326,6 +326,7 @@ class LBMPoroelasticity:
                 f_elasticity, r = el.step(f_elasticity, timestep, False, force, nonlinear_force=nonlinear_force)
                 self.last_inner_cycles = k + 1
                 r = float(r)
+                require_finite(r, "level-0 residual norm of the inner elasticity solve", k + 1)
                 r0 = r if r0 is None else r0
                 if r0 == 0.0 or r / r0 < self.elasticityTol:
                     break

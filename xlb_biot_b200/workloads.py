@@ -88,7 +88,8 @@ EXAMPLE_E, EXAMPLE_NU = 0.11, 0.8     # material of the reference's periodic exa
 
 
 def periodic_biot_1024(m, n=1024, levels=5, lam=None, mu=None, alpha=1.0, K=0.1, precision="f32/f32",
-                       darcy_precision=None, coarsest_precision=None, tol=None, max_cycles=8):
+                       darcy_precision=None, coarsest_precision=None, tol=None, max_cycles=8,
+                       residual_precision=None):
     """Periodic Biot consolidation with the initial pressure sin 2pi x sin 2pi y:
     elasticity with an L-level V-cycle per time step (``max_cycles`` cycles, or
     until the residual fell by ``tol``), Darcy with K = 0.1 (omega = 1.25),
@@ -128,6 +129,8 @@ def periodic_biot_1024(m, n=1024, levels=5, lam=None, mu=None, alpha=1.0, K=0.1,
         kw["coarsest_precision"] = coarsest_precision
     if tol is not None:
         kw["elasticity_tol"] = tol
+    if residual_precision:
+        kw["residual_precision"] = residual_precision
     return PB(**kw)
 
 
