@@ -260,6 +260,19 @@ int xlbb_elast_moments(int dtype, const XlbbGrid* g, const XlbbElastMaterial* ma
 int xlbb_elast_divgrad(int dtype, const XlbbGrid* g, const XlbbElastMaterial* mat, double div_scale,
                        const void* f, double scale, const XlbbRules* rules, const void* base,
                        void* out, void* stream);
+/*
+ * A poroelastic smoothing sweep in one kernel: xlbb_elast_divgrad of the
+ * sweep's own input s->f_in (base = s->fext, gradient rules grad_rules)
+ * handed to xlbb_elast_sweep as its external force, on the collide-and-push
+ * launch -- the smoothing and residual sweeps of _mg_step with the nonlinear
+ * force of src/poroelasticity.py:324 (src/elasticity.py:1258-1305), the same
+ * values bit for bit, one launch instead of two and no force field in memory.
+ * XLBB_F32 / XLBB_F64 only; XLBB_EUNSUPPORTED for fused sums (s->sumsq),
+ * s->div_out, or post-streaming rules without push words (use the two calls).
+ */
+int xlbb_elast_sweep_divgrad(int dtype, const XlbbGrid* g, const XlbbElastMaterial* mat,
+                             const XlbbElastSweep* s, double div_scale, double scale,
+                             const XlbbRules* grad_rules, void* stream);
 
 /* Elasticity equilibrium (LBMElasticity.equilibrium :909-957). */
 int xlbb_elast_equilibrium(int dtype, const XlbbGrid* g, const XlbbElastMaterial* mat,

@@ -117,6 +117,8 @@ SIGNATURES = {
     "xlbb_darcy_sweep_residual_noalloc": (I, [I, PG, ctypes.POINTER(DarcySweep), P, P]),
     "xlbb_darcy_gradient": (I, [I, PG, P, D, ctypes.POINTER(Rules), P, P, P]),
     "xlbb_elast_divgrad": (I, [I, PG, ctypes.POINTER(ElastMaterial), D, P, D, ctypes.POINTER(Rules), P, P, P]),
+    "xlbb_elast_sweep_divgrad": (I, [I, PG, ctypes.POINTER(ElastMaterial), ctypes.POINTER(ElastSweep), D, D,
+                                     ctypes.POINTER(Rules), P]),
     "xlbb_elast_moments": (I, [I, PG, ctypes.POINTER(ElastMaterial), P, P, P, P, P, P, D, P]),
     "xlbb_elast_equilibrium": (I, [I, PG, ctypes.POINTER(ElastMaterial), P, P, P, P, P, P]),
     "xlbb_darcy_moments": (I, [I, PG, P, D, P, P, P, P, P, P]),

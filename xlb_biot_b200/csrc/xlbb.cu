@@ -860,6 +860,58 @@ __global__ void __launch_bounds__(256) elast_divgrad_kernel(SweepGeom G, ElastMa
     out[o + G.plane] = gy;
 }
 
+// A damped smoothing sweep of the poroelastic multigrid in ONE kernel: the
+// coupling force base + G(div f) of the sweep's own input (the stages of
+// elast_divgrad_kernel: divergence of a 32 x 8 tile plus halo in shared
+// memory, the gradient stencil with its rules) is handed to the
+// collide-and-push sweep of the tile's cells as its external force, without
+// the force's round trip through memory or a second launch.  The operations
+// are those of xlbb_elast_divgrad followed by xlbb_elast_sweep on the
+// collide-and-push launch, so the results are the same bit for bit.
+template <typename T, bool RESID>
+__global__ void __launch_bounds__(256) elast_divgrad_push_kernel(const typename ElastPhys<T, RESID>::Args p, T lam,
+                                                                 T mu, T div_scale, T scale,
+                                                                 RulesView<T, 9> grules, const T* base) {
+    grid_dep_wait();
+    constexpr int BX = 32, BY = 8;
+    __shared__ T q[BY + 2][BX + 2];
+    const SweepGeom& G = p.geom;
+    const int x0 = blockIdx.x * BX, y0 = blockIdx.y * BY;
+    for (int k = threadIdx.y * BX + threadIdx.x; k < (BX + 2) * (BY + 2); k += BX * BY) {
+        const int lx = k % (BX + 2), ly = k / (BX + 2);
+        const int xs = ((x0 + lx - 1) % G.nx + G.nx) % G.nx, ys = ((y0 + ly - 1) % G.ny + G.ny) % G.ny;
+        q[ly][lx] = elast_div_at<T>(p.f_in, G.plane, (size_t)ys * G.pitch + xs, p.mat, lam, mu, div_scale);
+    }
+    __syncthreads();
+    const int x = x0 + threadIdx.x, y = y0 + threadIdx.y;
+    if (x >= G.nx || y >= G.ny) return;
+    T v[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) v[i] = q[threadIdx.y + 1 - cy9(i)][threadIdx.x + 1 - cx9(i)];
+    const size_t o = (size_t)y * G.pitch + x;
+    const int r = find_rule(grules, y, x);
+    if (r >= 0) {
+        const T qc = q[threadIdx.y + 1][threadIdx.x + 1];
+#pragma unroll
+        for (int d = 0; d < 9; ++d) {
+            const uint8_t code = __ldg(grules.code + (size_t)r * 9 + d);
+            v[d] = rule_value<T, 9>(code, v[d], qc, grules.cst[(size_t)r * 9 + d]);
+        }
+    }
+    T gx, gy;
+    gradient_sum<T>(v, scale, gx, gy);
+    if (base) {
+        gx = base[o] + gx;
+        gy = base[o + G.plane] + gy;
+    }
+    // as ElastPhys::load adds an external force to the static one
+    const bool hasF = p.force != nullptr;
+    push_cell<ElastPhys<T, RESID>, false>(p, y, x, [&](typename ElastPhys<T, RESID>::In& in) {
+        in.F0 = hasF ? in.F0 + gx : gx;
+        in.F1 = hasF ? in.F1 + gy : gy;
+    });
+}
+
 template <typename T>
 __global__ void elast_equilibrium_kernel(SweepGeom G, T lam, T mu, const T* lam_f, const T* mu_f, const T* eta,
                                          const T* sigma, const T* force, const T* fext, T* fo) {
@@ -2091,6 +2143,40 @@ int xlbb_elast_divgrad(int dtype, const XlbbGrid* g, const XlbbElastMaterial* ma
                  (const double*)base, (double*)out);
     else return fail(XLBB_EUNSUPPORTED, "xlbb_elast_divgrad: dtype");
     return check_launch("xlbb_elast_divgrad");
+}
+
+int xlbb_elast_sweep_divgrad(int dtype, const XlbbGrid* g, const XlbbElastMaterial* mat, const XlbbElastSweep* s,
+                             double div_scale, double scale, const XlbbRules* grad_rules, void* stream) {
+    if (!grid_ok(g) || !mat || !s || !s->f_in || !s->f_out || s->f_in == s->f_out)
+        return fail(XLBB_EBADARG, "xlbb_elast_sweep_divgrad: bad argument");
+    if (!rules_ok(s->pc, g) || !rules_ok(s->ps, g)) return fail(XLBB_EBADARG, "xlbb_elast_sweep_divgrad: incomplete rules");
+    if ((mat->mu_field == nullptr) != (mat->lam_field == nullptr))
+        return fail(XLBB_EBADARG, "xlbb_elast_sweep_divgrad: lam_field and mu_field go together");
+    if (s->sumsq || s->div_out || (dtype != XLBB_F32 && dtype != XLBB_F64))
+        return fail(XLBB_EUNSUPPORTED, "xlbb_elast_sweep_divgrad: fused sums, side outputs and mixed precision "
+                                       "take xlbb_elast_divgrad + xlbb_elast_sweep");
+    XlbbRules none = {0, nullptr, nullptr, nullptr, nullptr};
+    const XlbbRules& gr = grad_rules ? *grad_rules : none;
+    const dim3 grid((g->nx + 31) / 32, (g->ny + 7) / 8), blk(32, 8);
+#define XLBB_DGP(T_, R_)                                                                                      \
+    {                                                                                                         \
+        using Ph = ElastPhys<T_, R_>;                                                                         \
+        typename Ph::Args a = elast_args<T_, R_>(g, mat, s);                                                  \
+        if (!push_eligible<Ph>(a))                                                                            \
+            return fail(XLBB_EUNSUPPORTED, "xlbb_elast_sweep_divgrad: post-streaming rules without push words"); \
+        const T_* base = static_cast<const T_*>(s->fext);                                                     \
+        a.fext = nullptr;                                                                                     \
+        Ph::fill_ptrs(a);                                                                                     \
+        launch_k(elast_divgrad_push_kernel<T_, R_>, grid, blk, 0, XLBB_STREAM(stream), a, (T_)mat->lam,        \
+                 (T_)mat->mu, (T_)div_scale, (T_)scale, rules_view<T_, 9>(gr), base);                           \
+    }
+    if (dtype == XLBB_F32) {
+        if (s->resid) XLBB_DGP(float, true) else XLBB_DGP(float, false)
+    } else {
+        if (s->resid) XLBB_DGP(double, true) else XLBB_DGP(double, false)
+    }
+#undef XLBB_DGP
+    return check_launch("xlbb_elast_sweep_divgrad");
 }
 
 int xlbb_elast_equilibrium(int dtype, const XlbbGrid* g, const XlbbElastMaterial* mat, const void* eta,

@@ -30,13 +30,21 @@ __device__ __forceinline__ int rule_at(const RulesView<T, Q>& r, int zy, int zx)
 
 // Post-collision populations of cell (y, x): load, collide, post-collision rules
 // (the arithmetic of the row-marching sweep's collide stage).
-template <class Phys>
+// (adj: a change of the loaded inputs before the collision, e.g. a force
+// computed in the same kernel; the default changes nothing)
+struct NoAdjust {
+    template <class In>
+    __device__ void operator()(In&) const {}
+};
+
+template <class Phys, class Adj = NoAdjust>
 __device__ __forceinline__ void post_collision(const typename Phys::Args& p, int y, int x,
-                                               typename Phys::T (&fs)[Phys::Q]) {
+                                               typename Phys::T (&fs)[Phys::Q], const Adj& adj = Adj()) {
     using T = typename Phys::T;
     constexpr int Q = Phys::Q;
     typename Phys::In in;
     Phys::load(p, y, x, in);
+    adj(in);
     Phys::collide(p, y, x, in, fs);
     if (p.pc.count > 0) {
         const int r = probe_rule(load_probe(p.pc, y, x), x);
@@ -56,13 +64,13 @@ __device__ __forceinline__ void post_collision(const typename Phys::Args& p, int
 // One cell of the collide-and-push sweep; returns the FP64 squares of the
 // values it wrote (the sweep's fused sum: every output is written exactly once,
 // so the writers' sums add up to the sum over all outputs).
-template <class Phys, bool SUMSQ>
-__device__ __forceinline__ double push_cell(const typename Phys::Args& p, int y, int x) {
+template <class Phys, bool SUMSQ, class Adj = NoAdjust>
+__device__ __forceinline__ double push_cell(const typename Phys::Args& p, int y, int x, const Adj& adj = Adj()) {
     using T = typename Phys::T;
     constexpr int Q = Phys::Q;
     const SweepGeom& G = p.geom;
     T fs[Q];
-    post_collision<Phys>(p, y, x, fs);
+    post_collision<Phys>(p, y, x, fs, adj);
     const int ym = y == 0 ? G.ny - 1 : y - 1, yp = y == G.ny - 1 ? 0 : y + 1;
     const int xm = x == 0 ? G.nx - 1 : x - 1, xp = x == G.nx - 1 ? 0 : x + 1;
     // the cell's push word: directions rebuilt at their destination, own rules

@@ -64,6 +64,8 @@ class LBMElasticity:
 
     def __init__(self, **kwargs):
         self._init_kwargs = dict(kwargs)       # an FP64 twin is built from them (refine.py)
+        # the poroelastic coupling force fused into the smoothing sweeps (same values)
+        self._fused_coupling = bool(kwargs.get("fused_coupling", True))
         self.lamda = kwargs.get("lambda")
         self.mu = kwargs.get("mu")
         self.nx = kwargs.get("nx")
@@ -576,7 +578,7 @@ class LBMElasticity:
 
     # ------------------------------------------------------------------ kernels
     def _sweep(self, f, level, a=0.0, b=1.0, resid=None, fext=None, out=None, sumsq=False, div_out=None,
-               sumsq_diff=False, acc64=False, query=False, homogeneous=False):
+               sumsq_diff=False, acc64=False, query=False, homogeneous=False, coupling=None):
         """One fused sweep on ``level``; ``acc64``: FP64 arithmetic on the FP32
         level-0 fields (``residual_precision="f64"``).  ``query``: launch
         nothing, return the pipeline the library would run (diagnostic).
@@ -609,6 +611,14 @@ class LBMElasticity:
         if query:
             return _lib.check(_lib.lib().xlbb_elast_sweep_pipeline(code, L.grid(), self._mats[level], s),
                               "xlbb_elast_sweep_pipeline")
+        if coupling is not None:         # fext is the coupling force's base: the force is computed in-kernel
+            rules = coupling.darcy.gradient_rules(L.nx, L.ny, L.dtype)
+            st = _lib.lib().xlbb_elast_sweep_divgrad(code, L.grid(), self._mats[level], s, self._div_scale,
+                                                     float(coupling.scale), rules.struct(), _lib.stream_ptr())
+            if st == _lib.XLBB_EUNSUPPORTED:
+                return None
+            _lib.check(st, "xlbb_elast_sweep_divgrad")
+            return out
         if sumsq:
             self._n_partials = _lib.check(_lib.lib().xlbb_elast_sweep_partials(code, L.grid(), self._mats[level], s),
                                           "xlbb_elast_sweep_partials")
@@ -771,13 +781,14 @@ class LBMElasticity:
         fe = L.field(external_force, 2)
         g = self.gamma
         for _ in range(self.k_smooth):
-            ext = self._ext_force(fe, nonlinear_force, f, level)
-            f = self._sweep(f, level, 1.0 - g, g, resid=residual, fext=ext)
+            f = self._coupled_sweep(f, level, 1.0 - g, g, residual, fe, nonlinear_force)
         res_norm = None
         if level < self.levels - 1:
-            ext = self._ext_force(fe, nonlinear_force, f, level)
-            res = self._sweep(f, level, 1.0, -1.0, resid=residual, fext=ext, sumsq=(level == 0),
-                              acc64=(level == 0 and self._res64))
+            if level == 0:
+                ext = self._ext_force(fe, nonlinear_force, f, level)
+                res = self._sweep(f, level, 1.0, -1.0, resid=residual, fext=ext, sumsq=True, acc64=self._res64)
+            else:
+                res = self._coupled_sweep(f, level, 1.0, -1.0, residual, fe, nonlinear_force)
             if level == 0:
                 _lib.check(_lib.lib().xlbb_reduce_sum(self._partials.data_ptr(), self._n_partials,
                                                       self._scalar.data_ptr(),
@@ -788,11 +799,24 @@ class LBMElasticity:
             fc = self._mg_step(fc, timestep, level + 1, rc, nonlinear_force=nonlinear_force)
             self._prolong_add(fc, f, level)
         for _ in range(self.k_smooth):
-            ext = self._ext_force(fe, nonlinear_force, f, level)
-            f = self._sweep(f, level, 1.0 - g, g, resid=residual, fext=ext)
+            f = self._coupled_sweep(f, level, 1.0 - g, g, residual, fe, nonlinear_force)
         if level == 0:
             return f, res_norm
         return f
+
+    def _coupled_sweep(self, f, level, a, b, resid, fe, nonlinear_force):
+        """A sweep ``a f + b STEP(f - resid)`` whose external force is ``fe`` plus
+        the nonlinear force of its own input.  The poroelastic coupling force
+        (``DivGradForce``) is fused into the sweep (``xlbb_elast_sweep_divgrad``:
+        one launch, the same values bit for bit) when the sweep qualifies;
+        otherwise the force is evaluated first."""
+        L = self._L(level)
+        if self._fused_coupling and getattr(nonlinear_force, "fusable", False) and not self._sweep_acc64(L):
+            out = self._sweep(f, level, a, b, resid=resid, fext=fe, coupling=nonlinear_force)
+            if out is not None:
+                return out
+        ext = self._ext_force(fe, nonlinear_force, f, level)
+        return self._sweep(f, level, a, b, resid=resid, fext=ext)
 
     # ------------------------------------------------------------------ driver
     def run(self, t_max):

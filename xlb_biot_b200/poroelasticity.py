@@ -19,6 +19,8 @@ class DivGradForce:
     """``lambda f_el: darcy.gradient(elasticity.update_divergence(f_el), scale)``
     of ``src/poroelasticity.py:324`` as an object the kernels can evaluate."""
 
+    fusable = True          # the elasticity sweeps may compute it in-kernel (xlbb_elast_sweep_divgrad)
+
     def __init__(self, elasticity, darcy, scale):
         self.elasticity, self.darcy, self.scale = elasticity, darcy, scale
 
