@@ -43,6 +43,31 @@ __host__ __device__ inline size_t tail_smem_bytes(int nx, int ny, int levels) {
 
 // One damped sweep out = a f + b STEP(f - r) of a periodic nx x ny level held
 // in shared memory (planes of nx * ny cells); zero_in: f taken as zero.
+// elast_rates with every operation rounded on its own (no fused multiply-add):
+// the batched sweeps' rates are computed on the host (to_batch_inst), and the
+// tail reproduces them bit for bit.
+__device__ __forceinline__ float rn_add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float rn_sub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float rn_mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float rn_div(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ double rn_add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double rn_sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double rn_mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double rn_div(double a, double b) { return __ddiv_rn(a, b); }
+
+template <typename T>
+__device__ __forceinline__ void tail_rates(T lam, T mu, T& cs, T& cd, T& h, T& n) {
+    const T s = rn_add(lam, mu);
+    T g = rn_div(T(1.0), rn_sub(rn_mul(T(12.0), s), T(4.0)));
+    if (g > T(100) || g < T(-100)) g = T(0);
+    h = rn_add(T(0.25), rn_mul(T(0.5), g));
+    n = rn_mul(T(-0.25), g);
+    const T t = rn_mul(T(3), s);
+    cs = rn_div(rn_sub(t, T(1)), rn_add(t, T(1)));
+    const T m6 = rn_mul(T(6), mu);
+    cd = rn_div(rn_sub(m6, T(1)), rn_add(m6, T(1)));
+}
+
 template <typename U>
 __device__ __forceinline__ void tail_sweep(const U* fin, U* fout, const U* r, int nx, int ny, U a, U b, bool zero_in,
                                            U cs, U cd, U h, U n) {
@@ -146,9 +171,9 @@ __global__ void __launch_bounds__(TAIL_THREADS) batched_tail_kernel(const XlbbBa
     __syncthreads();
 
     T cs, cd, h, n;
-    elast_rates<T>(T(tl.lam), T(tl.mu), cs, cd, h, n);
+    tail_rates<T>(T(tl.lam), T(tl.mu), cs, cd, h, n);
     TC csc, cdc, hc, nc;
-    elast_rates<TC>(TC(tl.lam), TC(tl.mu), csc, cdc, hc, nc);
+    tail_rates<TC>(TC(tl.lam), TC(tl.mu), csc, cdc, hc, nc);
     const T a = T(1.0 - gamma), b = T(gamma);
     const TC ac = TC(1.0 - gamma), bc = TC(gamma);
 

@@ -214,7 +214,7 @@ class AdvectionDiffusionReactionBGK(LBMBase):
         it, rel, self.stalled = iterate_to_tolerance(replay, tol, max_sweeps - 1, stall_checks)
         return loop.result, it + 1, rel
 
-    def solve_refined(self, f=None, tol=1e-8, inner_tol=1e-5, check_every=1000, max_sweeps=10 ** 8, max_outer=30,
+    def solve_refined(self, f=None, tol=1e-8, inner_tol=None, check_every=1000, max_sweeps=10 ** 8, max_outer=30,
                       stall_checks=20):
         """Steady state to an FP64 relative residual ``tol`` with the bulk of the
         sweeps in FP32 (mixed-precision iterative refinement, ``refine.py``):

@@ -635,7 +635,7 @@ class LBMElasticity:
                                  for r in self._rules[level])
         return cache[level]
 
-    def solve_refined(self, f=None, tol=1e-8, inner_tol=1e-5, check_every=200, max_sweeps=10 ** 7, max_outer=30,
+    def solve_refined(self, f=None, tol=1e-8, inner_tol=None, check_every=200, max_sweeps=10 ** 7, max_outer=30,
                       external_force=None, stall_checks=20):
         """Pseudo-time iteration to an FP64 relative residual ``tol`` with the
         bulk of the sweeps in FP32 (mixed-precision iterative refinement,

@@ -330,6 +330,7 @@ class LBMPoroelasticity:
                 r = float(r)
                 require_finite(r, "level-0 residual norm of the inner elasticity solve", k + 1)
                 r0 = r if r0 is None else r0
+                self.last_inner_rel = r / r0 if r0 > 0 else 0.0
                 if r0 == 0.0 or r / r0 < self.elasticityTol:
                     break
         eta, sigma = el.update_macroscopic(f_elasticity, nonlinear_force.evaluate(el, f_elasticity, 0, force))

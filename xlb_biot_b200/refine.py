@@ -15,8 +15,9 @@ FP32 on the correction:
   constants zero).  With ``u = e + D`` this is ``u = A (u - D)``, i.e. the
   fused sweep with its residual input set to D (``resid`` of
   ``xlbb_elast_sweep`` / ``xlbb_darcy_sweep``), iterated from u = 0 as a CUDA
-  graph until its own pseudo-time residual has fallen by ``inner_tol`` (or
-  stalls at its rounding floor);
+  graph until its own pseudo-time residual has fallen as far as the
+  remaining defect needs (the first correction: to its FP32 rounding floor,
+  where it stalls);
 * update in FP64: ``F <- F + u - D``.
 
 Every outer step gains the accuracy an FP32 solve reaches on the correction,
@@ -119,7 +120,13 @@ def refine(defect, loop, F, tol, inner_tol, max_sweeps, max_outer, stall_checks,
         if rel < tol or stats["outer"] >= max_outer:
             return F - D, stats          # S(F): the sweep that measured the last defect
         loop.r.copy_(D)
-        n, irel, stalled = loop.solve(inner_tol, max_sweeps, stall_checks)
+        # the correction must take the defect below tol (with a factor 10 to
+        # spare): the first outer step runs to the FP32 rounding floor, the
+        # later ones only as far as the remaining defect needs
+        target = min(0.5, 0.1 * tol * d0 / dn) if dn > 0 else 0.5
+        if inner_tol is not None:
+            target = max(target, inner_tol)
+        n, irel, stalled = loop.solve(target, max_sweeps, stall_checks)
         stats["sweeps_f32"] += n
         stats["inner"].append({"sweeps": n, "relative_residual": irel, "stalled": stalled,
                                "defect_relative": rel})
