@@ -204,6 +204,7 @@ struct ElastPhys {
         T div_scale;
         int mix;   // 0: out = S; 1: out = a f + b S
         int sumsq_diff;   // sumsq of (out - f_in) instead of out
+        int ext_in_kernel = 0;   // the external force is computed by the kernel itself (not loaded)
         static constexpr int PMAX = 20;
         const S_* planes[PMAX];   // input planes in from_smem order (bulk-copy kernel)
         int np;
@@ -308,7 +309,7 @@ struct ElastPhys {
             const int c = y * p.geom.pitch + x;
             elast_rates<T>(T(__ldg(p.mat.lam_f + c)), T(__ldg(p.mat.mu_f + c)), cs, cd, h, n);
         }
-        elast_collide<T>(g, p.force != nullptr || p.fext != nullptr, in.F0, in.F1, cs, cd, h, n, o);
+        elast_collide<T>(g, p.force != nullptr || p.fext != nullptr || p.ext_in_kernel, in.F0, in.F1, cs, cd, h, n, o);
     }
     template <bool PREV>
     __device__ static double store(const Args& p, int y, int x, T (&S)[8], const T* fprev) {
@@ -341,7 +342,7 @@ struct ElastPhys {
 // ---------------------------------------------------------------------------
 // T_: arithmetic type; St_: storage type of the fields (St_ = float with
 // T_ = double is FP32 storage with FP64 arithmetic, the 'f64/f32' policy).
-template <typename T_, typename St_ = T_>
+template <typename T_, typename St_ = T_, bool RES_ = false>
 struct DarcyPhys {
     using T = T_;
     using St = St_;
@@ -432,7 +433,7 @@ struct DarcyPhys {
         T f[9];
 #pragma unroll
         for (int i = 0; i < 9; ++i) f[i] = in.f[i];
-        if (p.resid) {      // the sweep of f - resid (the correction equation of a refinement step)
+        if constexpr (RES_) {   // the sweep of f - resid (the correction equation of a refinement step)
             const size_t o = (size_t)y * p.geom.pitch + x;
 #pragma unroll
             for (int i = 0; i < 9; ++i) f[i] = f[i] - T(__ldg(p.resid + (o + (size_t)i * p.geom.plane)));
@@ -1135,11 +1136,18 @@ static long long darcy_partials_t(const XlbbGrid* g, const XlbbDarcySweep* s) {
 
 template <typename T, typename St = T>
 static int darcy_sweep_t(const XlbbGrid* g, const XlbbDarcySweep* s, cudaStream_t st) {
-    using Ph = DarcyPhys<T, St>;
-    typename Ph::Args a = darcy_args<Ph>(g, s);
     const XlbbSweepConfig c = effective_cfg(1, darcy_dtype<T, St>());
-    if (s->sumsq) launch_sweep<Ph, true>(c, g, st, a);
-    else launch_sweep<Ph, false>(c, g, st, a);
+    if (s->resid) {          // a separate instantiation: the plain sweep keeps its registers
+        using Ph = DarcyPhys<T, St, true>;
+        typename Ph::Args a = darcy_args<Ph>(g, s);
+        if (s->sumsq) launch_sweep<Ph, true>(c, g, st, a);
+        else launch_sweep<Ph, false>(c, g, st, a);
+    } else {
+        using Ph = DarcyPhys<T, St>;
+        typename Ph::Args a = darcy_args<Ph>(g, s);
+        if (s->sumsq) launch_sweep<Ph, true>(c, g, st, a);
+        else launch_sweep<Ph, false>(c, g, st, a);
+    }
     return check_launch("xlbb_darcy_sweep");
 }
 
@@ -2166,6 +2174,7 @@ int xlbb_elast_sweep_divgrad(int dtype, const XlbbGrid* g, const XlbbElastMateri
             return fail(XLBB_EUNSUPPORTED, "xlbb_elast_sweep_divgrad: post-streaming rules without push words"); \
         const T_* base = static_cast<const T_*>(s->fext);                                                     \
         a.fext = nullptr;                                                                                     \
+        a.ext_in_kernel = 1;                                                                                  \
         Ph::fill_ptrs(a);                                                                                     \
         launch_k(elast_divgrad_push_kernel<T_, R_>, grid, blk, 0, XLBB_STREAM(stream), a, (T_)mat->lam,        \
                  (T_)mat->mu, (T_)div_scale, (T_)scale, rules_view<T_, 9>(gr), base);                           \
