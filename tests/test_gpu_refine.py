@@ -30,14 +30,19 @@ def test_darcy_refined_matches_fp64_solve():
     s64, _ = darcy_lognormal(G, n=128, ell=8.0, precision="f64/f64")
     s32, _ = darcy_lognormal(G, n=128, ell=8.0, precision="f32/f32")
     f64, n64, r64 = s64.solve(tol=1e-8, check_every=500)
+    # the error reference: FP64 to 1e-12 (at 1e-8 the slow diffusion mode is
+    # still ~1e-8 / (1 - rho) away from the steady state)
+    fx, nx_, rx = s64.solve(tol=1e-12, check_every=500)
     f32, n32, r32 = s32.solve(tol=1e-8, check_every=500)
     fr, nr, rr = s32.solve_refined(tol=1e-8, check_every=500)
-    assert r64 < 1e-8 and rr < 1e-8 and fr.dtype == torch.float64
+    assert r64 < 1e-8 and rx < 1e-12 and rr < 1e-8 and fr.dtype == torch.float64
     st = s32.refine_stats
     assert st["sweeps_f64"] == st["outer"] + 1 and st["sweeps_f32"] > 10 * st["sweeps_f64"]
-    p64, pr, p32 = (s64.update_macroscopic(x) for x in (f64, fr, f32.double()))
-    err_ref, err_32 = _rel(pr, p64), _rel(p32, p64)
-    assert err_ref < 1e-6 and err_ref < 1e-2 * err_32, (err_ref, err_32, st)
+    px = s64.update_macroscopic(fx)
+    e64, eref, e32 = (_rel(s64.update_macroscopic(x), px) for x in (f64, fr, f32.double()))
+    # the refined FP32 solve is as accurate as the FP64 solve to the same
+    # tolerance, and far more accurate than the plain FP32 solve
+    assert eref <= 2.0 * e64 + 1e-9 and eref < 0.1 * e32, (eref, e64, e32, st)
 
 
 def test_elasticity_refined_matches_fp64_solve():
