@@ -1,5 +1,5 @@
 """The oracle's classes under the reference's names (test infrastructure only)."""
-from .lattice import Lattice, LatticeD2Q8, LatticeD2Q9, Policy  # noqa: F401
+from .lattice import Lattice, LatticeD2Q8, LatticeD2Q9, LatticeD3Q19, LatticeD3Q27, Policy  # noqa: F401
 from .boundary_conditions import BoundaryCondition, BounceBackHalfway  # noqa: F401
 from .elasticity import (LBMElasticity, ElasticityBounceBackFullway, ElasticityBounceBack,  # noqa: F401
                          ElasticityAntiBounceBack)

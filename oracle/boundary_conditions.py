@@ -14,21 +14,24 @@ def stream(f, c):
     """Periodic pull streaming ``f_i(x) <- f_i(x - c_i)`` via ``roll``
     (``src/elasticity.py:768-803``, ``src/base.py:649-683``).  On one device the
     ppermute halo swap of ``streaming_m`` (``:738-766``) is the identity."""
+    d = c.shape[0]
     out = np.empty_like(f)
     for i in range(f.shape[-1]):
-        out[..., i] = np.roll(f[..., i], (int(c[0, i]), int(c[1, i])), axis=(0, 1))
+        out[..., i] = np.roll(f[..., i], tuple(int(c[k, i]) for k in range(d)), axis=tuple(range(d)))
     return out
 
 
-def create_grid_mask(nx, ny, lattice, solid_halo_voxels):
-    """``src/elasticity.py:460-487``: a (nx+2, ny+2, q) boolean mask, True on the
-    one-cell halo (even for periodic sides) and on solid BC voxels, streamed."""
+def create_grid_mask(nx, ny, lattice, solid_halo_voxels, nz=0):
+    """``src/elasticity.py:460-487`` / ``src/base.py:414-449``: a (nx+2, ny+2,
+    [nz+2,] q) boolean mask, True on the one-cell halo (even for periodic
+    sides) and on solid BC voxels, streamed."""
     hw = 1
-    m = np.ones((nx + 2 * hw, ny + 2 * hw, lattice.q), dtype=bool)
-    m[hw:-hw, hw:-hw, :] = False
+    shape = (nx, ny) if lattice.d == 2 else (nx, ny, nz)
+    m = np.ones(tuple(n + 2 * hw for n in shape) + (lattice.q,), dtype=bool)
+    m[tuple(slice(hw, -hw) for _ in shape)] = False
     if solid_halo_voxels is not None:
         v = np.asarray(solid_halo_voxels)
-        m[v[:, 0] + hw, v[:, 1] + hw, :] = True
+        m[tuple(v[:, k] + hw for k in range(len(shape)))] = True
     return stream(m, lattice.c)
 
 

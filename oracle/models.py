@@ -1,4 +1,4 @@
-"""D2Q9 fluid BGK and KBC collision models (oracle) — TEST INFRASTRUCTURE ONLY.
+"""Fluid BGK (D2Q9, D3Q19, D3Q27) and KBC (D2Q9) collision models (oracle) — TEST INFRASTRUCTURE ONLY.
 
 Restates ``src/models.py:9-154`` (``BGKSim``, ``KBCSim``, the D2Q9 shear
 decomposition) on the ``LBMBase`` pieces they use (``src/base.py:351-372``
@@ -41,7 +41,7 @@ class EquilibriumBC(BoundaryCondition):
 
 
 class _FluidBase:
-    """``src/base.py:30-146`` (one device, two dimensions)."""
+    """``src/base.py:30-146`` (one device; two or three dimensions)."""
 
     def __init__(self, **kwargs):
         self.omega = kwargs.get("omega")
@@ -50,15 +50,25 @@ class _FluidBase:
         self.precisionPolicy = Policy(self.precision)
         self.lattice = kwargs.get("lattice")
         self.c, self.q, self.w, self.dim = self.lattice.c, self.lattice.q, self.lattice.w, self.lattice.d
-        self.gridInfo = {"nx": self.nx, "ny": self.ny, "nz": self.nz, "dim": 2, "lattice": self.lattice}
-        self.boundingBoxIndices = {
-            "bottom": np.array([[i, 0] for i in range(self.nx)], dtype=int),
-            "top": np.array([[i, self.ny - 1] for i in range(self.nx)], dtype=int),
-            "left": np.array([[0, i] for i in range(self.ny)], dtype=int),
-            "right": np.array([[self.nx - 1, i] for i in range(self.ny)], dtype=int)}
+        self.gridInfo = {"nx": self.nx, "ny": self.ny, "nz": self.nz, "dim": self.dim, "lattice": self.lattice}
+        nx, ny, nz = self.nx, self.ny, self.nz
+        if self.dim == 2:            # src/base.py:451-470
+            self.boundingBoxIndices = {
+                "bottom": np.array([[i, 0] for i in range(nx)], dtype=int),
+                "top": np.array([[i, ny - 1] for i in range(nx)], dtype=int),
+                "left": np.array([[0, i] for i in range(ny)], dtype=int),
+                "right": np.array([[nx - 1, i] for i in range(ny)], dtype=int)}
+        else:                        # src/base.py:472-484
+            self.boundingBoxIndices = {
+                "bottom": np.array([[i, j, 0] for i in range(nx) for j in range(ny)], dtype=int),
+                "top": np.array([[i, j, nz - 1] for i in range(nx) for j in range(ny)], dtype=int),
+                "left": np.array([[0, j, k] for j in range(ny) for k in range(nz)], dtype=int),
+                "right": np.array([[nx - 1, j, k] for j in range(ny) for k in range(nz)], dtype=int),
+                "front": np.array([[i, 0, k] for i in range(nx) for k in range(nz)], dtype=int),
+                "back": np.array([[i, ny - 1, k] for i in range(nx) for k in range(nz)], dtype=int)}
         self.BCs = []
         self.set_boundary_conditions()
-        grid_mask = create_grid_mask(self.nx, self.ny, self.lattice, solid_voxels(self.BCs))
+        grid_mask = create_grid_mask(nx, ny, self.lattice, solid_voxels(self.BCs), nz)
         for bc in self.BCs:
             bc.create_local_mask_and_normal_arrays(grid_mask)
 
@@ -72,8 +82,8 @@ class _FluidBase:
         """``src/base.py:528-559``."""
         rho0, u0 = self.initialize_macroscopic_fields()
         if rho0 is None or u0 is None:
-            return np.broadcast_to(self.w.astype(self.precisionPolicy.output_dtype),
-                                   (self.nx, self.ny, self.q)).copy()
+            shape = (self.nx, self.ny) if self.dim == 2 else (self.nx, self.ny, self.nz)
+            return np.broadcast_to(self.w.astype(self.precisionPolicy.output_dtype), shape + (self.q,)).copy()
         return self.equilibrium(rho0, u0)
 
     def equilibrium(self, rho, u, cast_output=True):

@@ -15,6 +15,7 @@ import sys
 import numpy as np
 
 sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(1, os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))))
 from problems import (elastic_material, make_darcy, make_periodic_biot, make_periodic_elasticity,  # noqa: E402
                       make_terzaghi, make_walled_elasticity)
 
@@ -234,6 +235,24 @@ def parameters_terzaghi(m, alpha=0.8):
             "units": np.array([params.get_unit(k) for k in "LHTP"]), "rejected": np.array(rejected)}
 
 
+def fluid_cavity(m, model, lattice="D2Q9", n=(24, 20), t_max=20):
+    """The cavities of ``examples/performance/MLUPS2d.py`` (BGK and KBC on
+    D2Q9) and ``MLUPS3d.py`` (BGK on D3Q19 / D3Q27) through the reference's
+    ``run`` (``src/base.py:848-948``): t_max + 1 steps from rest."""
+    from xlb_biot_b200.workloads import lid_driven_cavity, lid_driven_cavity_3d
+    if lattice == "D2Q9":
+        C, om = lid_driven_cavity(m, model)
+        s = C(lattice=m.LatticeD2Q9(PREC), omega=om(n[0]), nx=n[0], ny=n[1], nz=0, precision=PREC,
+              print_info_rate=0)
+    else:
+        C, om = lid_driven_cavity_3d(m)
+        lat = getattr(m, "Lattice" + lattice)(PREC)
+        s = C(lattice=lat, omega=om(n[0]), nx=n[0], ny=n[1], nz=n[2], precision=PREC, print_info_rate=0)
+    f = s.run(t_max)
+    rho, u = s.update_macroscopic(f)
+    return {"f": to_np(f), "rho": to_np(rho), "u": to_np(u)}
+
+
 CASES = {
     "elast_plain_16x16": lambda m: elast_plain(m, 16, 16),
     "elast_plain_37x22": lambda m: elast_plain(m, 37, 22),
@@ -255,6 +274,10 @@ CASES = {
     "elast_plain_16x16_f64f32": lambda m: elast_plain(m, 16, 16, prec="f64/f32"),
     "elast_dirichlet_mg3_f64f32": lambda m: elast_walled_mg(m, "dirichlet", prec="f64/f32"),
     "darcy_anti_f64f32": lambda m: darcy(m, "anti", prec="f64/f32"),
+    "fluid_cavity_bgk_d2q9": lambda m: fluid_cavity(m, "bgk"),
+    "fluid_cavity_kbc_d2q9": lambda m: fluid_cavity(m, "kbc"),
+    "fluid_cavity_bgk_d3q19": lambda m: fluid_cavity(m, "bgk", "D3Q19", (10, 8, 12)),
+    "fluid_cavity_bgk_d3q27": lambda m: fluid_cavity(m, "bgk", "D3Q27", (10, 8, 12)),
 }
 
 # relative tolerance of each case (FP64 runs: 1e-12; FP32 storage: 1e-5)

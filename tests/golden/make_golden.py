@@ -36,10 +36,12 @@ def reference_namespace(root):
     import src.darcy
     import src.elasticity
     import src.lattice
+    import src.models
     import src.poroelasticity
     import src.utils
     ns = {}
-    for mod in (src.lattice, src.boundary_conditions, src.elasticity, src.darcy, src.poroelasticity, src.utils):
+    for mod in (src.lattice, src.boundary_conditions, src.elasticity, src.darcy, src.poroelasticity, src.utils,
+                src.models):
         ns.update({k: getattr(mod, k) for k in dir(mod) if not k.startswith("_")})
     m = SimpleNamespace(**ns)
     m.golden_asarray = jnp.asarray

@@ -1,5 +1,5 @@
 """All public classes under the reference's names, in one namespace."""
-from .lattice import Lattice, LatticeD2Q8, LatticeD2Q9  # noqa: F401
+from .lattice import Lattice, LatticeD2Q8, LatticeD2Q9, LatticeD3Q19, LatticeD3Q27  # noqa: F401
 from .boundary_conditions import BoundaryCondition, BounceBackHalfway, BounceBack, EquilibriumBC  # noqa: F401
 from .elasticity import (LBMElasticity, ElasticityBounceBackFullway, ElasticityBounceBack,  # noqa: F401
                          ElasticityAntiBounceBack)

@@ -312,3 +312,25 @@ def lid_driven_cavity(m, model="bgk", u_wall=0.1, Re=100.0):
     def omega(n):
         return 1.0 / (3.0 * (u_wall * (n - 1) / Re) + 0.5)
     return Cavity, omega
+
+
+def lid_driven_cavity_3d(m, u_wall=0.1, Re=100.0):
+    """The fluid workload of ``examples/performance/MLUPS3d.py``: a cubic
+    cavity with full-way bounce-back on the left, right, bottom, front and back
+    faces and the equilibrium of (rho = 1, u = (u_wall, 0, 0)) on the top face
+    (z = nz - 1), BGK collision.  Returns the solver class and ``omega(n)``."""
+    class Cavity3D(m.BGKSim):
+        def set_boundary_conditions(self):
+            bb = self.boundingBoxIndices
+            walls = np.concatenate((bb["left"], bb["right"], bb["bottom"], bb["front"], bb["back"]))
+            self.BCs.append(m.BounceBack(tuple(walls.T), self.gridInfo, self.precisionPolicy))
+            lid = bb["top"]
+            dt = self.precisionPolicy.compute_dtype
+            rho_wall = np.ones((lid.shape[0], 1), dtype=dt)
+            vel_wall = np.zeros(lid.shape, dtype=dt)
+            vel_wall[:, 0] = u_wall
+            self.BCs.append(m.EquilibriumBC(tuple(lid.T), self.gridInfo, self.precisionPolicy, rho_wall, vel_wall))
+
+    def omega(n):
+        return 1.0 / (3.0 * (u_wall * (n - 1) / Re) + 0.5)
+    return Cavity3D, omega
