@@ -764,6 +764,66 @@ def run_mlups2d(args):
     return 0
 
 
+def run_mlups3d(args):
+    """The fluid path of ``examples/performance/MLUPS3d.py``: lid-driven cavity
+    (Re = 100, u_wall = 0.1, full-way bounce-back on five faces, equilibrium
+    lid), BGK, FP32, ``--cavity3d-n`` cubed cells (256^3: 1.3 GB of D3Q19
+    populations, far above L2), on D3Q19 (the example's lattice; the headline
+    of this line) and D3Q27, ``--steps`` calls of the public ``step`` timed
+    with CUDA events; roofline at 8 q B per cell (q populations read and
+    written, FP32).  CPU baseline: the oracle's D3Q19 BGK step (vectorised
+    NumPy, one process) on a 64^3 cavity."""
+    import time
+    import torch
+    import xlb_biot_b200.api as G
+    from xlb_biot_b200.workloads import lid_driven_cavity_3d as make_cavity
+    n = args.cavity3d_n
+    peak, peak_kind = measured_peak_hbm()
+    out = {}
+    for name in ("D3Q19", "D3Q27"):
+        C, om = make_cavity(G)
+        s = C(lattice=getattr(G, "Lattice" + name)("f32/f32"), omega=om(n), nx=n, ny=n, nz=n, precision="f32/f32",
+              print_info_rate=0)
+        q = s.q
+        f = s.assign_fields_sharded()
+        for t in range(args.warmup):
+            f, _ = s.step(f, t)
+
+        def loop(f=f):
+            for t in range(args.steps):
+                f, _ = s.step(f, t)
+            return f
+        f, t = _timed(loop)
+        cells = n ** 3
+        gbs = cells * 8 * q * args.steps / t / 1e9
+        out[name.lower()] = {"mlups": cells * args.steps / t / 1e6, "ms_per_step": t / args.steps * 1e3,
+                             "bytes_per_lu": 8 * q,
+                             "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
+                                          "frac": gbs / peak, "peak_kind": peak_kind},
+                             "finite": bool(torch.isfinite(f).all())}
+        del s, f
+        torch.cuda.empty_cache()
+    cpu = None
+    if not args.no_cpu_baseline:
+        import oracle.api as O
+        m = 64
+        Co, omo = make_cavity(O)
+        so = Co(lattice=O.LatticeD3Q19("f32/f32"), omega=omo(m), nx=m, ny=m, nz=m, precision="f32/f32")
+        fo = so.assign_fields_sharded()
+        fo, _ = so.step(fo, 0)
+        t0, k = time.time(), 0
+        while time.time() - t0 < 10.0:
+            fo, _ = so.step(fo, k)
+            k += 1
+        cpu = {"value": m ** 3 * k / (time.time() - t0) / 1e6, "unit": "MLUPS", "cores": 1, "kind": "port",
+               "sample": f"oracle D3Q19 BGK cavity step (NumPy, FP32), {m}^3 cells, {k} steps"}
+    print(json.dumps({"workload": f"mlups3d_cavity_{n}^3", "metric": "MLUPS", "value": out["d3q19"]["mlups"],
+                      "unit": "MLUPS", "dtype": "f32", "steps": args.steps, "warmup": args.warmup,
+                      "d3q19": out["d3q19"], "d3q27": out["d3q27"], "cpu_baseline": cpu,
+                      "data": "synthetic (cavity from rest, as the example)"}), flush=True)
+    return 0
+
+
 def run_c2solve(args):
     """The Darcy configuration as stated: 1024^2, log-normal k, run to steady
     state at a relative residual ||f^{n+1} - f^n|| / ||f^1 - f^0|| < 1e-8
@@ -1012,8 +1072,9 @@ def main():
     ap.add_argument("--adjoint-steps", type=int, default=200)
     ap.add_argument("--fd-directions", type=int, default=32)
     ap.add_argument("--cavity-n", type=int, default=4096)
+    ap.add_argument("--cavity3d-n", type=int, default=256)
     ap.add_argument("--workload", choices=["darcy", "c1", "c2solve", "c3", "c3inner", "c4", "c4sweep", "c4vcycle",
-                                           "c5", "mlups2d", "darcy_hbm"],
+                                           "c5", "mlups2d", "mlups3d", "darcy_hbm"],
                     default="darcy",
                     help="darcy: the headline line; c1/c3/c4/c5: the other configurations (one JSON line each)")
     ap.add_argument("--biot-steps", type=int, default=100)
@@ -1042,6 +1103,8 @@ def main():
         return run_c4vcycle(args)
     if args.workload == "mlups2d":
         return run_mlups2d(args)
+    if args.workload == "mlups3d":
+        return run_mlups3d(args)
     if args.workload == "c2solve":
         return run_c2solve(args)
     if args.workload == "c3inner":

@@ -208,6 +208,28 @@ int xlbb_darcy_sweep_pipeline(int dtype, const XlbbGrid* g, const XlbbDarcySweep
 int xlbb_fluid_sweep(int dtype, const XlbbGrid* g, const XlbbDarcySweep* s, int model, void* stream);
 
 /*
+ * Three-dimensional grid: nz planes of ny rows; row (y, z) is y + ny * z, cell
+ * (x, y, z) at (y + ny * z) * pitch + x, population i at i * plane further.
+ * Rule tables over such a grid index rows the same way (ny * nz rows).
+ */
+typedef struct {
+    int nx, ny, nz, pitch;
+    long long plane;
+} XlbbGrid3;
+
+/*
+ * One fused D3Q19 (q = 19) or D3Q27 (q = 27) BGK fluid step (BGKSim.collision,
+ * src/models.py:20-34, inside LBMBase.step, src/base.py:809-846, on the
+ * lattices of src/lattice.py:132-182): collision, PostCollision rules,
+ * streaming with periodic wrap in x, y and z, PostStreaming rules.  Uniform
+ * omega only; omega_field, source, ext_source, resid and sumsq must be NULL
+ * (XLBB_EBADARG), and PostStreaming rules need their push words
+ * (XLBB_EUNSUPPORTED otherwise).  Replaces the step that
+ * examples/performance/MLUPS3d.py times.
+ */
+int xlbb_fluid3_sweep(int dtype, const XlbbGrid3* g, const XlbbDarcySweep* s, int q, void* stream);
+
+/*
  * Darcy sweep plus its FP64 convergence residual, allocating nothing.
  * No counterpart in the reference: it exists for callers that cannot allocate
  * device memory (inside a CUDA-graph capture, host runtimes that hand the

@@ -29,17 +29,21 @@ def test_darcy_refined_matches_fp64_solve():
     from xlb_biot_b200.workloads import darcy_lognormal
     s64, _ = darcy_lognormal(G, n=128, ell=8.0, precision="f64/f64")
     s32, _ = darcy_lognormal(G, n=128, ell=8.0, precision="f32/f32")
+    # a solve returns the solver's own state buffer, which the next solve
+    # overwrites: every result is copied before the next one starts
     f64, n64, r64 = s64.solve(tol=1e-8, check_every=500)
+    p64 = s64.update_macroscopic(f64).clone()
     # the error reference: FP64 to 1e-12 (at 1e-8 the slow diffusion mode is
     # still ~1e-8 / (1 - rho) away from the steady state)
     fx, nx_, rx = s64.solve(tol=1e-12, check_every=500)
+    px = s64.update_macroscopic(fx).clone()
     f32, n32, r32 = s32.solve(tol=1e-8, check_every=500)
+    p32 = s64.update_macroscopic(f32.double()).clone()
     fr, nr, rr = s32.solve_refined(tol=1e-8, check_every=500)
     assert r64 < 1e-8 and rx < 1e-12 and rr < 1e-8 and fr.dtype == torch.float64
     st = s32.refine_stats
     assert st["sweeps_f64"] == st["outer"] + 1 and st["sweeps_f32"] > 10 * st["sweeps_f64"]
-    px = s64.update_macroscopic(fx)
-    e64, eref, e32 = (_rel(s64.update_macroscopic(x), px) for x in (f64, fr, f32.double()))
+    e64, eref, e32 = (_rel(x, px) for x in (p64, s64.update_macroscopic(fr), p32))
     # the refined FP32 solve is as accurate as the FP64 solve to the same
     # tolerance, and far more accurate than the plain FP32 solve
     assert eref <= 2.0 * e64 + 1e-9 and eref < 0.1 * e32, (eref, e64, e32, st)

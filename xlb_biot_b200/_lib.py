@@ -36,6 +36,11 @@ class Grid(ctypes.Structure):
     _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("pitch", ctypes.c_int), ("plane", ctypes.c_longlong)]
 
 
+class Grid3(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int), ("pitch", ctypes.c_int),
+                ("plane", ctypes.c_longlong)]
+
+
 class Rules(ctypes.Structure):
     _fields_ = [("count", ctypes.c_int), ("row_ptr", ctypes.c_void_p), ("cell_x", ctypes.c_void_p),
                 ("code", ctypes.c_void_p), ("cst", ctypes.c_void_p), ("mask", ctypes.c_void_p),
@@ -114,6 +119,7 @@ SIGNATURES = {
     "xlbb_darcy_sweep_partials": (I, [I, PG, ctypes.POINTER(DarcySweep)]),
     "xlbb_darcy_sweep_pipeline": (I, [I, PG, ctypes.POINTER(DarcySweep)]),
     "xlbb_fluid_sweep": (I, [I, PG, ctypes.POINTER(DarcySweep), I, P]),
+    "xlbb_fluid3_sweep": (I, [I, ctypes.POINTER(Grid3), ctypes.POINTER(DarcySweep), I, P]),
     "xlbb_darcy_sweep_residual_noalloc": (I, [I, PG, ctypes.POINTER(DarcySweep), P, P]),
     "xlbb_darcy_gradient": (I, [I, PG, P, D, ctypes.POINTER(Rules), P, P, P]),
     "xlbb_elast_divgrad": (I, [I, PG, ctypes.POINTER(ElastMaterial), D, P, D, ctypes.POINTER(Rules), P, P, P]),

@@ -56,7 +56,7 @@ class LBMBase:
         self._dcode = _lib.dtype_code(self._dtype)
         self._sweep_code = _lib.XLBB_F32_ACC64 if self._acc64 else self._dcode
         self._rule_dtype = torch.float64 if self._acc64 else self._dtype
-        self._layout = Layout(self.nx, self.ny, self._dtype)
+        self._layout = Layout(self.nx, self.ny, self._dtype, nz=self.nz)
         self.boundingBoxIndices = self.bounding_box_indices()
         self._create_boundary_data()
         self.force = self.get_force()
@@ -72,8 +72,8 @@ class LBMBase:
             raise ValueError("Lattice type must be provided.")
         if self.nz == 0 and value.name not in ['D2Q9']:
             raise ValueError("For 2D simulations, lattice type must be LatticeD2Q9.")
-        if self.nz != 0:
-            raise ValueError("3D simulations are not on the Biot path.")
+        if self.nz != 0 and value.name not in ['D3Q19', 'D3Q27']:
+            raise ValueError("For 3D simulations, lattice type must be LatticeD3Q19, or LatticeD3Q27.")
         self._lattice = value
 
     @property
@@ -160,15 +160,22 @@ class LBMBase:
         return set_precisions(precision)
 
     def bounding_box_indices(self):
-        """``src/base.py:451-470``."""
-        nx, ny = self.nx, self.ny
-        return {"bottom": np.array([[i, 0] for i in range(nx)], dtype=int),
-                "top": np.array([[i, ny - 1] for i in range(nx)], dtype=int),
-                "left": np.array([[0, i] for i in range(ny)], dtype=int),
-                "right": np.array([[nx - 1, i] for i in range(ny)], dtype=int)}
+        """``src/base.py:451-484``: edges (2D) or faces (3D) of the grid."""
+        nx, ny, nz = self.nx, self.ny, self.nz
+        if self.dim == 2:
+            return {"bottom": np.array([[i, 0] for i in range(nx)], dtype=int),
+                    "top": np.array([[i, ny - 1] for i in range(nx)], dtype=int),
+                    "left": np.array([[0, i] for i in range(ny)], dtype=int),
+                    "right": np.array([[nx - 1, i] for i in range(ny)], dtype=int)}
+        return {"bottom": np.array([[i, j, 0] for i in range(nx) for j in range(ny)], dtype=int),
+                "top": np.array([[i, j, nz - 1] for i in range(nx) for j in range(ny)], dtype=int),
+                "left": np.array([[0, j, k] for j in range(ny) for k in range(nz)], dtype=int),
+                "right": np.array([[nx - 1, j, k] for j in range(ny) for k in range(nz)], dtype=int),
+                "front": np.array([[i, 0, k] for i in range(nx) for k in range(nz)], dtype=int),
+                "back": np.array([[i, ny - 1, k] for i in range(nx) for k in range(nz)], dtype=int)}
 
     def create_grid_mask(self, solid_halo_voxels):
-        return grid_mask(self.nx, self.ny, self.lattice, solid_halo_voxels)
+        return grid_mask(self.nx, self.ny, self.lattice, solid_halo_voxels, nz=self.nz)
 
     def _create_boundary_data(self):
         """``src/base.py:351-372`` followed by rule compilation."""
@@ -190,6 +197,8 @@ class LBMBase:
         dt = torch_dtype(type)
         if len(shape) == 3:
             return Layout(shape[0], shape[1], dt).field(init_val, shape[2])
+        if len(shape) == 4:
+            return Layout(shape[0], shape[1], dt, nz=shape[2]).field(init_val, shape[3])
         x = init_val if isinstance(init_val, torch.Tensor) else torch.as_tensor(np.asarray(init_val))
         return torch.broadcast_to(x.to(device="cuda", dtype=dt), shape).clone()
 
@@ -213,7 +222,7 @@ class LBMBase:
         tensor algebra)."""
         L = self._layout
         rho = L.field(rho, 1)
-        u = L.field(u, 2)
+        u = L.field(u, self.dim)
         c = torch.as_tensor(self.c, device=L.device, dtype=L.dtype)
         w = torch.as_tensor(self.w, device=L.device, dtype=L.dtype)
         cu = 3.0 * (u @ c)

@@ -24,13 +24,18 @@ from .boundary_conditions import apply_in_order
 class CompiledRules:
     """Device-resident rule table of one grid and one phase."""
 
-    def __init__(self, q, ny, cells, code, cst, dtype, device, nx=None, push=False):
+    def __init__(self, q, ny, cells, code, cst, dtype, device, nx=None, push=False, shape=None, cells_nd=None):
+        """``cells``: (x, row) of every rule cell, row = y (2D) or y + ny * z
+        (3D, ``shape`` = (nx, ny, nz)); ``cells_nd``: the same cells as (x, y[, z])."""
         self.q = q
         self.count = len(cells)
         self.nx = int(nx) if nx is not None else (int(cells[:, 0].max()) + 1 if len(cells) else 1)
+        self.shape = tuple(shape) if shape is not None else (self.nx, ny)
+        self.cells_nd = np.asarray(cells_nd) if cells_nd is not None else np.asarray(cells)
         order = np.lexsort((cells[:, 0], cells[:, 1])) if self.count else np.zeros(0, dtype=np.int64)
         cells = cells[order]
         self.cells = cells
+        self.cells_nd = self.cells_nd[order] if self.count else self.cells_nd
         self.code_np = code[order]
         self.cst_np = cst[order]
         row_ptr = np.zeros(ny + 1, dtype=np.int32)
@@ -68,16 +73,22 @@ class CompiledRules:
         code = self.code_np
         if np.any(code == neg_keep) or np.any((code == keep) & (self.cst_np != 0)):
             return None
-        from .lattice import LatticeD2Q8, LatticeD2Q9
-        c = np.asarray((LatticeD2Q8 if q == 8 else LatticeD2Q9)("f64/f64").c, dtype=np.int64)
-        zx, zy = self.cells[:, 0], self.cells[:, 1]
-        words = np.zeros(ny * nx, dtype=np.uint32)
-        np.bitwise_or.at(words, zy * nx + zx, np.uint32(1 << 16))
+        from .lattice import LatticeD2Q8, LatticeD2Q9, LatticeD3Q19, LatticeD3Q27
+        lat = {8: LatticeD2Q8, 9: LatticeD2Q9, 19: LatticeD3Q19, 27: LatticeD3Q27}[q]
+        c = np.asarray(lat("f64/f64").c, dtype=np.int64)
+        shape = self.shape
+        dim = len(shape)
+        z = self.cells_nd.astype(np.int64)
+        lin = np.ravel_multi_index(tuple(z[:, k] for k in range(dim)), shape, order="F")
+        words = np.zeros(int(np.prod(shape)), dtype=np.uint32)
+        # bit d: direction d of the cell is rebuilt at its destination; the flag
+        # bit marks a rule cell (16 for the 2D lattices, 31 for the 3D ones)
+        flag = np.uint32(1 << (16 if q <= 16 else 31))
+        np.bitwise_or.at(words, lin, flag)
         for d in range(q):
             rebuilt = code[:, d] != keep
-            sx = (zx[rebuilt] - c[0, d]) % nx
-            sy = (zy[rebuilt] - c[1, d]) % ny
-            np.bitwise_or.at(words, sy * nx + sx, np.uint32(1 << d))
+            src = tuple((z[rebuilt, k] - c[k, d]) % shape[k] for k in range(dim))
+            np.bitwise_or.at(words, np.ravel_multi_index(src, shape, order="F"), np.uint32(1 << d))
         return torch.as_tensor(words.view(np.int32), device=device)
 
     def struct(self):
@@ -99,32 +110,36 @@ def _run(bcs, fout, fin, step, names):
     return apply_in_order(bcs, fout, fin, implementation_step=step, names=names)
 
 
-def compile_rules(bcs, nx, ny, q, dtype, device, step=None, names=None, check=True):
+def compile_rules(bcs, nx, ny, q, dtype, device, step=None, names=None, check=True, nz=0):
     """Rules of ``bcs`` for one phase: ``step`` in {"PostCollision",
-    "PostStreaming"} (apply_bc semantics) or ``names`` (the gradient's filter)."""
+    "PostStreaming"} (apply_bc semantics) or ``names`` (the gradient's filter);
+    ``nz > 0``: a three-dimensional grid (rows y + ny * z)."""
+    shape = (nx, ny) if nz == 0 else (nx, ny, nz)
+    dim = len(shape)
+    rows = ny * (nz if nz else 1)
     if step is not None:
         active = [bc for bc in bcs if bc.implementationStep == step]
     else:
         active = [bc for bc in bcs if bc.name in names]
     cells = []
     for bc in active:
-        idx = np.array(bc.indices, dtype=np.int64).reshape(2, -1).T
-        ok = (idx[:, 0] >= 0) & (idx[:, 0] < nx) & (idx[:, 1] >= 0) & (idx[:, 1] < ny)
+        idx = np.array(bc.indices, dtype=np.int64).reshape(dim, -1).T
+        ok = np.logical_and.reduce([(idx[:, k] >= 0) & (idx[:, k] < shape[k]) for k in range(dim)])
         cells.append(idx[ok])
     if not cells or sum(len(c) for c in cells) == 0:
-        return CompiledRules(q, ny, np.zeros((0, 2), np.int64), np.zeros((0, q), np.uint8), np.zeros((0, q)),
-                             dtype, device, nx)
+        return CompiledRules(q, rows, np.zeros((0, 2), np.int64), np.zeros((0, q), np.uint8), np.zeros((0, q)),
+                             dtype, device, nx, shape=shape, cells_nd=np.zeros((0, dim), np.int64))
     cells = np.unique(np.vstack(cells), axis=0)
-    cx, cy = cells[:, 0], cells[:, 1]
+    at = tuple(cells[:, k] for k in range(dim))
 
     def probe(fout_vec, fin_vec):
-        fout = np.zeros((nx, ny, q))
-        fin = np.zeros((nx, ny, q))
+        fout = np.zeros(shape + (q,))
+        fin = np.zeros(shape + (q,))
         if fout_vec is not None:
-            fout[cx, cy] = fout_vec
+            fout[at] = fout_vec
         if fin_vec is not None:
-            fin[cx, cy] = fin_vec
-        return _run(bcs, fout, fin, step, names)[cx, cy]
+            fin[at] = fin_vec
+        return _run(bcs, fout, fin, step, names)[at]
 
     c0 = probe(None, None)
     eye = np.eye(q)
@@ -163,9 +178,13 @@ def compile_rules(bcs, nx, ny, q, dtype, device, step=None, names=None, check=Tr
         code[:, d] = cd
     # push words: post-streaming rules (collide-and-push sweep, transposed sweeps)
     # and the gradient's rules (its transposed stencil gathers the same way)
-    rules = CompiledRules(q, ny, cells, code, c0, dtype, device, nx, push=(step == "PostStreaming" or step is None))
+    cells2 = cells[:, :2].copy()
+    if dim == 3:
+        cells2[:, 1] = cells[:, 1] + ny * cells[:, 2]
+    rules = CompiledRules(q, rows, cells2, code, c0, dtype, device, nx,
+                          push=(step == "PostStreaming" or step is None), shape=shape, cells_nd=cells)
     if check:
-        _self_check(bcs, nx, ny, q, step, names, rules)
+        _self_check(bcs, shape, q, step, names, rules)
     return rules
 
 
@@ -192,31 +211,30 @@ def apply_rules_device(rules, fout, fin):
     if rules.count == 0:
         return out
     q = rules.q
-    cx = torch.as_tensor(rules.cells[:, 0], device=fout.device)
-    cy = torch.as_tensor(rules.cells[:, 1], device=fout.device)
-    cur, src = fout[cx, cy], fin[cx, cy]
+    at = tuple(torch.as_tensor(rules.cells_nd[:, k], device=fout.device) for k in range(rules.cells_nd.shape[1]))
+    cur, src = fout[at], fin[at]
     code = rules.code.view(-1, q).long()
     k = torch.where(code < q, code, torch.where(code < 2 * q, code - q, torch.zeros_like(code)))
     s = torch.gather(src, 1, k)
     base = torch.where(code < q, s, torch.where(code < 2 * q, -s, torch.where(
         code == 2 * q, torch.zeros_like(s), torch.where(code == 2 * q + 1, cur, -cur))))
-    out[cx, cy] = base + rules.cst.view(-1, q).to(fout.dtype)
+    out[at] = base + rules.cst.view(-1, q).to(fout.dtype)
     return out
 
 
-def _self_check(bcs, nx, ny, q, step, names, rules):
+def _self_check(bcs, shape, q, step, names, rules):
     if rules.count == 0:
         return
     rng = np.random.default_rng(1234)
-    fout = rng.standard_normal((nx, ny, q))
-    fin = rng.standard_normal((nx, ny, q))
+    fout = rng.standard_normal(tuple(shape) + (q,))
+    fin = rng.standard_normal(tuple(shape) + (q,))
     ref = _run(bcs, fout.copy(), fin, step, names)
-    cx, cy = rules.cells[:, 0], rules.cells[:, 1]
-    got = evaluate_rules(rules, fout[cx, cy], fin[cx, cy])
-    scale = max(1.0, float(np.abs(ref[cx, cy]).max()))
-    if not np.allclose(got, ref[cx, cy], rtol=0, atol=1e-12 * scale):
+    at = tuple(rules.cells_nd[:, k] for k in range(len(shape)))
+    got = evaluate_rules(rules, fout[at], fin[at])
+    scale = max(1.0, float(np.abs(ref[at]).max()))
+    if not np.allclose(got, ref[at], rtol=0, atol=1e-12 * scale):
         raise NotImplementedError("boundary conditions are not cell-local affine maps; cannot compile them")
-    mask = np.ones((nx, ny), dtype=bool)
-    mask[cx, cy] = False
+    mask = np.ones(tuple(shape), dtype=bool)
+    mask[at] = False
     if not np.array_equal(ref[mask], fout[mask]):
         raise NotImplementedError("boundary conditions modify cells outside their index sets")

@@ -58,18 +58,20 @@ def _at_add(arr, idx, vals):
     return arr
 
 
-def grid_mask(nx, ny, lattice, solid_voxels):
-    """Grid mask of ``src/elasticity.py:460-487`` / ``src/base.py:414-439`` on one
-    device: (nx+2, ny+2, q), True on the one-cell halo (also where the domain is
-    periodic) and on solid BC voxels, then streamed."""
-    m = np.ones((nx + 2, ny + 2, lattice.q), dtype=bool)
-    m[1:-1, 1:-1, :] = False
+def grid_mask(nx, ny, lattice, solid_voxels, nz=0):
+    """Grid mask of ``src/elasticity.py:460-487`` / ``src/base.py:414-449`` on one
+    device: (nx+2, ny+2, [nz+2,] q), True on the one-cell halo (also where the
+    domain is periodic) and on solid BC voxels, then streamed."""
+    shape = (nx, ny) if lattice.d == 2 else (nx, ny, nz)
+    d = len(shape)
+    m = np.ones(tuple(n + 2 for n in shape) + (lattice.q,), dtype=bool)
+    m[tuple(slice(1, -1) for _ in shape)] = False
     if solid_voxels is not None:
         v = np.asarray(solid_voxels)
-        m[v[:, 0] + 1, v[:, 1] + 1, :] = True
+        m[tuple(v[:, k] + 1 for k in range(d))] = True
     out = np.empty_like(m)
     for i in range(lattice.q):
-        out[..., i] = np.roll(m[..., i], (int(lattice.c[0, i]), int(lattice.c[1, i])), axis=(0, 1))
+        out[..., i] = np.roll(m[..., i], tuple(int(lattice.c[k, i]) for k in range(d)), axis=tuple(range(d)))
     return out
 
 

@@ -552,6 +552,7 @@ struct FluidPhys : DarcyPhys<T_> {
 };
 
 #include "xlbb_push.cuh"
+#include "xlbb_fluid3.cuh"
 
 // Launch geometry of the sweeps: tx owned columns per CTA, strips of rows
 // chosen so that the grid holds about ctas_per_sm CTAs per SM (one wave),
@@ -1159,6 +1160,24 @@ static int fluid_sweep_t(const XlbbGrid* g, const XlbbDarcySweep* s, cudaStream_
     if (s->sumsq) launch_sweep<Ph, true>(c, g, st, a);
     else launch_sweep<Ph, false>(c, g, st, a);
     return check_launch("xlbb_fluid_sweep");
+}
+
+static bool grid3_ok(const XlbbGrid3* g) {
+    return g && g->nx > 0 && g->ny > 0 && g->nz > 0 && g->pitch >= g->nx && g->ny <= 65535 && g->nz <= 65535 &&
+           g->plane >= (long long)g->pitch * g->ny * g->nz && g->plane < (1LL << 31);
+}
+
+template <typename T, int Q>
+static int fluid3_sweep_t(const XlbbGrid3* g, const XlbbDarcySweep* s, cudaStream_t st) {
+    Fluid3Args<T, Q> a;
+    a.nx = g->nx; a.ny = g->ny; a.nz = g->nz; a.pitch = g->pitch; a.plane = g->plane;
+    a.f_in = static_cast<const T*>(s->f_in);
+    a.f_out = static_cast<T*>(s->f_out);
+    a.omega = T(s->omega);
+    a.pc = rules_view<T, Q>(s->pc);
+    a.ps = rules_view<T, Q>(s->ps);
+    launch_k(fluid3_push_kernel<T, Q>, dim3((g->nx + 127) / 128, g->ny, g->nz), 128, 0, st, a);
+    return check_launch("xlbb_fluid3_sweep");
 }
 
 static inline dim3 row_grid(int nx, int ny, int bs) { return dim3((nx + bs - 1) / bs, ny); }
@@ -2101,6 +2120,22 @@ int xlbb_fluid_sweep(int dtype, const XlbbGrid* g, const XlbbDarcySweep* s, int 
     if (dtype == XLBB_F64)
         return kbc ? fluid_sweep_t<double, true>(g, s, XLBB_STREAM(stream)) : fluid_sweep_t<double, false>(g, s, XLBB_STREAM(stream));
     return fail(XLBB_EUNSUPPORTED, "xlbb_fluid_sweep: dtype");
+}
+
+int xlbb_fluid3_sweep(int dtype, const XlbbGrid3* g, const XlbbDarcySweep* s, int q, void* stream) {
+    if (!grid3_ok(g) || !s || !s->f_in || !s->f_out) return fail(XLBB_EBADARG, "xlbb_fluid3_sweep: bad argument");
+    if (q != 19 && q != 27) return fail(XLBB_EBADARG, "xlbb_fluid3_sweep: q must be 19 or 27");
+    if (s->f_in == s->f_out) return fail(XLBB_EBADARG, "xlbb_fluid3_sweep: f_in and f_out must differ");
+    if (s->omega_field || s->source || s->ext_source || s->resid || s->sumsq)
+        return fail(XLBB_EBADARG, "xlbb_fluid3_sweep: omega_field, source, ext_source, resid and sumsq must be NULL");
+    const XlbbGrid rows = {g->nx, g->ny * g->nz, g->pitch, g->plane};
+    if (!rules_ok(s->pc, &rows) || !rules_ok(s->ps, &rows)) return fail(XLBB_EBADARG, "xlbb_fluid3_sweep: incomplete rules");
+    if (s->ps.count > 0 && s->ps.row_ptr && !s->ps.push)
+        return fail(XLBB_EUNSUPPORTED, "xlbb_fluid3_sweep: PostStreaming rules without push words");
+    const cudaStream_t st = XLBB_STREAM(stream);
+    if (dtype == XLBB_F32) return q == 19 ? fluid3_sweep_t<float, 19>(g, s, st) : fluid3_sweep_t<float, 27>(g, s, st);
+    if (dtype == XLBB_F64) return q == 19 ? fluid3_sweep_t<double, 19>(g, s, st) : fluid3_sweep_t<double, 27>(g, s, st);
+    return fail(XLBB_EUNSUPPORTED, "xlbb_fluid3_sweep: dtype");
 }
 
 int xlbb_darcy_gradient(int dtype, const XlbbGrid* g, const void* q, double scale, const XlbbRules* rules,

@@ -1,0 +1,119 @@
+// Three-dimensional BGK fluid sweep: the step of src/base.py:809-846 with the
+// BGK collision of src/models.py:9-34 on the D3Q19 and D3Q27 lattices
+// (velocity order and weights of src/lattice.py:132-182), the path of
+// examples/performance/MLUPS3d.py.  One thread per cell collides and pushes
+// every post-collision population to the cell it streams to (periodic wrap in
+// x, y and z); PostCollision rules are applied before the push, PostStreaming
+// rules through per-cell push words (as the 2D collide-and-push sweep does:
+// directions a destination rebuilds from its own post-collision values are
+// skipped by the pushing cell and written by the destination, whose push word
+// carries the rule flag in bit 31).  Rows are (y, z) pairs, row = z ny + y.
+// Included inside namespace xlbb.
+#pragma once
+
+// Velocity i of D3Q19 / D3Q27: the reference enumerates (x, y, z) over
+// {0, -1, 1}^3 with x slowest; k3 is the position of velocity i in that
+// 27-entry enumeration (D3Q19 leaves out the 8 corners k = 13, 14, 16, 17,
+// 22, 23, 25, 26).
+template <int Q>
+__host__ __device__ constexpr int k3(int i) {
+    return Q == 27 ? i
+                   : (i <= 12 ? i : i == 13 ? 15 : i == 14 ? 18 : i == 15 ? 19 : i == 16 ? 20 : i == 17 ? 21 : 24);
+}
+__host__ __device__ constexpr int v3(int d) { return d == 0 ? 0 : (d == 1 ? -1 : 1); }
+template <int Q>
+__host__ __device__ constexpr int c3x(int i) { return v3(k3<Q>(i) / 9); }
+template <int Q>
+__host__ __device__ constexpr int c3y(int i) { return v3((k3<Q>(i) / 3) % 3); }
+template <int Q>
+__host__ __device__ constexpr int c3z(int i) { return v3(k3<Q>(i) % 3); }
+
+// Weights by |c|^2: D3Q19 1/3, 2/36, 1/36; D3Q27 8/27, 2/27, 1/54, 1/216.
+template <typename T, int Q>
+__host__ __device__ constexpr T w3(int i) {
+    return Q == 19
+               ? ((c3x<Q>(i) * c3x<Q>(i) + c3y<Q>(i) * c3y<Q>(i) + c3z<Q>(i) * c3z<Q>(i)) == 0   ? T(1.0 / 3.0)
+                  : (c3x<Q>(i) * c3x<Q>(i) + c3y<Q>(i) * c3y<Q>(i) + c3z<Q>(i) * c3z<Q>(i)) == 1 ? T(2.0 / 36.0)
+                                                                                              : T(1.0 / 36.0))
+               : ((c3x<Q>(i) * c3x<Q>(i) + c3y<Q>(i) * c3y<Q>(i) + c3z<Q>(i) * c3z<Q>(i)) == 0   ? T(8.0 / 27.0)
+                  : (c3x<Q>(i) * c3x<Q>(i) + c3y<Q>(i) * c3y<Q>(i) + c3z<Q>(i) * c3z<Q>(i)) == 1 ? T(2.0 / 27.0)
+                  : (c3x<Q>(i) * c3x<Q>(i) + c3y<Q>(i) * c3y<Q>(i) + c3z<Q>(i) * c3z<Q>(i)) == 2 ? T(1.0 / 54.0)
+                                                                                              : T(1.0 / 216.0));
+}
+
+template <typename T, int Q>
+struct Fluid3Args {
+    int nx, ny, nz, pitch;
+    long long plane;
+    const T* f_in;
+    T* f_out;
+    T omega;
+    RulesView<T, Q> pc, ps;
+};
+
+template <typename T, int Q>
+__global__ void __launch_bounds__(128) fluid3_push_kernel(const Fluid3Args<T, Q> p) {
+    grid_dep_wait();
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y, z = blockIdx.z;
+    if (x >= p.nx) return;
+    const int row = z * p.ny + y;
+    const size_t o = (size_t)row * p.pitch + x;
+    const long long P = p.plane;
+    T f[Q];
+#pragma unroll
+    for (int i = 0; i < Q; ++i) f[i] = __ldg(p.f_in + (o + (size_t)i * P));
+    // src/base.py:748-772: rho = sum f, u = sum c f / rho (one reciprocal of rho)
+    T rho = f[0], jx = T(0), jy = T(0), jz = T(0);
+#pragma unroll
+    for (int i = 1; i < Q; ++i) rho += f[i];
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        if (c3x<Q>(i) > 0) jx += f[i]; else if (c3x<Q>(i) < 0) jx -= f[i];
+        if (c3y<Q>(i) > 0) jy += f[i]; else if (c3y<Q>(i) < 0) jy -= f[i];
+        if (c3z<Q>(i) > 0) jz += f[i]; else if (c3z<Q>(i) < 0) jz -= f[i];
+    }
+    const T irho = T(1) / rho;
+    const T ux = jx * irho, uy = jy * irho, uz = jz * irho;
+    const T usqr = T(1.5) * (ux * ux + uy * uy + uz * uz);
+    const T om = p.omega;
+    T fs[Q];
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        const T cu = T(3) * (T(c3x<Q>(i)) * ux + T(c3y<Q>(i)) * uy + T(c3z<Q>(i)) * uz);
+        const T feq = rho * w3<T, Q>(i) * (T(1) + cu * (T(1) + T(0.5) * cu) - usqr);
+        fs[i] = f[i] - om * (f[i] - feq);
+    }
+    if (p.pc.count > 0) {        // post-collision rules: source values are the step's input
+        const int r = probe_rule(load_probe(p.pc, row, x), x);
+        if (r >= 0) {
+#pragma unroll
+            for (int d = 0; d < Q; ++d) {
+                const uint8_t code = __ldg(p.pc.code + (size_t)r * Q + d);
+                const int k = code < Q ? code : (code < 2 * Q ? code - Q : 0);
+                fs[d] = rule_value<T, Q>(code, fs[d], pick<T, Q>(f, k), p.pc.cst[(size_t)r * Q + d]);
+            }
+        }
+    }
+    const uint32_t pw = p.ps.count > 0 ? __ldg(p.ps.push + (size_t)row * p.nx + x) : 0u;
+    const int xm = x == 0 ? p.nx - 1 : x - 1, xp = x == p.nx - 1 ? 0 : x + 1;
+    const int ym = y == 0 ? p.ny - 1 : y - 1, yp = y == p.ny - 1 ? 0 : y + 1;
+    const int zm = z == 0 ? p.nz - 1 : z - 1, zp = z == p.nz - 1 ? 0 : z + 1;
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        const int dx = c3x<Q>(i) > 0 ? xp : (c3x<Q>(i) < 0 ? xm : x);
+        const int dy = c3y<Q>(i) > 0 ? yp : (c3y<Q>(i) < 0 ? ym : y);
+        const int dz = c3z<Q>(i) > 0 ? zp : (c3z<Q>(i) < 0 ? zm : z);
+        if (!(pw & (1u << i))) p.f_out[((size_t)(dz * p.ny + dy) * p.pitch + dx) + (size_t)i * P] = fs[i];
+    }
+    if (pw & (1u << 31)) {       // this cell's post-streaming rules, from its own post-collision values
+        const int r = rule_at(p.ps, row, x);
+#pragma unroll
+        for (int d = 0; d < Q; ++d) {
+            const uint8_t code = __ldg(p.ps.code + (size_t)r * Q + d);
+            if (code != 2 * Q + 1) {
+                const int k = code < Q ? code : (code < 2 * Q ? code - Q : 0);
+                p.f_out[o + (size_t)d * P] = rule_value<T, Q>(code, T(0), pick<T, Q>(fs, k), p.ps.cst[(size_t)r * Q + d]);
+            }
+        }
+    }
+}

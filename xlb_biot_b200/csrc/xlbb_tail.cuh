@@ -132,7 +132,7 @@ template <typename T, typename TC>
 __global__ void __launch_bounds__(TAIL_THREADS) batched_tail_kernel(const XlbbBatchTail* __restrict__ tails,
                                                                      double gamma, int k, size_t smem_bytes) {
     grid_dep_wait();
-    extern __shared__ __align__(16) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char smem[];
     const XlbbBatchTail tl = tails[blockIdx.x];
     const int m = tl.levels;
     // a record that does not fit the launch is skipped (nothing is touched)

@@ -28,6 +28,8 @@ class AdvectionDiffusionReactionBGK(LBMBase):
     """``src/darcy.py:22-296``."""
 
     def __init__(self, **kwargs):
+        if kwargs.get("nz", 0):
+            raise NotImplementedError("the Darcy (advection-diffusion) path is two-dimensional (nz = 0)")
         super().__init__(**kwargs)
         self.vel = kwargs.get("vel", None)
         if self.vel is None:

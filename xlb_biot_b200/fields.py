@@ -35,20 +35,34 @@ def pitch_for(nx, dtype):
 
 class Layout:
     """Pitch/plane of all fields of one grid, so that one kernel launch can take
-    several fields with the same geometry."""
+    several fields with the same geometry.  A three-dimensional grid (nz > 0)
+    stores its rows (y, z) as ny * nz rows of one plane, z slowest; users see
+    an (nx, ny, nz, c) view."""
 
-    def __init__(self, nx, ny, dtype, device=None):
-        self.nx, self.ny, self.dtype = int(nx), int(ny), dtype
+    def __init__(self, nx, ny, dtype, device=None, nz=0):
+        self.nx, self.ny, self.nz, self.dtype = int(nx), int(ny), int(nz), dtype
         self.device = device if device is not None else torch.device("cuda", torch.cuda.current_device())
         self.pitch = pitch_for(nx, dtype)
-        self.plane = self.pitch * self.ny
+        self.rows = self.ny * (self.nz if self.nz > 0 else 1)
+        self.plane = self.pitch * self.rows
+
+    @property
+    def shape(self):
+        return (self.nx, self.ny) if self.nz == 0 else (self.nx, self.ny, self.nz)
 
     def grid(self):
-        return _lib.Grid(self.nx, self.ny, self.pitch, self.plane)
+        """The 2-D grid of the kernels: nx columns, all rows (ny, or ny * nz)."""
+        return _lib.Grid(self.nx, self.rows, self.pitch, self.plane)
+
+    def grid3(self):
+        return _lib.Grid3(self.nx, self.ny, max(self.nz, 1), self.pitch, self.plane)
+
+    def _strides(self):
+        return (1, self.pitch) if self.nz == 0 else (1, self.pitch, self.pitch * self.ny)
 
     def empty(self, c):
         buf = torch.empty(c * self.plane, dtype=self.dtype, device=self.device)
-        return buf.as_strided((self.nx, self.ny, c), (1, self.pitch, self.plane))
+        return buf.as_strided(self.shape + (c,), self._strides() + (self.plane,))
 
     def zeros(self, c):
         t = self.empty(c)
@@ -56,15 +70,20 @@ class Layout:
         return t
 
     def conforms(self, t, c=None):
-        return (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == self.dtype and t.dim() == 3
-                and t.shape[0] == self.nx and t.shape[1] == self.ny and (c is None or t.shape[2] == c)
-                and t.stride(0) == 1 and (self.ny == 1 or t.stride(1) == self.pitch)
-                and (t.shape[2] == 1 or t.stride(2) == self.plane)
-                and t.device == self.device)
+        nd = len(self.shape)
+        if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == self.dtype and t.dim() == nd + 1
+                and tuple(t.shape[:nd]) == self.shape and (c is None or t.shape[nd] == c)
+                and t.device == self.device):
+            return False
+        st = self._strides()
+        for k in range(nd):
+            if t.shape[k] > 1 and t.stride(k) != st[k]:
+                return False
+        return t.shape[nd] == 1 or t.stride(nd) == self.plane
 
     def field(self, x, c=None):
         """A conforming tensor with the values of ``x`` (numpy array, torch tensor
-        or scalar broadcast to ``(nx, ny, c)``); no copy if ``x`` conforms."""
+        or scalar broadcast to ``shape + (c,)``); no copy if ``x`` conforms."""
         if x is None:
             return None
         if self.conforms(x, c):
@@ -73,15 +92,21 @@ class Layout:
             src = x.to(device=self.device, dtype=self.dtype)
         else:
             src = torch.as_tensor(np.asarray(x), device=self.device).to(self.dtype)
-        if src.dim() == 2:
+        nd = len(self.shape)
+        if src.dim() == nd:
             src = src[..., None]
         if c is None:
-            c = src.shape[-1] if src.dim() == 3 else 1
+            c = src.shape[-1] if src.dim() == nd + 1 else 1
         out = self.empty(c)
-        out.copy_(torch.broadcast_to(src, (self.nx, self.ny, c)))
+        out.copy_(torch.broadcast_to(src, self.shape + (c,)))
         return out
 
 
 def buf_of(t):
     """The flat plane buffer behind a conforming field view."""
-    return t.as_strided((t.shape[2] * t.stride(2) if t.shape[2] > 1 else t.shape[1] * t.stride(1),), (1,))
+    c = t.shape[-1]
+    if c > 1:
+        n = c * t.stride(-1)
+    else:
+        n = t.shape[-2] * t.stride(-2)
+    return t.as_strided((n,), (1,))

@@ -1,15 +1,15 @@
-"""D2Q9 fluid collision models (``src/models.py``) on B200.
+"""Fluid collision models (``src/models.py``) on B200.
 
 ``BGKSim`` and ``KBCSim`` keep the reference's keywords, hooks
 (``set_boundary_conditions``, ``initialize_macroscopic_fields``,
 ``output_data``) and ``run``/``step`` loop (``src/base.py:809-948``); their step
-is one launch of the fused CUDA sweep ``xlbb_fluid_sweep`` (collision, compiled
-PostCollision rules, periodic streaming, compiled PostStreaming rules).  This
-is the fluid path of ``examples/performance/MLUPS2d.py`` (lid-driven cavity with
-``BounceBack`` and ``EquilibriumBC``).
+is one launch of a fused CUDA sweep (collision, compiled PostCollision rules,
+periodic streaming, compiled PostStreaming rules): ``xlbb_fluid_sweep`` on
+D2Q9 (BGK and KBC; the path of ``examples/performance/MLUPS2d.py``) and
+``xlbb_fluid3_sweep`` on D3Q19 / D3Q27 (BGK; ``MLUPS3d.py``), both with the
+lid-driven cavity's ``BounceBack`` and ``EquilibriumBC``.
 
-Scope: two dimensions, the D2Q9 lattice, no body force (``get_force`` must
-return None); the 3-D lattices of the reference's CFD examples are not built.
+Scope: no body force (``get_force`` must return None); KBC on D2Q9 only.
 """
 import time
 
@@ -31,8 +31,10 @@ class _FluidSim(LBMBase):
         super().__init__(**kwargs)
         if self._acc64:
             raise NotImplementedError("the fluid models compute in their storage type: use 'f32/f32' or 'f64/f64'")
-        if self.lattice.q != 9 or self.lattice.d != 2:
-            raise NotImplementedError("the fluid models run on the D2Q9 lattice")
+        if (self.lattice.d, self.lattice.q) not in ((2, 9), (3, 19), (3, 27)):
+            raise NotImplementedError("the fluid models run on the D2Q9, D3Q19 and D3Q27 lattices")
+        if self.dim == 3 and self._model != FLUID_BGK:
+            raise NotImplementedError("the 3-D fluid sweep implements the BGK collision")
         if self.force is not None:
             raise NotImplementedError("body forces (apply_force) are not implemented for the fluid models")
         self._partials = torch.empty(0, dtype=torch.float64, device=self._layout.device)
@@ -40,15 +42,19 @@ class _FluidSim(LBMBase):
 
     def _compile_rules(self):
         L = self._layout
-        self._pc = compile_rules(self.BCs, L.nx, L.ny, 9, self._dtype, L.device, step="PostCollision")
-        self._ps = compile_rules(self.BCs, L.nx, L.ny, 9, self._dtype, L.device, step="PostStreaming")
+        self._pc = compile_rules(self.BCs, L.nx, L.ny, self.q, self._dtype, L.device, step="PostCollision", nz=L.nz)
+        self._ps = compile_rules(self.BCs, L.nx, L.ny, self.q, self._dtype, L.device, step="PostStreaming", nz=L.nz)
+        if L.nz and self._ps.count and self._ps.push is None:
+            raise NotImplementedError("the 3-D fluid sweep applies PostStreaming rules that rebuild populations "
+                                      "from the cell's own post-collision values (no negated or shifted "
+                                      "streamed values)")
 
     # ------------------------------------------------------------------ kernels
     def update_macroscopic(self, f):
         """``src/base.py:748-772``: rho = sum f, u = sum c f / rho (device
         tensor algebra)."""
         L = self._layout
-        f = L.field(f, 9)
+        f = L.field(f, self.q)
         c = torch.as_tensor(self.c, device=L.device, dtype=L.dtype)
         rho = torch.sum(f, dim=-1, keepdim=True)
         return rho, (f @ c.T) / rho
@@ -56,7 +62,8 @@ class _FluidSim(LBMBase):
     def streaming(self, f):
         out = torch.empty_like(f)
         for i in range(self.q):
-            out[..., i] = torch.roll(f[..., i], (int(self.c[0, i]), int(self.c[1, i])), dims=(0, 1))
+            out[..., i] = torch.roll(f[..., i], tuple(int(self.c[k, i]) for k in range(self.dim)),
+                                     dims=tuple(range(self.dim)))
         return out
 
     def apply_bc(self, fout, fin, timestep, implementation_step):
@@ -64,7 +71,15 @@ class _FluidSim(LBMBase):
 
     def _sweep(self, f, out=None, sumsq=False):
         L = self._layout
-        out = L.empty(9) if out is None else out
+        out = L.empty(self.q) if out is None else out
+        if L.nz:
+            if sumsq:
+                raise NotImplementedError("the 3-D fluid sweep has no fused residual sum")
+            s = _lib.DarcySweep(f.data_ptr(), out.data_ptr(), float(self.omega), None, None, None,
+                                self._pc.struct(), self._ps.struct(), None)
+            _lib.check(_lib.lib().xlbb_fluid3_sweep(self._dcode, L.grid3(), s, self.q, _lib.stream_ptr()),
+                       "xlbb_fluid3_sweep")
+            return out
         if sumsq:
             n_max = _lib.check(_lib.lib().xlbb_darcy_sweep_ctas(self._dcode, L.grid()), "xlbb_darcy_sweep_ctas")
             if self._partials.numel() < n_max:
@@ -87,7 +102,7 @@ class _FluidSim(LBMBase):
     def step(self, f_poststreaming, timestep, return_fpost=False):
         """``src/base.py:809-846``: one fused sweep; with ``return_fpost`` the
         post-collision populations (after the PostCollision rules) as well."""
-        f = self._layout.field(f_poststreaming, 9)
+        f = self._layout.field(f_poststreaming, self.q)
         out = self._sweep(f)
         if return_fpost:
             return out, self.apply_bc(self.collision(f), f, timestep, "PostCollision")
@@ -102,7 +117,7 @@ class _FluidSim(LBMBase):
             ck = self.load_latest_checkpoint()
             if ck is not None:
                 latest = int(ck["timestep"])
-                f = self._layout.field(ck["f"], 9)
+                f = self._layout.field(ck["f"], self.q)
                 print(f"Restored checkpoint at step {latest}.")
                 start_step = latest + 1
                 if not (t_max > start_step):
@@ -129,9 +144,10 @@ class _FluidSim(LBMBase):
         if self.computeMLUPS:
             torch.cuda.synchronize()
             end = time.time()
-            print(f"Domain: {self.nx} x {self.ny}")
-            print(f"Number of voxels: {self.nx * self.ny}")
-            print(f"MLUPS: {self.nx * self.ny * t_max / (end - start) / 1e6}")
+            cells = self.nx * self.ny * (self.nz if self.dim == 3 else 1)
+            print("Domain: " + " x ".join(str(n) for n in (self.nx, self.ny, self.nz)[:self.dim]))
+            print(f"Number of voxels: {cells}")
+            print(f"MLUPS: {cells * t_max / (end - start) / 1e6}")
         return f
 
     def handle_io_timestep(self, timestep, f, fstar, rho, u, rho_prev, u_prev):
@@ -148,10 +164,10 @@ class BGKSim(_FluidSim):
         """The collision alone (API compatibility; the time loop uses the fused
         sweep).  Device tensor algebra."""
         L = self._layout
-        f = L.field(f, 9)
+        f = L.field(f, self.q)
         rho, u = self.update_macroscopic(f)
         feq = self.equilibrium(rho, u, cast_output=False)
-        return L.field(f - self.omega * (f - feq), 9)
+        return L.field(f - self.omega * (f - feq), self.q)
 
 
 class KBCSim(_FluidSim):

@@ -40,7 +40,7 @@ def homogeneous_rules(rules, ny, dtype, device):
     if rules.count == 0:
         return rules
     return CompiledRules(rules.q, ny, rules.cells, rules.code_np, np.zeros_like(rules.cst_np), dtype, device,
-                         rules.nx, push=True)
+                         rules.nx, push=True, shape=rules.shape, cells_nd=rules.cells_nd)
 
 
 def twin64(solver):
