@@ -218,16 +218,18 @@ typedef struct {
 } XlbbGrid3;
 
 /*
- * One fused D3Q19 (q = 19) or D3Q27 (q = 27) BGK fluid step (BGKSim.collision,
- * src/models.py:20-34, inside LBMBase.step, src/base.py:809-846, on the
- * lattices of src/lattice.py:132-182): collision, PostCollision rules,
+ * One fused D3Q19 (q = 19) or D3Q27 (q = 27) fluid step: model XLBB_FLUID_BGK
+ * (BGKSim.collision, src/models.py:20-34) on either lattice, XLBB_FLUID_KBC
+ * (KBCSim.collision, :47-72, shear decomposition :156-214) on D3Q27 only;
+ * inside LBMBase.step, src/base.py:809-846, on the lattices of
+ * src/lattice.py:132-182: collision, PostCollision rules,
  * streaming with periodic wrap in x, y and z, PostStreaming rules.  Uniform
  * omega only; omega_field, source, ext_source, resid and sumsq must be NULL
  * (XLBB_EBADARG), and PostStreaming rules need their push words
  * (XLBB_EUNSUPPORTED otherwise).  Replaces the step that
  * examples/performance/MLUPS3d.py times.
  */
-int xlbb_fluid3_sweep(int dtype, const XlbbGrid3* g, const XlbbDarcySweep* s, int q, void* stream);
+int xlbb_fluid3_sweep(int dtype, const XlbbGrid3* g, const XlbbDarcySweep* s, int q, int model, void* stream);
 
 /*
  * Darcy sweep plus its FP64 convergence residual, allocating nothing.

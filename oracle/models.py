@@ -130,7 +130,45 @@ class BGKSim(_FluidBase):
 
 
 class KBCSim(_FluidBase):
-    """``src/models.py:36-72,115-154`` (D2Q9)."""
+    """``src/models.py:36-72,115-214`` (D2Q9 and D3Q27)."""
+
+    def __init__(self, **kwargs):
+        # src/models.py:42-45
+        if kwargs.get("lattice").name != "D3Q27" and kwargs.get("nz") > 0:
+            raise ValueError("KBC collision operator in 3D must only be used with D3Q27 lattice.")
+        super().__init__(**kwargs)
+
+    def momentum_flux(self, fneq):
+        """``src/base.py:727-746``: fneq . cc, cc the products c_a c_b (a <= b,
+        row-major: xx, xy[, xz], yy[, yz, zz]) of ``src/lattice.py:184-210``."""
+        c = np.array(self.c, dtype=fneq.dtype)
+        d = c.shape[0]
+        cc = np.stack([c[a] * c[b] for a in range(d) for b in range(a, d)], axis=1)
+        return np.dot(fneq, cc)
+
+    def fdecompose_shear_d3q27(self, fneq):
+        """``src/models.py:156-214``: with Pi = (xx, xy, xz, yy, yz, zz),
+        N_xz = Pi_xx - Pi_zz and N_yz = Pi_yy - Pi_zz, the axis directions get
+        (2 N_xz - N_yz) / 6 (x), (2 N_yz - N_xz) / 6 (y), -(N_xz + N_yz) / 6 (z),
+        the face diagonals +-Pi_ab / 4 by the sign of c_a c_b, the rest and the
+        corners zero."""
+        Pi = self.momentum_flux(fneq)
+        nxz = Pi[..., 0] - Pi[..., 5]
+        nyz = Pi[..., 3] - Pi[..., 5]
+        s = np.zeros_like(fneq)
+        s[..., 9] = (2.0 * nxz - nyz) / 6.0
+        s[..., 18] = (2.0 * nxz - nyz) / 6.0
+        s[..., 3] = (-nxz + 2.0 * nyz) / 6.0
+        s[..., 6] = (-nxz + 2.0 * nyz) / 6.0
+        s[..., 1] = (-nxz - nyz) / 6.0
+        s[..., 2] = (-nxz - nyz) / 6.0
+        for i, j, comp in ((12, 24, 1), (10, 20, 2), (8, 4, 4)):      # c_a c_b = +1
+            s[..., i] = Pi[..., comp] / 4.0
+            s[..., j] = Pi[..., comp] / 4.0
+        for i, j, comp in ((21, 15, 1), (19, 11, 2), (7, 5, 4)):      # c_a c_b = -1
+            s[..., i] = -Pi[..., comp] / 4.0
+            s[..., j] = -Pi[..., comp] / 4.0
+        return s
 
     def fdecompose_shear_d2q9(self, fneq):
         """``src/models.py:127-154``; momentum flux ``fneq . cc`` with
@@ -157,7 +195,10 @@ class KBCSim(_FluidBase):
         rho, u = self.update_macroscopic(f)
         feq = self.equilibrium(rho, u, cast_output=False)
         fneq = f - feq
-        deltaS = self.fdecompose_shear_d2q9(fneq) * rho / 4.0
+        if self.dim == 2:
+            deltaS = self.fdecompose_shear_d2q9(fneq) * rho / 4.0
+        else:
+            deltaS = self.fdecompose_shear_d3q27(fneq) * rho
         deltaH = fneq - deltaS
         invBeta = 1.0 / beta
         gamma = invBeta - (2.0 - invBeta) * np.sum(deltaS * deltaH / feq, axis=-1) / (

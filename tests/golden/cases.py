@@ -237,7 +237,7 @@ def parameters_terzaghi(m, alpha=0.8):
 
 def fluid_cavity(m, model, lattice="D2Q9", n=(24, 20), t_max=20):
     """The cavities of ``examples/performance/MLUPS2d.py`` (BGK and KBC on
-    D2Q9) and ``MLUPS3d.py`` (BGK on D3Q19 / D3Q27) through the reference's
+    D2Q9) and ``MLUPS3d.py`` (BGK on D3Q19 / D3Q27; KBC on D3Q27) through the reference's
     ``run`` (``src/base.py:848-948``): t_max + 1 steps from rest."""
     from xlb_biot_b200.workloads import lid_driven_cavity, lid_driven_cavity_3d
     if lattice == "D2Q9":
@@ -245,7 +245,7 @@ def fluid_cavity(m, model, lattice="D2Q9", n=(24, 20), t_max=20):
         s = C(lattice=m.LatticeD2Q9(PREC), omega=om(n[0]), nx=n[0], ny=n[1], nz=0, precision=PREC,
               print_info_rate=0)
     else:
-        C, om = lid_driven_cavity_3d(m)
+        C, om = lid_driven_cavity_3d(m, model=model)
         lat = getattr(m, "Lattice" + lattice)(PREC)
         s = C(lattice=lat, omega=om(n[0]), nx=n[0], ny=n[1], nz=n[2], precision=PREC, print_info_rate=0)
     f = s.run(t_max)
@@ -278,6 +278,7 @@ CASES = {
     "fluid_cavity_kbc_d2q9": lambda m: fluid_cavity(m, "kbc"),
     "fluid_cavity_bgk_d3q19": lambda m: fluid_cavity(m, "bgk", "D3Q19", (10, 8, 12)),
     "fluid_cavity_bgk_d3q27": lambda m: fluid_cavity(m, "bgk", "D3Q27", (10, 8, 12)),
+    "fluid_cavity_kbc_d3q27": lambda m: fluid_cavity(m, "kbc", "D3Q27", (10, 8, 12)),
 }
 
 # relative tolerance of each case (FP64 runs: 1e-12; FP32 storage: 1e-5)

@@ -12,7 +12,9 @@ omega array on the solver directly (the reference's ``omega`` setter accepts
 floats only, ``src/base.py:166-173``; its collision expressions broadcast an
 array).
 
-    python tests/golden/make_golden.py [--reference /path/to/xlb-biot]
+    python tests/golden/make_golden.py [--reference /path/to/xlb-biot] [--cases NAME ...]
+
+``--cases`` regenerates only the named cases and keeps the others' arrays.
 """
 import argparse
 import json
@@ -53,19 +55,32 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default=os.environ.get("XLB_BIOT_REFERENCE", "/root/reference"))
     ap.add_argument("--out", default=OUT)
+    ap.add_argument("--cases", nargs="*", default=None)
     args = ap.parse_args()
     m = reference_namespace(args.reference)
     sys.path.insert(0, HERE)
     from cases import CASES
+    import numpy as np
     arrays, manifest = {}, {}
-    for name, case in CASES.items():
+    todo = CASES
+    if args.cases:
+        unknown = sorted(set(args.cases) - set(CASES))
+        if unknown:
+            raise SystemExit(f"unknown cases: {unknown}")
+        with np.load(args.out) as old:
+            for key in old.files:
+                name = key.split("/")[0]
+                if name in CASES and name not in args.cases:
+                    arrays[key] = old[key]
+                    manifest.setdefault(name, {})[key.split("/", 1)[1]] = list(old[key].shape)
+        todo = {k: CASES[k] for k in args.cases}
+    for name, case in todo.items():
         t0 = time.time()
         res = case(m)
         manifest[name] = {k: list(v.shape) for k, v in res.items()}
         for k, v in res.items():
             arrays[f"{name}/{k}"] = v
         print(f"{name}: {sorted(res)} ({time.time() - t0:.1f} s)", file=sys.stderr)
-    import numpy as np
     np.savez_compressed(args.out, **arrays)
     with open(os.path.splitext(args.out)[0] + ".json", "w") as fh:
         json.dump({"generator": "tests/golden/make_golden.py", "source": "s-lunowa/xlb-biot src/*.py under the "

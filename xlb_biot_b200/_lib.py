@@ -119,7 +119,7 @@ SIGNATURES = {
     "xlbb_darcy_sweep_partials": (I, [I, PG, ctypes.POINTER(DarcySweep)]),
     "xlbb_darcy_sweep_pipeline": (I, [I, PG, ctypes.POINTER(DarcySweep)]),
     "xlbb_fluid_sweep": (I, [I, PG, ctypes.POINTER(DarcySweep), I, P]),
-    "xlbb_fluid3_sweep": (I, [I, ctypes.POINTER(Grid3), ctypes.POINTER(DarcySweep), I, P]),
+    "xlbb_fluid3_sweep": (I, [I, ctypes.POINTER(Grid3), ctypes.POINTER(DarcySweep), I, I, P]),
     "xlbb_darcy_sweep_residual_noalloc": (I, [I, PG, ctypes.POINTER(DarcySweep), P, P]),
     "xlbb_darcy_gradient": (I, [I, PG, P, D, ctypes.POINTER(Rules), P, P, P]),
     "xlbb_elast_divgrad": (I, [I, PG, ctypes.POINTER(ElastMaterial), D, P, D, ctypes.POINTER(Rules), P, P, P]),

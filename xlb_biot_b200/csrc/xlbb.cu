@@ -1167,7 +1167,7 @@ static bool grid3_ok(const XlbbGrid3* g) {
            g->plane >= (long long)g->pitch * g->ny * g->nz && g->plane < (1LL << 31);
 }
 
-template <typename T, int Q>
+template <typename T, int Q, bool KBC = false>
 static int fluid3_sweep_t(const XlbbGrid3* g, const XlbbDarcySweep* s, cudaStream_t st) {
     Fluid3Args<T, Q> a;
     a.nx = g->nx; a.ny = g->ny; a.nz = g->nz; a.pitch = g->pitch; a.plane = g->plane;
@@ -1176,7 +1176,7 @@ static int fluid3_sweep_t(const XlbbGrid3* g, const XlbbDarcySweep* s, cudaStrea
     a.omega = T(s->omega);
     a.pc = rules_view<T, Q>(s->pc);
     a.ps = rules_view<T, Q>(s->ps);
-    launch_k(fluid3_push_kernel<T, Q>, dim3((g->nx + 127) / 128, g->ny, g->nz), 128, 0, st, a);
+    launch_k(fluid3_push_kernel<T, Q, KBC>, dim3((g->nx + 127) / 128, g->ny, g->nz), 128, 0, st, a);
     return check_launch("xlbb_fluid3_sweep");
 }
 
@@ -2122,9 +2122,11 @@ int xlbb_fluid_sweep(int dtype, const XlbbGrid* g, const XlbbDarcySweep* s, int 
     return fail(XLBB_EUNSUPPORTED, "xlbb_fluid_sweep: dtype");
 }
 
-int xlbb_fluid3_sweep(int dtype, const XlbbGrid3* g, const XlbbDarcySweep* s, int q, void* stream) {
+int xlbb_fluid3_sweep(int dtype, const XlbbGrid3* g, const XlbbDarcySweep* s, int q, int model, void* stream) {
     if (!grid3_ok(g) || !s || !s->f_in || !s->f_out) return fail(XLBB_EBADARG, "xlbb_fluid3_sweep: bad argument");
     if (q != 19 && q != 27) return fail(XLBB_EBADARG, "xlbb_fluid3_sweep: q must be 19 or 27");
+    if (model != XLBB_FLUID_BGK && !(model == XLBB_FLUID_KBC && q == 27))
+        return fail(XLBB_EBADARG, "xlbb_fluid3_sweep: model (KBC needs q = 27)");
     if (s->f_in == s->f_out) return fail(XLBB_EBADARG, "xlbb_fluid3_sweep: f_in and f_out must differ");
     if (s->omega_field || s->source || s->ext_source || s->resid || s->sumsq)
         return fail(XLBB_EBADARG, "xlbb_fluid3_sweep: omega_field, source, ext_source, resid and sumsq must be NULL");
@@ -2133,8 +2135,13 @@ int xlbb_fluid3_sweep(int dtype, const XlbbGrid3* g, const XlbbDarcySweep* s, in
     if (s->ps.count > 0 && s->ps.row_ptr && !s->ps.push)
         return fail(XLBB_EUNSUPPORTED, "xlbb_fluid3_sweep: PostStreaming rules without push words");
     const cudaStream_t st = XLBB_STREAM(stream);
-    if (dtype == XLBB_F32) return q == 19 ? fluid3_sweep_t<float, 19>(g, s, st) : fluid3_sweep_t<float, 27>(g, s, st);
-    if (dtype == XLBB_F64) return q == 19 ? fluid3_sweep_t<double, 19>(g, s, st) : fluid3_sweep_t<double, 27>(g, s, st);
+    const bool kbc = model == XLBB_FLUID_KBC;
+    if (dtype == XLBB_F32)
+        return q == 19 ? fluid3_sweep_t<float, 19>(g, s, st)
+                       : (kbc ? fluid3_sweep_t<float, 27, true>(g, s, st) : fluid3_sweep_t<float, 27>(g, s, st));
+    if (dtype == XLBB_F64)
+        return q == 19 ? fluid3_sweep_t<double, 19>(g, s, st)
+                       : (kbc ? fluid3_sweep_t<double, 27, true>(g, s, st) : fluid3_sweep_t<double, 27>(g, s, st));
     return fail(XLBB_EUNSUPPORTED, "xlbb_fluid3_sweep: dtype");
 }
 

@@ -1,5 +1,6 @@
-// Three-dimensional BGK fluid sweep: the step of src/base.py:809-846 with the
-// BGK collision of src/models.py:9-34 on the D3Q19 and D3Q27 lattices
+// Three-dimensional fluid sweep: the step of src/base.py:809-846 with the BGK
+// collision of src/models.py:9-34 on the D3Q19 and D3Q27 lattices, or the KBC
+// collision of src/models.py:36-72 on D3Q27
 // (velocity order and weights of src/lattice.py:132-182), the path of
 // examples/performance/MLUPS3d.py.  One thread per cell collides and pushes
 // every post-collision population to the cell it streams to (periodic wrap in
@@ -51,8 +52,30 @@ struct Fluid3Args {
     RulesView<T, Q> pc, ps;
 };
 
+// Shear part of a D3Q27 non-equilibrium population per unit density
+// (src/models.py:156-214): with the momentum flux Pi of fneq, N_xz = Pi_xx -
+// Pi_zz and N_yz = Pi_yy - Pi_zz, the axis directions carry (2 N_xz - N_yz) / 6
+// (x), (2 N_yz - N_xz) / 6 (y), -(N_xz + N_yz) / 6 (z), the face diagonals
+// c_a c_b Pi_ab / 4, the rest population and the corners nothing.
 template <typename T, int Q>
+__device__ __forceinline__ T kbc_shear3(int i, T nxz, T nyz, T pxy, T pxz, T pyz) {
+    const int ax = c3x<Q>(i) * c3x<Q>(i), ay = c3y<Q>(i) * c3y<Q>(i), az = c3z<Q>(i) * c3z<Q>(i);
+    if (ax + ay + az == 1) {
+        if (ax) return (T(2) * nxz - nyz) / T(6);
+        if (ay) return (-nxz + T(2) * nyz) / T(6);
+        return (-nxz - nyz) / T(6);
+    }
+    if (ax + ay + az == 2) {
+        if (!az) return T(c3x<Q>(i) * c3y<Q>(i)) * (pxy / T(4));
+        if (!ay) return T(c3x<Q>(i) * c3z<Q>(i)) * (pxz / T(4));
+        return T(c3y<Q>(i) * c3z<Q>(i)) * (pyz / T(4));
+    }
+    return T(0);
+}
+
+template <typename T, int Q, bool KBC>
 __global__ void __launch_bounds__(128) fluid3_push_kernel(const Fluid3Args<T, Q> p) {
+    static_assert(!KBC || Q == 27, "the KBC collision is defined on D3Q27");
     grid_dep_wait();
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y, z = blockIdx.z;
     if (x >= p.nx) return;
@@ -77,11 +100,49 @@ __global__ void __launch_bounds__(128) fluid3_push_kernel(const Fluid3Args<T, Q>
     const T usqr = T(1.5) * (ux * ux + uy * uy + uz * uz);
     const T om = p.omega;
     T fs[Q];
+    if constexpr (!KBC) {
 #pragma unroll
-    for (int i = 0; i < Q; ++i) {
-        const T cu = T(3) * (T(c3x<Q>(i)) * ux + T(c3y<Q>(i)) * uy + T(c3z<Q>(i)) * uz);
-        const T feq = rho * w3<T, Q>(i) * (T(1) + cu * (T(1) + T(0.5) * cu) - usqr);
-        fs[i] = f[i] - om * (f[i] - feq);
+        for (int i = 0; i < Q; ++i) {
+            const T cu = T(3) * (T(c3x<Q>(i)) * ux + T(c3y<Q>(i)) * uy + T(c3z<Q>(i)) * uz);
+            const T feq = rho * w3<T, Q>(i) * (T(1) + cu * (T(1) + T(0.5) * cu) - usqr);
+            fs[i] = f[i] - om * (f[i] - feq);
+        }
+    } else {
+        // src/models.py:47-72: fs (here) holds feq until the last loop
+        T pxx = T(0), pxy = T(0), pxz = T(0), pyy = T(0), pyz = T(0), pzz = T(0);
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            const T cu = T(3) * (T(c3x<Q>(i)) * ux + T(c3y<Q>(i)) * uy + T(c3z<Q>(i)) * uz);
+            fs[i] = rho * w3<T, Q>(i) * (T(1) + cu * (T(1) + T(0.5) * cu) - usqr);
+            const T fn = f[i] - fs[i];
+            if (c3x<Q>(i)) pxx += fn;
+            if (c3y<Q>(i)) pyy += fn;
+            if (c3z<Q>(i)) pzz += fn;
+            if (c3x<Q>(i) * c3y<Q>(i) > 0) pxy += fn; else if (c3x<Q>(i) * c3y<Q>(i) < 0) pxy -= fn;
+            if (c3x<Q>(i) * c3z<Q>(i) > 0) pxz += fn; else if (c3x<Q>(i) * c3z<Q>(i) < 0) pxz -= fn;
+            if (c3y<Q>(i) * c3z<Q>(i) > 0) pyz += fn; else if (c3y<Q>(i) * c3z<Q>(i) < 0) pyz -= fn;
+        }
+        const T nxz = pxx - pzz, nyz = pyy - pzz;
+        // entropic products <x, y> = sum x y / feq, one reciprocal of feq per
+        // direction shared by both products
+        T sh = T(0), hh = T(0);
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            const T dS = kbc_shear3<T, Q>(i, nxz, nyz, pxy, pxz, pyz) * rho;
+            const T dH = (f[i] - fs[i]) - dS;
+            const T ife = T(1) / fs[i];
+            sh += (dS * dH) * ife;
+            hh += (dH * dH) * ife;
+        }
+        const T beta = om * T(0.5);
+        const T ib = T(1) / beta;
+        const T gamma = ib - (T(2) - ib) * sh / (T(1e-32) + hh);
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            const T dS = kbc_shear3<T, Q>(i, nxz, nyz, pxy, pxz, pyz) * rho;
+            const T dH = (f[i] - fs[i]) - dS;
+            fs[i] = f[i] - beta * (T(2) * dS + gamma * dH);
+        }
     }
     if (p.pc.count > 0) {        // post-collision rules: source values are the step's input
         const int r = probe_rule(load_probe(p.pc, row, x), x);

@@ -6,10 +6,11 @@
 is one launch of a fused CUDA sweep (collision, compiled PostCollision rules,
 periodic streaming, compiled PostStreaming rules): ``xlbb_fluid_sweep`` on
 D2Q9 (BGK and KBC; the path of ``examples/performance/MLUPS2d.py``) and
-``xlbb_fluid3_sweep`` on D3Q19 / D3Q27 (BGK; ``MLUPS3d.py``), both with the
-lid-driven cavity's ``BounceBack`` and ``EquilibriumBC``.
+``xlbb_fluid3_sweep`` on D3Q19 / D3Q27 (BGK, the path of ``MLUPS3d.py``;
+KBC on D3Q27), both with the lid-driven cavity's ``BounceBack`` and
+``EquilibriumBC``.
 
-Scope: no body force (``get_force`` must return None); KBC on D2Q9 only.
+Scope: no body force (``get_force`` must return None).
 """
 import time
 
@@ -33,8 +34,6 @@ class _FluidSim(LBMBase):
             raise NotImplementedError("the fluid models compute in their storage type: use 'f32/f32' or 'f64/f64'")
         if (self.lattice.d, self.lattice.q) not in ((2, 9), (3, 19), (3, 27)):
             raise NotImplementedError("the fluid models run on the D2Q9, D3Q19 and D3Q27 lattices")
-        if self.dim == 3 and self._model != FLUID_BGK:
-            raise NotImplementedError("the 3-D fluid sweep implements the BGK collision")
         if self.force is not None:
             raise NotImplementedError("body forces (apply_force) are not implemented for the fluid models")
         self._partials = torch.empty(0, dtype=torch.float64, device=self._layout.device)
@@ -77,7 +76,8 @@ class _FluidSim(LBMBase):
                 raise NotImplementedError("the 3-D fluid sweep has no fused residual sum")
             s = _lib.DarcySweep(f.data_ptr(), out.data_ptr(), float(self.omega), None, None, None,
                                 self._pc.struct(), self._ps.struct(), None)
-            _lib.check(_lib.lib().xlbb_fluid3_sweep(self._dcode, L.grid3(), s, self.q, _lib.stream_ptr()),
+            _lib.check(_lib.lib().xlbb_fluid3_sweep(self._dcode, L.grid3(), s, self.q, self._model,
+                                                    _lib.stream_ptr()),
                        "xlbb_fluid3_sweep")
             return out
         if sumsq:
@@ -171,8 +171,9 @@ class BGKSim(_FluidSim):
 
 
 class KBCSim(_FluidSim):
-    """``src/models.py:36-72``: the entropic KBC collision (D2Q9 shear
-    decomposition ``fdecompose_shear_d2q9``, ``:127-154``)."""
+    """``src/models.py:36-72``: the entropic KBC collision (shear
+    decompositions ``fdecompose_shear_d2q9``, ``:127-154``, and
+    ``fdecompose_shear_d3q27``, ``:156-214``)."""
     _model = FLUID_KBC
 
     def __init__(self, **kwargs):
@@ -191,16 +192,39 @@ class KBCSim(_FluidSim):
             s[..., i] = v
         return s
 
+    def momentum_flux(self, fneq):
+        """``src/base.py:727-746``: fneq . cc (cc: c_a c_b, a <= b)."""
+        return fneq @ torch.as_tensor(np.asarray(self.lattice.cc, dtype=np.float64), device=fneq.device,
+                                      dtype=fneq.dtype)
+
+    def fdecompose_shear_d3q27(self, fneq):
+        Pi = self.momentum_flux(fneq)
+        nxz = Pi[..., 0] - Pi[..., 5]
+        nyz = Pi[..., 3] - Pi[..., 5]
+        s = torch.zeros_like(fneq)
+        for i, v in ((9, (2.0 * nxz - nyz) / 6.0), (18, (2.0 * nxz - nyz) / 6.0),
+                     (3, (-nxz + 2.0 * nyz) / 6.0), (6, (-nxz + 2.0 * nyz) / 6.0),
+                     (1, (-nxz - nyz) / 6.0), (2, (-nxz - nyz) / 6.0)):
+            s[..., i] = v
+        for i, j, k in ((12, 24, 1), (10, 20, 2), (8, 4, 4)):
+            s[..., i] = s[..., j] = Pi[..., k] / 4.0
+        for i, j, k in ((21, 15, 1), (19, 11, 2), (7, 5, 4)):
+            s[..., i] = s[..., j] = -Pi[..., k] / 4.0
+        return s
+
     def collision(self, f):
         """The collision alone (API compatibility).  Device tensor algebra."""
         L = self._layout
-        f = L.field(f, 9)
+        f = L.field(f, self.q)
         rho, u = self.update_macroscopic(f)
         feq = self.equilibrium(rho, u, cast_output=False)
         fneq = f - feq
-        dS = self.fdecompose_shear_d2q9(fneq) * rho / 4.0
+        if self.dim == 2:
+            dS = self.fdecompose_shear_d2q9(fneq) * rho / 4.0
+        else:
+            dS = self.fdecompose_shear_d3q27(fneq) * rho
         dH = fneq - dS
         beta = self.omega * 0.5
         ib = 1.0 / beta
         gamma = ib - (2.0 - ib) * torch.sum(dS * dH / feq, -1) / (1e-32 + torch.sum(dH * dH / feq, -1))
-        return L.field(f - beta * (2.0 * dS + gamma[..., None] * dH), 9)
+        return L.field(f - beta * (2.0 * dS + gamma[..., None] * dH), self.q)

@@ -314,12 +314,15 @@ def lid_driven_cavity(m, model="bgk", u_wall=0.1, Re=100.0):
     return Cavity, omega
 
 
-def lid_driven_cavity_3d(m, u_wall=0.1, Re=100.0):
+def lid_driven_cavity_3d(m, u_wall=0.1, Re=100.0, model="bgk"):
     """The fluid workload of ``examples/performance/MLUPS3d.py``: a cubic
     cavity with full-way bounce-back on the left, right, bottom, front and back
     faces and the equilibrium of (rho = 1, u = (u_wall, 0, 0)) on the top face
-    (z = nz - 1), BGK collision.  Returns the solver class and ``omega(n)``."""
-    class Cavity3D(m.BGKSim):
+    (z = nz - 1); BGK collision as the example (``model="kbc"``: the KBC
+    collision, D3Q27 only).  Returns the solver class and ``omega(n)``."""
+    base = m.BGKSim if model == "bgk" else m.KBCSim
+
+    class Cavity3D(base):
         def set_boundary_conditions(self):
             bb = self.boundingBoxIndices
             walls = np.concatenate((bb["left"], bb["right"], bb["bottom"], bb["front"], bb["back"]))
