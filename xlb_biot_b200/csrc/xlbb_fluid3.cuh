@@ -42,6 +42,8 @@ __host__ __device__ constexpr T w3(int i) {
                                                                                               : T(1.0 / 216.0));
 }
 
+constexpr int FLUID3_THREADS = 128;    // threads per CTA (x extent of a CTA's row segment)
+
 template <typename T, int Q>
 struct Fluid3Args {
     int nx, ny, nz, pitch;
@@ -73,15 +75,22 @@ __device__ __forceinline__ T kbc_shear3(int i, T nxz, T nyz, T pxy, T pxz, T pyz
     return T(0);
 }
 
+// A rule reads the population of a direction chosen at run time: rule cells
+// stage the rule's source values in shared memory (one column per thread,
+// bank = thread) and index them there, instead of a Q-way register select
+// per rule direction (Q^2 selects per rule cell).
 template <typename T, int Q, bool KBC>
-__global__ void __launch_bounds__(128) fluid3_push_kernel(const Fluid3Args<T, Q> p) {
+__global__ void __launch_bounds__(FLUID3_THREADS) fluid3_push_kernel(const Fluid3Args<T, Q> p) {
     static_assert(!KBC || Q == 27, "the KBC collision is defined on D3Q27");
+    __shared__ T stage[Q][FLUID3_THREADS];
     grid_dep_wait();
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y, z = blockIdx.z;
     if (x >= p.nx) return;
     const int row = z * p.ny + y;
     const size_t o = (size_t)row * p.pitch + x;
     const long long P = p.plane;
+    // f: the cell's populations, collided in place (post-collision rules
+    // re-load the inputs they need, so the inputs need not stay in registers)
     T f[Q];
 #pragma unroll
     for (int i = 0; i < Q; ++i) f[i] = __ldg(p.f_in + (o + (size_t)i * P));
@@ -99,22 +108,22 @@ __global__ void __launch_bounds__(128) fluid3_push_kernel(const Fluid3Args<T, Q>
     const T ux = jx * irho, uy = jy * irho, uz = jz * irho;
     const T usqr = T(1.5) * (ux * ux + uy * uy + uz * uz);
     const T om = p.omega;
-    T fs[Q];
     if constexpr (!KBC) {
 #pragma unroll
         for (int i = 0; i < Q; ++i) {
             const T cu = T(3) * (T(c3x<Q>(i)) * ux + T(c3y<Q>(i)) * uy + T(c3z<Q>(i)) * uz);
             const T feq = rho * w3<T, Q>(i) * (T(1) + cu * (T(1) + T(0.5) * cu) - usqr);
-            fs[i] = f[i] - om * (f[i] - feq);
+            f[i] = f[i] - om * (f[i] - feq);
         }
     } else {
-        // src/models.py:47-72: fs (here) holds feq until the last loop
+        // src/models.py:47-72
+        T fe[Q];
         T pxx = T(0), pxy = T(0), pxz = T(0), pyy = T(0), pyz = T(0), pzz = T(0);
 #pragma unroll
         for (int i = 0; i < Q; ++i) {
             const T cu = T(3) * (T(c3x<Q>(i)) * ux + T(c3y<Q>(i)) * uy + T(c3z<Q>(i)) * uz);
-            fs[i] = rho * w3<T, Q>(i) * (T(1) + cu * (T(1) + T(0.5) * cu) - usqr);
-            const T fn = f[i] - fs[i];
+            fe[i] = rho * w3<T, Q>(i) * (T(1) + cu * (T(1) + T(0.5) * cu) - usqr);
+            const T fn = f[i] - fe[i];
             if (c3x<Q>(i)) pxx += fn;
             if (c3y<Q>(i)) pyy += fn;
             if (c3z<Q>(i)) pzz += fn;
@@ -129,8 +138,8 @@ __global__ void __launch_bounds__(128) fluid3_push_kernel(const Fluid3Args<T, Q>
 #pragma unroll
         for (int i = 0; i < Q; ++i) {
             const T dS = kbc_shear3<T, Q>(i, nxz, nyz, pxy, pxz, pyz) * rho;
-            const T dH = (f[i] - fs[i]) - dS;
-            const T ife = T(1) / fs[i];
+            const T dH = (f[i] - fe[i]) - dS;
+            const T ife = T(1) / fe[i];
             sh += (dS * dH) * ife;
             hh += (dH * dH) * ife;
         }
@@ -140,18 +149,21 @@ __global__ void __launch_bounds__(128) fluid3_push_kernel(const Fluid3Args<T, Q>
 #pragma unroll
         for (int i = 0; i < Q; ++i) {
             const T dS = kbc_shear3<T, Q>(i, nxz, nyz, pxy, pxz, pyz) * rho;
-            const T dH = (f[i] - fs[i]) - dS;
-            fs[i] = f[i] - beta * (T(2) * dS + gamma * dH);
+            const T dH = (f[i] - fe[i]) - dS;
+            f[i] = f[i] - beta * (T(2) * dS + gamma * dH);
         }
     }
+    const int t = threadIdx.x;
     if (p.pc.count > 0) {        // post-collision rules: source values are the step's input
         const int r = probe_rule(load_probe(p.pc, row, x), x);
         if (r >= 0) {
 #pragma unroll
+            for (int k = 0; k < Q; ++k) stage[k][t] = __ldg(p.f_in + (o + (size_t)k * P));
+#pragma unroll
             for (int d = 0; d < Q; ++d) {
                 const uint8_t code = __ldg(p.pc.code + (size_t)r * Q + d);
                 const int k = code < Q ? code : (code < 2 * Q ? code - Q : 0);
-                fs[d] = rule_value<T, Q>(code, fs[d], pick<T, Q>(f, k), p.pc.cst[(size_t)r * Q + d]);
+                f[d] = rule_value<T, Q>(code, f[d], stage[k][t], p.pc.cst[(size_t)r * Q + d]);
             }
         }
     }
@@ -164,16 +176,18 @@ __global__ void __launch_bounds__(128) fluid3_push_kernel(const Fluid3Args<T, Q>
         const int dx = c3x<Q>(i) > 0 ? xp : (c3x<Q>(i) < 0 ? xm : x);
         const int dy = c3y<Q>(i) > 0 ? yp : (c3y<Q>(i) < 0 ? ym : y);
         const int dz = c3z<Q>(i) > 0 ? zp : (c3z<Q>(i) < 0 ? zm : z);
-        if (!(pw & (1u << i))) p.f_out[((size_t)(dz * p.ny + dy) * p.pitch + dx) + (size_t)i * P] = fs[i];
+        if (!(pw & (1u << i))) p.f_out[((size_t)(dz * p.ny + dy) * p.pitch + dx) + (size_t)i * P] = f[i];
     }
     if (pw & (1u << 31)) {       // this cell's post-streaming rules, from its own post-collision values
         const int r = rule_at(p.ps, row, x);
+#pragma unroll
+        for (int k = 0; k < Q; ++k) stage[k][t] = f[k];
 #pragma unroll
         for (int d = 0; d < Q; ++d) {
             const uint8_t code = __ldg(p.ps.code + (size_t)r * Q + d);
             if (code != 2 * Q + 1) {
                 const int k = code < Q ? code : (code < 2 * Q ? code - Q : 0);
-                p.f_out[o + (size_t)d * P] = rule_value<T, Q>(code, T(0), pick<T, Q>(fs, k), p.ps.cst[(size_t)r * Q + d]);
+                p.f_out[o + (size_t)d * P] = rule_value<T, Q>(code, T(0), stage[k][t], p.ps.cst[(size_t)r * Q + d]);
             }
         }
     }
