@@ -412,6 +412,19 @@ int xlbb_batched_prolong_add_map(int dtype_fine, int dtype_coarse, const XlbbBat
                                  const int* map_dev, int nblocks, double* parts, const int* begin_dev, int ninst,
                                  double* norms, void* stream);
 int xlbb_segment_sum(const double* parts, const int* begin_dev, int nseg, double* out, void* stream);
+/*
+ * Removes the mean first moments (the mean of sum_i c_i f_i, the rigid
+ * displacement mode a periodic problem leaves undetermined) from the level-0
+ * populations of a batch: the fine fields of tr_dev (their coarse fields are
+ * not used), block map and begin_dev as for xlbb_batched_prolong_add_map;
+ * sums[2 i] / sums[2 i + 1] receive the FP64 moment sums of instance i before
+ * the shift; parts: caller scratch of 2 * nblocks doubles.  No counterpart in
+ * the reference (whose FP64 iteration keeps this mode at zero to rounding):
+ * the V-cycle from zero with a zero-mean force conserves it in exact
+ * arithmetic, and FP32 rounding makes it drift over hundreds of cycles.
+ */
+int xlbb_batched_remove_mean_moment(int dtype, const XlbbBatchTransfer* tr_dev, const int* map_dev, int nblocks,
+                                    double* parts, const int* begin_dev, int ninst, double* sums, void* stream);
 
 /*
  * Persistent multigrid tail of a periodic batch (the recursion of

@@ -12,6 +12,11 @@ import torch
 pytestmark = pytest.mark.gpu
 
 
+def G_c8():
+    from xlb_biot_b200.lattice import LatticeD2Q8
+    return LatticeD2Q8("f64/f64").c
+
+
 def _single(G, n, lam, mu, force, prec, levels, cycles, coarsest_precision=None, residual_precision=None):
     class E(G.LBMElasticity):
         def get_force(self):
@@ -85,8 +90,9 @@ def test_batched_per_instance_levels_fp64_coarsest(prec, tol, rp):
 
 def test_error_criterion_reaches_fp64_accuracy():
     """FP32 batch with the FP64-arithmetic level-0 residual, stopped by the
-    estimated-error criterion at 1e-6: every instance's displacement is within
-    a few 1e-6 of an all-FP64 batch solved to 1e-11."""
+    estimated-error criterion at 1e-6 and ending with the removal of the
+    drifted rigid-displacement mode: every instance's displacement is within
+    1e-6 of an all-FP64 batch solved to 1e-11."""
     from xlb_biot_b200.batched import BatchedElasticity
     from xlb_biot_b200.workloads import batch_instances
     sizes, lams, mus, forces = batch_instances(count=12, sizes=(32, 48, 64, 96), seed=2)
@@ -100,7 +106,33 @@ def test_error_criterion_reaches_fp64_accuracy():
     for i in range(len(sizes)):
         u, u64 = b.displacement(i), b64.displacement(i)
         err = float(torch.linalg.vector_norm(u - u64) / torch.linalg.vector_norm(u64))
-        assert err < 3e-6, (i, err)
+        assert err < 1e-6, (i, err)
+
+
+@pytest.mark.parametrize("prec", ["f64/f64", "f32/f32"])
+def test_remove_mean_moment_shifts_only_the_first_moments(prec):
+    """``remove_mean_moment`` on random populations: afterwards every instance's
+    mean first moments are zero, and each population moved by exactly
+    (cx_i m_x + cy_i m_y) / 6 with m the mean before -- the other moments of
+    every cell are unchanged."""
+    from xlb_biot_b200.batched import BatchedElasticity
+    sizes = [(16, 16), (24, 40), (64, 32)]
+    forces = [np.zeros((nx, ny, 2)) for nx, ny in sizes]
+    b = BatchedElasticity(sizes, [1.0] * 3, [1.0] * 3, forces, levels=2, precision=prec)
+    g = torch.Generator(device="cuda").manual_seed(3)
+    (arena,) = b.X[0].values()
+    arena.buf.copy_(torch.rand(arena.buf.shape, generator=g, device="cuda", dtype=arena.buf.dtype) + 0.25)
+    c = torch.as_tensor(np.asarray(G_c8(), dtype=np.float64), device="cuda")
+    before = [b.populations(i).double().clone() for i in range(3)]
+    b.remove_mean_moment()
+    torch.cuda.synchronize()
+    eps = 1e-13 if prec == "f64/f64" else 2e-7
+    for i in range(3):
+        f0, f1 = before[i], b.populations(i).double()
+        m = torch.einsum("xyq,dq->d", f0, c) / (f0.shape[0] * f0.shape[1])
+        expect = f0 - torch.einsum("d,dq->q", m, c) / 6.0
+        assert float((f1 - expect).abs().max()) <= eps * float(f0.abs().max()), i
+        assert float(torch.einsum("xyq,dq->d", f1, c).abs().max()) <= 10 * eps * float(f0.abs().sum()), i
 
 
 @pytest.mark.parametrize("prec", ["f64/f64", "f32/f32"])

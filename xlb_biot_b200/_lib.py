@@ -149,6 +149,7 @@ SIGNATURES = {
     "xlbb_batched_prolong_add_norms": (I, [I, I, P, I, P, P, P]),
     "xlbb_batched_prolong_add_map": (I, [I, I, P, P, I, P, P, I, P, P]),
     "xlbb_segment_sum": (I, [P, P, I, P, P]),
+    "xlbb_batched_remove_mean_moment": (I, [I, P, P, I, P, P, I, P, P]),
     "xlbb_elast_sweep_adjoint": (I, [I, PG, ctypes.POINTER(ElastMaterial), ctypes.POINTER(ElastSweepAdjoint), P]),
     "xlbb_darcy_sweep_adjoint": (I, [I, PG, ctypes.POINTER(DarcySweepAdjoint), P]),
     "xlbb_darcy_gradient_adjoint": (I, [I, PG, P, D, ctypes.POINTER(Rules), P, P]),

@@ -109,11 +109,13 @@ class BatchedElasticity:
     the top-most level where an instance's remaining levels fit in
     ``tail_smem`` bytes of shared memory, its V-cycle is finished by one
     launch for all instances (``xlbb_batched_tail``: a CTA per instance, the
-    levels in shared memory; same results as the level-by-level launches)."""
+    levels in shared memory; same results as the level-by-level launches).
+    ``remove_mean``: ``solve`` ends with ``remove_mean_moment`` (the rigid
+    displacement mode, zero in exact arithmetic, reset after FP32 drift)."""
 
     def __init__(self, sizes, lams, mus, forces, levels=5, gamma=0.75, k_smooth=2, precision="f32/f32",
                  coarsest_precision=None, residual_precision=None, strip_rows=16, ctas_per_sm=4, vectorized=True,
-                 persistent_tail=True, tail_smem=100 * 1024):
+                 persistent_tail=True, tail_smem=100 * 1024, remove_mean=True):
         _lib.require_cuda()
         lib = _lib.lib()
         if k_smooth % 2:
@@ -292,8 +294,39 @@ class BatchedElasticity:
                                                             nx, ny, lv[g] - t))
             buf = torch.as_tensor(np.frombuffer(bytes(recs), dtype=np.uint8).copy(), device=dev)
             self.tail = (buf, len(tail_ids), smem, _lib.dtype_code(dt), _lib.dtype_code(coarse_dt))
+        # records of xlbb_batched_remove_mean_moment: every instance's level-0 populations
+        self.remove_mean = bool(remove_mean)
+        self._mean = []
+        for d, ids in self.groups[0].items():
+            arena = self.X[0][d]
+            recs = (_lib.BatchTransfer * len(ids))()
+            for k, g in enumerate(ids):
+                nx, ny = self.shapes[0][g]
+                recs[k] = _lib.BatchTransfer(arena.ptr(g), None, nx, ny, arena.pitch[arena.pos[g]], 0,
+                                             arena.plane[arena.pos[g]], 0)
+            blocks, begin = balanced_block_map([self.shapes[0][g][0] * self.shapes[0][g][1] for g in ids])
+            self._mean.append((torch.as_tensor(np.frombuffer(bytes(recs), dtype=np.uint8).copy(), device=dev),
+                               torch.as_tensor(blocks.reshape(-1), device=dev), len(blocks),
+                               torch.as_tensor(begin, device=dev), len(ids),
+                               torch.zeros(2 * len(blocks), dtype=torch.float64, device=dev),
+                               torch.zeros(2 * len(ids), dtype=torch.float64, device=dev), _lib.dtype_code(d)))
         self.launches_per_cycle = 0
         self.graph = None
+
+    def remove_mean_moment(self):
+        """Sets the mean first moments of every instance's level-0 populations to
+        zero (``xlbb_batched_remove_mean_moment``).  A periodic problem leaves
+        the rigid displacement undetermined; the V-cycle from zero with a
+        zero-mean force keeps it at zero in exact arithmetic, and this restores
+        that invariant after FP32 rounding made it drift (a random walk that
+        grows with the number of cycles).  ``solve`` calls it once at the end
+        unless the batch was built with ``remove_mean=False``."""
+        lib = _lib.lib()
+        for rec, mp, nb, begin, ni, parts, sums, code in self._mean:
+            _lib.check(lib.xlbb_batched_remove_mean_moment(
+                code, ctypes.c_void_p(rec.data_ptr()), ctypes.c_void_p(mp.data_ptr()), nb,
+                ctypes.c_void_p(parts.data_ptr()), ctypes.c_void_p(begin.data_ptr()), ni,
+                ctypes.c_void_p(sums.data_ptr()), _lib.stream_ptr()), "xlbb_batched_remove_mean_moment")
 
     # ------------------------------------------------------------------ kernels
     def _sweep(self, l, ln, a, b, sumsq=False, zero_in=False):
@@ -408,6 +441,8 @@ class BatchedElasticity:
                 self.converged_at[(self.converged_at < 0) & (rel < tol)] = cycles
                 if np.all(rel < tol):
                     break
+            if self.remove_mean:
+                self.remove_mean_moment()
             return cycles, rel
         if criterion != "error":
             raise ValueError("criterion must be 'residual' or 'error'")
@@ -436,6 +471,8 @@ class BatchedElasticity:
             prev = c
             if np.all(self.converged_at >= 0):
                 break
+        if self.remove_mean:
+            self.remove_mean_moment()
         return cycles, est
 
     def populations(self, i):
