@@ -1927,6 +1927,72 @@ __global__ void __launch_bounds__(256) batched_prolong_map_kernel(const XlbbBatc
     }
 }
 
+// The mean first moments of a batch's level-0 populations (the mean of
+// sum_i c_i f_i over an instance's cells, the displacement mode that a
+// periodic problem leaves undetermined).  In exact arithmetic the V-cycle
+// from zero with a zero-mean force keeps it at zero (collision adds the
+// force, streaming and the transfers conserve it, the restricted residual has
+// none); FP32 rounding makes it drift.  moment_map: FP64 partial sums of
+// sum_i cx_i f_i and sum_i cy_i f_i over a block's cells (block map as the
+// prolongation's); shift_map: f_i -= (cx_i mx + cy_i my) / 6, which moves the
+// first moments by (mx, my) and leaves the others unchanged (sum_i c_i c_i^T
+// = 6 I on D2Q8, odd moments of c vanish).
+template <typename T>
+__global__ void __launch_bounds__(256) batched_moment_map_kernel(const XlbbBatchTransfer* __restrict__ tr,
+                                                                  const int2* __restrict__ map, int nb,
+                                                                  double* parts) {
+    grid_dep_wait();
+    __shared__ double red[8];
+    const int2 m = map[blockIdx.x];
+    const XlbbBatchTransfer T_ = tr[m.x];
+    const T* __restrict__ ff = static_cast<const T*>(T_.fine);
+    const int n = T_.nx_f * T_.ny_f;
+    double sx = 0.0, sy = 0.0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int e = m.y + k * 256 + threadIdx.x;
+        if (e < n) {
+            const size_t of = (size_t)(e / T_.nx_f) * T_.pitch_f + e % T_.nx_f;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const double v = (double)__ldg(ff + of + (size_t)i * T_.plane_f);
+                sx += cx8(i) * v;
+                sy += cy8(i) * v;
+            }
+        }
+    }
+    const double a = block_sum(sx, red);
+    const double b = block_sum(sy, red);
+    if (threadIdx.x == 0) {
+        parts[blockIdx.x] = a;
+        parts[nb + blockIdx.x] = b;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) batched_shift_map_kernel(const XlbbBatchTransfer* __restrict__ tr,
+                                                                 const int2* __restrict__ map,
+                                                                 const double* __restrict__ sums) {
+    grid_dep_wait();
+    const int2 m = map[blockIdx.x];
+    const XlbbBatchTransfer T_ = tr[m.x];
+    T* __restrict__ ff = static_cast<T*>(const_cast<void*>(T_.fine));
+    const int n = T_.nx_f * T_.ny_f;
+    const double mx = sums[2 * m.x] / n, my = sums[2 * m.x + 1] / n;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int e = m.y + k * 256 + threadIdx.x;
+        if (e < n) {
+            const size_t of = (size_t)(e / T_.nx_f) * T_.pitch_f + e % T_.nx_f;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const size_t a = of + (size_t)i * T_.plane_f;
+                ff[a] = T((double)ff[a] - (cx8(i) * mx + cy8(i) * my) / 6.0);
+            }
+        }
+    }
+}
+
 // norms[2 i] = sum of parts[begin[i] .. begin[i+1]), norms[2 i + 1] the same
 // over parts[nb + ...] (fixed order: deterministic).
 __global__ void pair_segment_sum_kernel(const double* parts, int nb, const int* begin, int nseg, double* norms) {
@@ -2664,6 +2730,22 @@ int xlbb_batched_tail(int dtype, int dtype_coarse, const XlbbBatchTail* tails_de
     else return fail(XLBB_EUNSUPPORTED, "xlbb_batched_tail: dtype pair");
 #undef XLBB_TAIL
     return check_launch("xlbb_batched_tail");
+}
+
+int xlbb_batched_remove_mean_moment(int dtype, const XlbbBatchTransfer* tr_dev, const int* map_dev, int nblocks,
+                                    double* parts, const int* begin_dev, int ninst, double* sums, void* stream) {
+    if (!tr_dev || !map_dev || nblocks <= 0 || !parts || !begin_dev || ninst <= 0 || !sums)
+        return fail(XLBB_EBADARG, "xlbb_batched_remove_mean_moment: bad argument");
+    cudaStream_t st = XLBB_STREAM(stream);
+    const int2* map = reinterpret_cast<const int2*>(map_dev);
+    if (dtype == XLBB_F32) launch_k(batched_moment_map_kernel<float>, nblocks, 256, 0, st, tr_dev, map, nblocks, parts);
+    else if (dtype == XLBB_F64)
+        launch_k(batched_moment_map_kernel<double>, nblocks, 256, 0, st, tr_dev, map, nblocks, parts);
+    else return fail(XLBB_EUNSUPPORTED, "xlbb_batched_remove_mean_moment: dtype");
+    launch_k(pair_segment_sum_kernel, ninst, 256, 0, st, (const double*)parts, nblocks, begin_dev, ninst, sums);
+    if (dtype == XLBB_F32) launch_k(batched_shift_map_kernel<float>, nblocks, 256, 0, st, tr_dev, map, (const double*)sums);
+    else launch_k(batched_shift_map_kernel<double>, nblocks, 256, 0, st, tr_dev, map, (const double*)sums);
+    return check_launch("xlbb_batched_remove_mean_moment");
 }
 
 int xlbb_segment_sum(const double* parts, const int* begin_dev, int nseg, double* out, void* stream) {
