@@ -75,25 +75,65 @@ __device__ __forceinline__ T kbc_shear3(int i, T nxz, T nyz, T pxy, T pxz, T pyz
     return T(0);
 }
 
-// A rule reads the population of a direction chosen at run time: rule cells
-// stage the rule's source values in shared memory (one column per thread,
-// bank = thread) and index them there, instead of a Q-way register select
-// per rule direction (Q^2 selects per rule cell).
+// Rules, a warp per rule cell.  A cavity's x walls put one rule cell in a
+// quarter of the warps, where it would keep its warp for Q dependent rule
+// evaluations; instead the whole warp takes the rule cell's directions, one
+// per lane (coalesced code and constant loads, source values read from the
+// cell's shared-memory column), and shuffles move the cell's values in and
+// out.  (Evaluating the warps made only of rule cells -- y and z walls, lid --
+// lane by lane as well needs a second code path whose registers cost the
+// whole sweep more than it saves: measured 0.63 against 0.67 of the HBM copy
+// bandwidth on the 256^3 D3Q19 cavity.)
+constexpr uint32_t FLUID3_FULL = 0xffffffffu;
+
+template <typename T, int Q>
+__device__ __forceinline__ T lane_value(const T (&v)[Q], int lane, int src_lane) {
+    // v[lane] of lane src_lane, for every lane < Q
+    T out = T(0);
+#pragma unroll
+    for (int j = 0; j < Q; ++j) {
+        const T b = __shfl_sync(FLUID3_FULL, v[j], src_lane);
+        if (lane == j) out = b;
+    }
+    return out;
+}
+
+template <typename T, int Q>
+__device__ __forceinline__ void gather_lanes(T (&v)[Q], T val, int lane, int dst_lane) {
+    // v[j] of lane dst_lane <- val of lane j, for j < Q
+#pragma unroll
+    for (int j = 0; j < Q; ++j) {
+        const T b = __shfl_sync(FLUID3_FULL, val, j);
+        if (lane == dst_lane) v[j] = b;
+    }
+}
+
 template <typename T, int Q, bool KBC>
 __global__ void __launch_bounds__(FLUID3_THREADS) fluid3_push_kernel(const Fluid3Args<T, Q> p) {
     static_assert(!KBC || Q == 27, "the KBC collision is defined on D3Q27");
+    static_assert(Q <= 32, "a warp takes one direction per lane");
     __shared__ T stage[Q][FLUID3_THREADS];
     grid_dep_wait();
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y, z = blockIdx.z;
-    if (x >= p.nx) return;
+    const int t = threadIdx.x, lane = t & 31, wbase = t & ~31;
+    const int x = blockIdx.x * blockDim.x + t, y = blockIdx.y, z = blockIdx.z;
+    // every lane stays to the end (warp-wide shuffles); lanes past the row's
+    // end compute on the rest state and touch no memory
+    const bool valid = x < p.nx;
+    const int xs = valid ? x : p.nx - 1;
     const int row = z * p.ny + y;
-    const size_t o = (size_t)row * p.pitch + x;
+    const size_t o = (size_t)row * p.pitch + xs;
     const long long P = p.plane;
-    // f: the cell's populations, collided in place (post-collision rules
-    // re-load the inputs they need, so the inputs need not stay in registers)
+    // rule lookups and push word first: independent of the populations
+    const int rpc = (valid && p.pc.count > 0) ? probe_rule(load_probe(p.pc, row, xs), xs) : -1;
+    const uint32_t pw = (valid && p.ps.count > 0) ? __ldg(p.ps.push + (size_t)row * p.nx + xs) : 0u;
+    // f: the cell's populations, collided in place
     T f[Q];
 #pragma unroll
-    for (int i = 0; i < Q; ++i) f[i] = __ldg(p.f_in + (o + (size_t)i * P));
+    for (int i = 0; i < Q; ++i) f[i] = valid ? __ldg(p.f_in + (o + (size_t)i * P)) : w3<T, Q>(i);
+    if (rpc >= 0) {              // a rule cell keeps its inputs for its post-collision rules
+#pragma unroll
+        for (int k = 0; k < Q; ++k) stage[k][t] = f[k];
+    }
     // src/base.py:748-772: rho = sum f, u = sum c f / rho (one reciprocal of rho)
     T rho = f[0], jx = T(0), jy = T(0), jz = T(0);
 #pragma unroll
@@ -153,41 +193,59 @@ __global__ void __launch_bounds__(FLUID3_THREADS) fluid3_push_kernel(const Fluid
             f[i] = f[i] - beta * (T(2) * dS + gamma * dH);
         }
     }
-    const int t = threadIdx.x;
-    if (p.pc.count > 0) {        // post-collision rules: source values are the step's input
-        const int r = probe_rule(load_probe(p.pc, row, x), x);
-        if (r >= 0) {
-#pragma unroll
-            for (int k = 0; k < Q; ++k) stage[k][t] = __ldg(p.f_in + (o + (size_t)k * P));
-#pragma unroll
-            for (int d = 0; d < Q; ++d) {
-                const uint8_t code = __ldg(p.pc.code + (size_t)r * Q + d);
+    // post-collision rules (source values: the step's input, staged above)
+    uint32_t todo = __ballot_sync(FLUID3_FULL, rpc >= 0);
+    if (todo) {
+        __syncwarp();
+        do {
+            const int l = __ffs(todo) - 1;
+            todo &= todo - 1;
+            const int r = __shfl_sync(FLUID3_FULL, rpc, l);
+            const T cur = lane_value<T, Q>(f, lane, l);
+            T val = cur;
+            if (lane < Q) {
+                const uint8_t code = __ldg(p.pc.code + (size_t)r * Q + lane);
                 const int k = code < Q ? code : (code < 2 * Q ? code - Q : 0);
-                f[d] = rule_value<T, Q>(code, f[d], stage[k][t], p.pc.cst[(size_t)r * Q + d]);
+                val = rule_value<T, Q>(code, cur, stage[k][wbase + l], p.pc.cst[(size_t)r * Q + lane]);
             }
+            gather_lanes<T, Q>(f, val, lane, l);
+        } while (todo);
+    }
+    if (valid) {
+        const int xm = x == 0 ? p.nx - 1 : x - 1, xp = x == p.nx - 1 ? 0 : x + 1;
+        const int ym = y == 0 ? p.ny - 1 : y - 1, yp = y == p.ny - 1 ? 0 : y + 1;
+        const int zm = z == 0 ? p.nz - 1 : z - 1, zp = z == p.nz - 1 ? 0 : z + 1;
+#pragma unroll
+        for (int i = 0; i < Q; ++i) {
+            const int dx = c3x<Q>(i) > 0 ? xp : (c3x<Q>(i) < 0 ? xm : x);
+            const int dy = c3y<Q>(i) > 0 ? yp : (c3y<Q>(i) < 0 ? ym : y);
+            const int dz = c3z<Q>(i) > 0 ? zp : (c3z<Q>(i) < 0 ? zm : z);
+            if (!(pw & (1u << i))) p.f_out[((size_t)(dz * p.ny + dy) * p.pitch + dx) + (size_t)i * P] = f[i];
         }
     }
-    const uint32_t pw = p.ps.count > 0 ? __ldg(p.ps.push + (size_t)row * p.nx + x) : 0u;
-    const int xm = x == 0 ? p.nx - 1 : x - 1, xp = x == p.nx - 1 ? 0 : x + 1;
-    const int ym = y == 0 ? p.ny - 1 : y - 1, yp = y == p.ny - 1 ? 0 : y + 1;
-    const int zm = z == 0 ? p.nz - 1 : z - 1, zp = z == p.nz - 1 ? 0 : z + 1;
+    // the flagged cells' post-streaming rules, from their own post-collision values
+    const bool flagged = (pw >> 31) & 1u;
+    todo = __ballot_sync(FLUID3_FULL, flagged);
+    if (todo) {
+        const int rps = flagged ? rule_at(p.ps, row, xs) : -1;
+        __syncwarp();            // the post-collision rules' reads of stage are done
+        if (flagged) {
 #pragma unroll
-    for (int i = 0; i < Q; ++i) {
-        const int dx = c3x<Q>(i) > 0 ? xp : (c3x<Q>(i) < 0 ? xm : x);
-        const int dy = c3y<Q>(i) > 0 ? yp : (c3y<Q>(i) < 0 ? ym : y);
-        const int dz = c3z<Q>(i) > 0 ? zp : (c3z<Q>(i) < 0 ? zm : z);
-        if (!(pw & (1u << i))) p.f_out[((size_t)(dz * p.ny + dy) * p.pitch + dx) + (size_t)i * P] = f[i];
-    }
-    if (pw & (1u << 31)) {       // this cell's post-streaming rules, from its own post-collision values
-        const int r = rule_at(p.ps, row, x);
-#pragma unroll
-        for (int k = 0; k < Q; ++k) stage[k][t] = f[k];
-#pragma unroll
-        for (int d = 0; d < Q; ++d) {
-            const uint8_t code = __ldg(p.ps.code + (size_t)r * Q + d);
-            if (code != 2 * Q + 1) {
-                const int k = code < Q ? code : (code < 2 * Q ? code - Q : 0);
-                p.f_out[o + (size_t)d * P] = rule_value<T, Q>(code, T(0), stage[k][t], p.ps.cst[(size_t)r * Q + d]);
+            for (int k = 0; k < Q; ++k) stage[k][t] = f[k];
+        }
+        __syncwarp();
+        while (todo) {
+            const int l = __ffs(todo) - 1;
+            todo &= todo - 1;
+            const int r = __shfl_sync(FLUID3_FULL, rps, l);
+            if (lane < Q) {
+                const uint8_t code = __ldg(p.ps.code + (size_t)r * Q + lane);
+                if (code != 2 * Q + 1) {
+                    const int k = code < Q ? code : (code < 2 * Q ? code - Q : 0);
+                    const size_t ol = (size_t)row * p.pitch + (blockIdx.x * blockDim.x + wbase + l);
+                    p.f_out[ol + (size_t)lane * P] =
+                        rule_value<T, Q>(code, T(0), stage[k][wbase + l], p.ps.cst[(size_t)r * Q + lane]);
+                }
             }
         }
     }
