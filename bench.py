@@ -775,11 +775,11 @@ def run_mlups2d(args):
 def run_mlups3d(args):
     """The fluid path of ``examples/performance/MLUPS3d.py``: lid-driven cavity
     (Re = 100, u_wall = 0.1, full-way bounce-back on five faces, equilibrium
-    lid), BGK, FP32, ``--cavity3d-n`` cubed cells (256^3: 1.3 GB of D3Q19
-    populations, far above L2), on D3Q19 (the example's lattice; the headline
-    of this line) and D3Q27, ``--steps`` calls of the public ``step`` timed
-    with CUDA events; roofline at 8 q B per cell (q populations read and
-    written, FP32).  CPU baseline: the oracle's D3Q19 BGK step (vectorised
+    lid), FP32, ``--cavity3d-n`` cubed cells (256^3: 1.3 GB of D3Q19
+    populations, far above L2), BGK on D3Q19 (the example's lattice; the
+    headline of this line) and D3Q27, and KBC on D3Q27, ``--steps`` calls of
+    the public ``step`` timed with CUDA events; roofline at 8 q B per cell (q
+    populations read and written, FP32).  CPU baseline: the oracle's D3Q19 BGK step (vectorised
     NumPy, one process) on a 64^3 cavity."""
     import time
     import torch
@@ -788,8 +788,8 @@ def run_mlups3d(args):
     n = args.cavity3d_n
     peak, peak_kind = measured_peak_hbm()
     out = {}
-    for name in ("D3Q19", "D3Q27"):
-        C, om = make_cavity(G)
+    for name, model in (("D3Q19", "bgk"), ("D3Q27", "bgk"), ("D3Q27", "kbc")):
+        C, om = make_cavity(G, model=model)
         s = C(lattice=getattr(G, "Lattice" + name)("f32/f32"), omega=om(n), nx=n, ny=n, nz=n, precision="f32/f32",
               print_info_rate=0)
         q = s.q
@@ -809,7 +809,8 @@ def run_mlups3d(args):
         f, t = _timed(loop)
         cells = n ** 3
         gbs = cells * 8 * q * args.steps / t / 1e9
-        out[name.lower()] = {"mlups": cells * args.steps / t / 1e6, "ms_per_step": t / args.steps * 1e3,
+        out[name.lower() + ("" if model == "bgk" else "_kbc")] = {
+                             "mlups": cells * args.steps / t / 1e6, "ms_per_step": t / args.steps * 1e3,
                              "bytes_per_lu": 8 * q,
                              "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
                                           "frac": gbs / peak, "peak_kind": peak_kind},
@@ -832,7 +833,8 @@ def run_mlups3d(args):
                "sample": f"oracle D3Q19 BGK cavity step (NumPy, FP32), {m}^3 cells, {k} steps"}
     print(json.dumps({"workload": f"mlups3d_cavity_{n}^3", "metric": "MLUPS", "value": out["d3q19"]["mlups"],
                       "unit": "MLUPS", "dtype": "f32", "steps": args.steps, "warmup": args.warmup,
-                      "d3q19": out["d3q19"], "d3q27": out["d3q27"], "cpu_baseline": cpu,
+                      "d3q19": out["d3q19"], "d3q27": out["d3q27"], "d3q27_kbc": out["d3q27_kbc"],
+                      "cpu_baseline": cpu,
                       "data": "synthetic (cavity from rest, as the example)"}), flush=True)
     return 0
 
