@@ -901,7 +901,8 @@ def run_c2solve(args):
 
 
 PIPELINE_KERNELS = {0: "xlbb::sweep_kernel<DarcyPhys<float>>", 1: "xlbb::sweep_bulk_kernel<DarcyPhys<float>>",
-                    2: "xlbb::sweep_warp_kernel<DarcyPhys<float>>", 3: "xlbb::push_kernel<DarcyPhys<float>>"}
+                    2: "xlbb::sweep_warp_kernel<DarcyPhys<float>>", 3: "xlbb::push_kernel<DarcyPhys<float>>",
+                    4: "xlbb::darcy_push4_kernel"}
 
 
 def darcy_out_of_l2(peak, replays=5):

@@ -38,13 +38,11 @@ def set_config(kernel, tx, depth, ctas_per_sm, min_rows, pipeline=0):
 def candidates(dtype_bytes=4, kernel=ELASTICITY):
     """Every launch shape the library instantiates for the given element size
     and kernel family (pipelines 3 and 4 ignore depth, CTAs per SM and strip
-    height; pipeline 4, the four-column form of eligible FP32 elasticity
-    sweeps, is pipeline 3 for every other sweep, so the D2Q9 family does not
-    list it)."""
+    height; pipeline 4, the four-column form of eligible FP32 sweeps -- the
+    periodic elasticity sweep and the D2Q9 Darcy sweep -- is pipeline 3 for
+    every other sweep)."""
     out = []
     for pipe, depths in DEPTH.items():
-        if pipe == 4 and kernel != ELASTICITY:
-            continue
         ctas, rows = (CTAS_PER_SM, MIN_ROWS) if pipe < 3 else ((1,), (8,))   # pipelines 3, 4: only tx matters
         for t, d, c, m in itertools.product(TX if pipe != 2 else (128,), depths, ctas, rows):
             if dtype_bytes == 8 and (t > 128 or d > 4 or pipe == 4):

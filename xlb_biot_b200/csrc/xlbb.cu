@@ -553,6 +553,7 @@ struct FluidPhys : DarcyPhys<T_> {
 
 #include "xlbb_push.cuh"
 #include "xlbb_fluid3.cuh"
+#include "xlbb_darcy4.cuh"
 
 // Launch geometry of the sweeps: tx owned columns per CTA, strips of rows
 // chosen so that the grid holds about ctas_per_sm CTAs per SM (one wave),
@@ -1135,8 +1136,30 @@ static long long darcy_partials_t(const XlbbGrid* g, const XlbbDarcySweep* s) {
     return launch_ctas(g, resolve_shape(c, push_eligible<Ph>(a), sizeof(T) == 4));
 }
 
+// Whether a Darcy sweep takes the four-column kernel (launch pipeline 4):
+// FP32 storage and arithmetic, no resid and no fused sum, post-streaming rules
+// only with their push words, rows and planes of whole float4 (nx, pitch and
+// plane multiples of 4; planes and push words 16-byte aligned).
+static bool darcy4_ok(const XlbbGrid* g, const XlbbDarcySweep* s) {
+    auto a16 = [](const void* q) { return (reinterpret_cast<uintptr_t>(q) & 15u) == 0; };
+    const bool ps_rules = rules_view<float, 9>(s->ps).count > 0;
+    return s->resid == nullptr && s->sumsq == nullptr && g->nx % 4 == 0 && g->pitch % 4 == 0 &&
+           g->plane % 4 == 0 && a16(s->f_in) && a16(s->f_out) && a16(s->omega_field) && a16(s->source) &&
+           a16(s->ext_source) && (!ps_rules || (s->ps.push != nullptr && a16(s->ps.push)));
+}
+
 template <typename T, typename St = T>
 static int darcy_sweep_t(const XlbbGrid* g, const XlbbDarcySweep* s, cudaStream_t st) {
+    if constexpr (sizeof(T) == 4 && sizeof(St) == 4) {
+        if (g_cfg[1].pipeline == 4 && darcy4_ok(g, s)) {
+            using Ph = DarcyPhys<float>;
+            typename Ph::Args a = darcy_args<Ph>(g, s);
+            Ph::fill_ptrs(a);
+            launch_k(darcy_push4_kernel, dim3((g->nx + 127) / 128, (g->ny + DARCY4_ROWS - 1) / DARCY4_ROWS),
+                     dim3(32, DARCY4_ROWS), 0, st, a);
+            return check_launch("xlbb_darcy_sweep");
+        }
+    }
     const XlbbSweepConfig c = effective_cfg(1, darcy_dtype<T, St>());
     if (s->resid) {          // a separate instantiation: the plain sweep keeps its registers
         using Ph = DarcyPhys<T, St, true>;
@@ -2155,6 +2178,7 @@ int xlbb_elast_sweep_pipeline(int dtype, const XlbbGrid* g, const XlbbElastMater
 int xlbb_darcy_sweep_pipeline(int dtype, const XlbbGrid* g, const XlbbDarcySweep* s) {
     if (!grid_ok(g) || !s || (dtype != XLBB_F32 && dtype != XLBB_F64 && dtype != XLBB_F32_ACC64))
         return fail(XLBB_EBADARG, "xlbb_darcy_sweep_pipeline: bad argument");
+    if (dtype == XLBB_F32 && g_cfg[1].pipeline == 4 && darcy4_ok(g, s)) return 4;
     const XlbbSweepConfig c = effective_cfg(1, dtype);
     const bool push = push_eligible<DarcyPhys<double>>(darcy_args<DarcyPhys<double>>(g, s));
     return resolve_shape(c, push, dtype == XLBB_F32).pipeline;

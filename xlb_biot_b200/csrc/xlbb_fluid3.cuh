@@ -80,11 +80,10 @@ __device__ __forceinline__ T kbc_shear3(int i, T nxz, T nyz, T pxy, T pxz, T pyz
 // evaluations; instead the whole warp takes the rule cell's directions, one
 // per lane (coalesced code and constant loads, source values read from the
 // cell's shared-memory column), and shuffles move the cell's values in and
-// out.  (Evaluating the warps made only of rule cells -- y and z walls, lid --
-// lane by lane as well needs a second code path whose registers cost the
-// whole sweep more than it saves: measured 0.63 against 0.67 of the HBM copy
-// bandwidth on the 256^3 D3Q19 cavity.)
+// out.  Warps with more than FLUID3_WARP_RULES rule cells are evaluated lane
+// by lane (rolled loops through shared memory) where FLUID3_LANE_RULES says so.
 constexpr uint32_t FLUID3_FULL = 0xffffffffu;
+constexpr int FLUID3_WARP_RULES = 4;
 
 template <typename T, int Q>
 __device__ __forceinline__ T lane_value(const T (&v)[Q], int lane, int src_lane) {
@@ -108,11 +107,28 @@ __device__ __forceinline__ void gather_lanes(T (&v)[Q], T val, int lane, int dst
     }
 }
 
+// The FP32 D3Q19 BGK sweep also evaluates the warps made mostly of rule cells
+// (y and z walls, lid) lane by lane, at the registers it takes without that
+// path (below): on the 256^3 cavity 0.69 of the HBM copy
+// bandwidth against 0.67.  On D3Q27 the same path cost more than it saved
+// (0.59 against 0.65), so that sweep keeps the warp-per-rule-cell path only.
 template <typename T, int Q, bool KBC>
-__global__ void __launch_bounds__(FLUID3_THREADS) fluid3_push_kernel(const Fluid3Args<T, Q> p) {
+constexpr bool FLUID3_LANE_RULES = sizeof(T) == 4 && Q == 19 && !KBC;
+
+// CTAs per SM the sweeps are compiled for: D3Q19 FP32 56 registers, D3Q27
+// FP32 72 (what they take without a bound), FP32 KBC at most 128
+template <typename T, int Q, bool KBC>
+constexpr int fluid3_min_ctas() {
+    return sizeof(T) != 4 ? 1 : (KBC ? 4 : (Q == 19 ? 9 : 7));
+}
+
+template <typename T, int Q, bool KBC>
+__global__ void __launch_bounds__(FLUID3_THREADS, fluid3_min_ctas<T, Q, KBC>()) fluid3_push_kernel(const Fluid3Args<T, Q> p) {
     static_assert(!KBC || Q == 27, "the KBC collision is defined on D3Q27");
     static_assert(Q <= 32, "a warp takes one direction per lane");
     __shared__ T stage[Q][FLUID3_THREADS];
+    // post-collision values of the lane-by-lane rule path (below)
+    __shared__ T post[FLUID3_LANE_RULES<T, Q, KBC> ? Q : 1][FLUID3_THREADS];
     grid_dep_wait();
     const int t = threadIdx.x, lane = t & 31, wbase = t & ~31;
     const int x = blockIdx.x * blockDim.x + t, y = blockIdx.y, z = blockIdx.z;
@@ -195,6 +211,23 @@ __global__ void __launch_bounds__(FLUID3_THREADS) fluid3_push_kernel(const Fluid
     }
     // post-collision rules (source values: the step's input, staged above)
     uint32_t todo = __ballot_sync(FLUID3_FULL, rpc >= 0);
+    if constexpr (FLUID3_LANE_RULES<T, Q, KBC>) {
+        if (__popc(todo) > FLUID3_WARP_RULES) {     // a warp of rule cells: lane by lane, rolled loop
+            if (rpc >= 0) {
+#pragma unroll
+                for (int k = 0; k < Q; ++k) post[k][t] = f[k];
+#pragma unroll 1
+                for (int d = 0; d < Q; ++d) {
+                    const uint8_t code = __ldg(p.pc.code + (size_t)rpc * Q + d);
+                    const int k = code < Q ? code : (code < 2 * Q ? code - Q : 0);
+                    post[d][t] = rule_value<T, Q>(code, post[d][t], stage[k][t], p.pc.cst[(size_t)rpc * Q + d]);
+                }
+#pragma unroll
+                for (int k = 0; k < Q; ++k) f[k] = post[k][t];
+            }
+            todo = 0;
+        }
+    }
     if (todo) {
         __syncwarp();
         do {
@@ -234,6 +267,22 @@ __global__ void __launch_bounds__(FLUID3_THREADS) fluid3_push_kernel(const Fluid
             for (int k = 0; k < Q; ++k) stage[k][t] = f[k];
         }
         __syncwarp();
+        if constexpr (FLUID3_LANE_RULES<T, Q, KBC>) {
+            if (__popc(todo) > FLUID3_WARP_RULES) {     // a warp of rule cells: lane by lane, rolled loop
+                if (flagged) {
+#pragma unroll 1
+                    for (int d = 0; d < Q; ++d) {
+                        const uint8_t code = __ldg(p.ps.code + (size_t)rps * Q + d);
+                        if (code != 2 * Q + 1) {
+                            const int k = code < Q ? code : (code < 2 * Q ? code - Q : 0);
+                            p.f_out[o + (size_t)d * P] =
+                                rule_value<T, Q>(code, T(0), stage[k][t], p.ps.cst[(size_t)rps * Q + d]);
+                        }
+                    }
+                }
+                todo = 0;
+            }
+        }
         while (todo) {
             const int l = __ffs(todo) - 1;
             todo &= todo - 1;

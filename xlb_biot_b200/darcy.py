@@ -168,7 +168,8 @@ class AdvectionDiffusionReactionBGK(LBMBase):
 
     def sweep_pipeline(self, f=None, out=None):
         """The launch pipeline a sweep of this solver runs now (3: collide and
-        push; 0-2: row-marching kernels), as the library resolves it."""
+        push; 4: the same with four cells per lane and 16-byte accesses; 0-2:
+        row-marching kernels), as the library resolves it."""
         L = self._layout
         f = L.empty(9) if f is None else f
         out = L.empty(9) if out is None else out
