@@ -1199,8 +1199,9 @@ static int fluid3_sweep_t(const XlbbGrid3* g, const XlbbDarcySweep* s, cudaStrea
     a.omega = T(s->omega);
     a.pc = rules_view<T, Q>(s->pc);
     a.ps = rules_view<T, Q>(s->ps);
-    launch_k(fluid3_push_kernel<T, Q, KBC>, dim3((g->nx + FLUID3_THREADS - 1) / FLUID3_THREADS, g->ny, g->nz),
-             FLUID3_THREADS, 0, st, a);
+    const dim3 grid((g->nx + FLUID3_THREADS - 1) / FLUID3_THREADS, g->ny, g->nz);
+    if constexpr (FLUID3_LANE_RULES<T, Q, KBC>) launch_k(fluid3_push19_kernel, grid, FLUID3_THREADS, 0, st, a);
+    else launch_k(fluid3_push_kernel<T, Q, KBC>, grid, FLUID3_THREADS, 0, st, a);
     return check_launch("xlbb_fluid3_sweep");
 }
 

@@ -109,21 +109,14 @@ __device__ __forceinline__ void gather_lanes(T (&v)[Q], T val, int lane, int dst
 
 // The FP32 D3Q19 BGK sweep also evaluates the warps made mostly of rule cells
 // (y and z walls, lid) lane by lane, at the registers it takes without that
-// path (below): on the 256^3 cavity 0.69 of the HBM copy
+// path (fluid3_push19_kernel): on the 256^3 cavity 0.69 of the HBM copy
 // bandwidth against 0.67.  On D3Q27 the same path cost more than it saved
 // (0.59 against 0.65), so that sweep keeps the warp-per-rule-cell path only.
 template <typename T, int Q, bool KBC>
 constexpr bool FLUID3_LANE_RULES = sizeof(T) == 4 && Q == 19 && !KBC;
 
-// CTAs per SM the sweeps are compiled for: D3Q19 FP32 56 registers, D3Q27
-// FP32 72 (what they take without a bound), FP32 KBC at most 128
 template <typename T, int Q, bool KBC>
-constexpr int fluid3_min_ctas() {
-    return sizeof(T) != 4 ? 1 : (KBC ? 4 : (Q == 19 ? 9 : 7));
-}
-
-template <typename T, int Q, bool KBC>
-__global__ void __launch_bounds__(FLUID3_THREADS, fluid3_min_ctas<T, Q, KBC>()) fluid3_push_kernel(const Fluid3Args<T, Q> p) {
+__device__ __forceinline__ void fluid3_sweep_body(const Fluid3Args<T, Q>& p) {
     static_assert(!KBC || Q == 27, "the KBC collision is defined on D3Q27");
     static_assert(Q <= 32, "a warp takes one direction per lane");
     __shared__ T stage[Q][FLUID3_THREADS];
@@ -298,4 +291,16 @@ __global__ void __launch_bounds__(FLUID3_THREADS, fluid3_min_ctas<T, Q, KBC>()) 
             }
         }
     }
+}
+
+template <typename T, int Q, bool KBC>
+__global__ void __launch_bounds__(FLUID3_THREADS) fluid3_push_kernel(const Fluid3Args<T, Q> p) {
+    fluid3_sweep_body<T, Q, KBC>(p);
+}
+
+// FP32 D3Q19 BGK, compiled for 9 CTAs per SM: the 56 registers it takes without
+// the lane-by-lane rule path.  (An explicit bound on the other sweeps changed
+// their code for the worse: D3Q27 at the same 72 registers 0.53 against 0.64.)
+__global__ void __launch_bounds__(FLUID3_THREADS, 9) fluid3_push19_kernel(const Fluid3Args<float, 19> p) {
+    fluid3_sweep_body<float, 19, false>(p);
 }
