@@ -1200,8 +1200,17 @@ static int fluid3_sweep_t(const XlbbGrid3* g, const XlbbDarcySweep* s, cudaStrea
     a.pc = rules_view<T, Q>(s->pc);
     a.ps = rules_view<T, Q>(s->ps);
     const dim3 grid((g->nx + FLUID3_THREADS - 1) / FLUID3_THREADS, g->ny, g->nz);
-    if constexpr (FLUID3_LANE_RULES<T, Q, KBC>) launch_k(fluid3_push19_kernel, grid, FLUID3_THREADS, 0, st, a);
-    else launch_k(fluid3_push_kernel<T, Q, KBC>, grid, FLUID3_THREADS, 0, st, a);
+    if constexpr (KBC) {         // the collision-bound KBC sweep: bulk and rule cells as two launches
+        launch_k(fluid3_bulk_kernel<T, Q, KBC>, grid, FLUID3_THREADS, 0, st, a);
+        const long long nrules = (long long)a.pc.count + a.ps.count;
+        if (nrules > 0)
+            launch_k(fluid3_rules_kernel<T, Q, KBC>, dim3((unsigned)((nrules + FLUID3_THREADS - 1) / FLUID3_THREADS)),
+                     FLUID3_THREADS, 0, st, a);
+    } else if constexpr (FLUID3_LANE_RULES<T, Q, KBC>) {
+        launch_k(fluid3_push19_kernel, grid, FLUID3_THREADS, 0, st, a);
+    } else {
+        launch_k(fluid3_push_kernel<T, Q, KBC>, grid, FLUID3_THREADS, 0, st, a);
+    }
     return check_launch("xlbb_fluid3_sweep");
 }
 

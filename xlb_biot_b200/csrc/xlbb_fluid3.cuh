@@ -115,34 +115,10 @@ __device__ __forceinline__ void gather_lanes(T (&v)[Q], T val, int lane, int dst
 template <typename T, int Q, bool KBC>
 constexpr bool FLUID3_LANE_RULES = sizeof(T) == 4 && Q == 19 && !KBC;
 
+// The collision of one cell, in place: BGK (src/models.py:20-34) or KBC
+// (src/models.py:47-72) with the second-order equilibrium.
 template <typename T, int Q, bool KBC>
-__device__ __forceinline__ void fluid3_sweep_body(const Fluid3Args<T, Q>& p) {
-    static_assert(!KBC || Q == 27, "the KBC collision is defined on D3Q27");
-    static_assert(Q <= 32, "a warp takes one direction per lane");
-    __shared__ T stage[Q][FLUID3_THREADS];
-    // post-collision values of the lane-by-lane rule path (below)
-    __shared__ T post[FLUID3_LANE_RULES<T, Q, KBC> ? Q : 1][FLUID3_THREADS];
-    grid_dep_wait();
-    const int t = threadIdx.x, lane = t & 31, wbase = t & ~31;
-    const int x = blockIdx.x * blockDim.x + t, y = blockIdx.y, z = blockIdx.z;
-    // every lane stays to the end (warp-wide shuffles); lanes past the row's
-    // end compute on the rest state and touch no memory
-    const bool valid = x < p.nx;
-    const int xs = valid ? x : p.nx - 1;
-    const int row = z * p.ny + y;
-    const size_t o = (size_t)row * p.pitch + xs;
-    const long long P = p.plane;
-    // rule lookups and push word first: independent of the populations
-    const int rpc = (valid && p.pc.count > 0) ? probe_rule(load_probe(p.pc, row, xs), xs) : -1;
-    const uint32_t pw = (valid && p.ps.count > 0) ? __ldg(p.ps.push + (size_t)row * p.nx + xs) : 0u;
-    // f: the cell's populations, collided in place
-    T f[Q];
-#pragma unroll
-    for (int i = 0; i < Q; ++i) f[i] = valid ? __ldg(p.f_in + (o + (size_t)i * P)) : w3<T, Q>(i);
-    if (rpc >= 0) {              // a rule cell keeps its inputs for its post-collision rules
-#pragma unroll
-        for (int k = 0; k < Q; ++k) stage[k][t] = f[k];
-    }
+__device__ __forceinline__ void fluid3_collide(T (&f)[Q], const T om) {
     // src/base.py:748-772: rho = sum f, u = sum c f / rho (one reciprocal of rho)
     T rho = f[0], jx = T(0), jy = T(0), jz = T(0);
 #pragma unroll
@@ -156,7 +132,6 @@ __device__ __forceinline__ void fluid3_sweep_body(const Fluid3Args<T, Q>& p) {
     const T irho = T(1) / rho;
     const T ux = jx * irho, uy = jy * irho, uz = jz * irho;
     const T usqr = T(1.5) * (ux * ux + uy * uy + uz * uz);
-    const T om = p.omega;
     if constexpr (!KBC) {
 #pragma unroll
         for (int i = 0; i < Q; ++i) {
@@ -202,6 +177,37 @@ __device__ __forceinline__ void fluid3_sweep_body(const Fluid3Args<T, Q>& p) {
             f[i] = f[i] - beta * (T(2) * dS + gamma * dH);
         }
     }
+}
+
+template <typename T, int Q, bool KBC>
+__device__ __forceinline__ void fluid3_sweep_body(const Fluid3Args<T, Q>& p) {
+    static_assert(!KBC || Q == 27, "the KBC collision is defined on D3Q27");
+    static_assert(Q <= 32, "a warp takes one direction per lane");
+    __shared__ T stage[Q][FLUID3_THREADS];
+    // post-collision values of the lane-by-lane rule path (below)
+    __shared__ T post[FLUID3_LANE_RULES<T, Q, KBC> ? Q : 1][FLUID3_THREADS];
+    grid_dep_wait();
+    const int t = threadIdx.x, lane = t & 31, wbase = t & ~31;
+    const int x = blockIdx.x * blockDim.x + t, y = blockIdx.y, z = blockIdx.z;
+    // every lane stays to the end (warp-wide shuffles); lanes past the row's
+    // end compute on the rest state and touch no memory
+    const bool valid = x < p.nx;
+    const int xs = valid ? x : p.nx - 1;
+    const int row = z * p.ny + y;
+    const size_t o = (size_t)row * p.pitch + xs;
+    const long long P = p.plane;
+    // rule lookups and push word first: independent of the populations
+    const int rpc = (valid && p.pc.count > 0) ? probe_rule(load_probe(p.pc, row, xs), xs) : -1;
+    const uint32_t pw = (valid && p.ps.count > 0) ? __ldg(p.ps.push + (size_t)row * p.nx + xs) : 0u;
+    // f: the cell's populations, collided in place
+    T f[Q];
+#pragma unroll
+    for (int i = 0; i < Q; ++i) f[i] = valid ? __ldg(p.f_in + (o + (size_t)i * P)) : w3<T, Q>(i);
+    if (rpc >= 0) {              // a rule cell keeps its inputs for its post-collision rules
+#pragma unroll
+        for (int k = 0; k < Q; ++k) stage[k][t] = f[k];
+    }
+    fluid3_collide<T, Q, KBC>(f, p.omega);
     // post-collision rules (source values: the step's input, staged above)
     uint32_t todo = __ballot_sync(FLUID3_FULL, rpc >= 0);
     if constexpr (FLUID3_LANE_RULES<T, Q, KBC>) {
@@ -303,4 +309,116 @@ __global__ void __launch_bounds__(FLUID3_THREADS) fluid3_push_kernel(const Fluid
 // their code for the worse: D3Q27 at the same 72 registers 0.53 against 0.64.)
 __global__ void __launch_bounds__(FLUID3_THREADS, 9) fluid3_push19_kernel(const Fluid3Args<float, 19> p) {
     fluid3_sweep_body<float, 19, false>(p);
+}
+
+// ---------------------------------------------------------------------------
+// The same step as two launches: every cell without a rule in a kernel with
+// no rule code at all, then the rule cells, one thread each, from the rule
+// tables (a cell with both kinds of rule is taken once, by its post-collision
+// rule).  The two write disjoint outputs: every output is written once, by
+// the cell it streams from or by its own post-streaming rule.  The KBC sweep
+// runs this way (its collision takes fewer registers without rule code: 1.56
+// against 1.75 ms on the 256^3 D3Q27 cavity); for BGK the fused kernel above
+// is faster (D3Q19 0.69 against 0.58, D3Q27 0.64 against 0.58 of the HBM copy
+// bandwidth: the rule cells of the x walls, scattered one per row, cost the
+// separate launch more than the warp-shared rule path).
+// ---------------------------------------------------------------------------
+
+template <typename T, int Q>
+__device__ __forceinline__ void fluid3_push_all(const Fluid3Args<T, Q>& p, int x, int y, int z, uint32_t pw,
+                                                const T (&f)[Q]) {
+    const long long P = p.plane;
+    const int xm = x == 0 ? p.nx - 1 : x - 1, xp = x == p.nx - 1 ? 0 : x + 1;
+    const int ym = y == 0 ? p.ny - 1 : y - 1, yp = y == p.ny - 1 ? 0 : y + 1;
+    const int zm = z == 0 ? p.nz - 1 : z - 1, zp = z == p.nz - 1 ? 0 : z + 1;
+#pragma unroll
+    for (int i = 0; i < Q; ++i) {
+        const int dx = c3x<Q>(i) > 0 ? xp : (c3x<Q>(i) < 0 ? xm : x);
+        const int dy = c3y<Q>(i) > 0 ? yp : (c3y<Q>(i) < 0 ? ym : y);
+        const int dz = c3z<Q>(i) > 0 ? zp : (c3z<Q>(i) < 0 ? zm : z);
+        if (!(pw & (1u << i))) p.f_out[((size_t)(dz * p.ny + dy) * p.pitch + dx) + (size_t)i * P] = f[i];
+    }
+}
+
+template <typename T, int Q, bool KBC>
+__global__ void __launch_bounds__(FLUID3_THREADS) fluid3_bulk_kernel(const Fluid3Args<T, Q> p) {
+    grid_dep_wait();
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y, z = blockIdx.z;
+    if (x >= p.nx) return;
+    const int row = z * p.ny + y;
+    const size_t o = (size_t)row * p.pitch + x;
+    const uint32_t pw = p.ps.count > 0 ? __ldg(p.ps.push + (size_t)row * p.nx + x) : 0u;
+    const bool pc_rule = p.pc.count > 0 && probe_rule(load_probe(p.pc, row, x), x) >= 0;
+    T f[Q];
+#pragma unroll
+    for (int i = 0; i < Q; ++i) f[i] = __ldg(p.f_in + (o + (size_t)i * p.plane));
+    if (pc_rule || ((pw >> 31) & 1u)) return;     // a rule cell: fluid3_rules_kernel
+    fluid3_collide<T, Q, KBC>(f, p.omega);
+    fluid3_push_all<T, Q>(p, x, y, z, pw, f);
+}
+
+// Row of rule r of a CSR rule table over `rows` rows.
+template <typename T, int Q>
+__device__ __forceinline__ int fluid3_rule_row(const RulesView<T, Q>& rv, int r, int rows) {
+    int lo = 0, hi = rows;       // the last row whose first rule is <= r
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(rv.row_ptr + mid) <= r) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+template <typename T, int Q, bool KBC>
+__global__ void __launch_bounds__(FLUID3_THREADS) fluid3_rules_kernel(const Fluid3Args<T, Q> p) {
+    __shared__ T stage[Q][FLUID3_THREADS];
+    grid_dep_wait();
+    const int t = threadIdx.x;
+    const int r = blockIdx.x * blockDim.x + t;
+    const int npc = p.pc.count, nps = p.ps.count, rows = p.ny * p.nz;
+    if (r >= npc + nps) return;
+    int row, x, rpc = -1;
+    if (r < npc) {
+        rpc = r;
+        row = fluid3_rule_row(p.pc, r, rows);
+        x = __ldg(p.pc.cell_x + r);
+    } else {
+        const int q = r - npc;
+        row = fluid3_rule_row(p.ps, q, rows);
+        x = __ldg(p.ps.cell_x + q);
+        if (npc > 0 && probe_rule(load_probe(p.pc, row, x), x) >= 0) return;   // taken by its post-collision rule
+    }
+    const int y = row % p.ny, z = row / p.ny;
+    const size_t o = (size_t)row * p.pitch + x;
+    const long long P = p.plane;
+    const uint32_t pw = nps > 0 ? __ldg(p.ps.push + (size_t)row * p.nx + x) : 0u;
+    T f[Q];
+#pragma unroll
+    for (int i = 0; i < Q; ++i) f[i] = __ldg(p.f_in + (o + (size_t)i * P));
+    if (rpc >= 0) {              // the inputs its post-collision rules read, indexed at run time
+#pragma unroll
+        for (int k = 0; k < Q; ++k) stage[k][t] = f[k];
+    }
+    fluid3_collide<T, Q, KBC>(f, p.omega);
+    if (rpc >= 0) {
+#pragma unroll
+        for (int d = 0; d < Q; ++d) {
+            const uint8_t code = __ldg(p.pc.code + (size_t)rpc * Q + d);
+            const int k = code < Q ? code : (code < 2 * Q ? code - Q : 0);
+            f[d] = rule_value<T, Q>(code, f[d], stage[k][t], p.pc.cst[(size_t)rpc * Q + d]);
+        }
+    }
+    fluid3_push_all<T, Q>(p, x, y, z, pw, f);
+    if ((pw >> 31) & 1u) {       // its post-streaming rules, from its own post-collision values
+        const int rps = rule_at(p.ps, row, x);
+#pragma unroll
+        for (int k = 0; k < Q; ++k) stage[k][t] = f[k];
+#pragma unroll
+        for (int d = 0; d < Q; ++d) {
+            const uint8_t code = __ldg(p.ps.code + (size_t)rps * Q + d);
+            if (code != 2 * Q + 1) {
+                const int k = code < Q ? code : (code < 2 * Q ? code - Q : 0);
+                p.f_out[o + (size_t)d * P] = rule_value<T, Q>(code, T(0), stage[k][t], p.ps.cst[(size_t)rps * Q + d]);
+            }
+        }
+    }
 }
