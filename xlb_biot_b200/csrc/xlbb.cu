@@ -535,7 +535,7 @@ struct FluidPhys : DarcyPhys<T_> {
 #pragma unroll
             for (int i = 0; i < 9; ++i) {
                 const T dH = fneq[i] - dS[i];
-                const T ife = T(1) / feq[i];
+                const T ife = kbc_rcp<T>(feq[i]);
                 sh += (dS[i] * dH) * ife;
                 hh += (dH * dH) * ife;
             }

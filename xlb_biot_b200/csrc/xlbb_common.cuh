@@ -68,6 +68,14 @@ __device__ __forceinline__ T rule_value(uint8_t code, T cur, T src_val, T cst) {
 
 __device__ __forceinline__ int wrap(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
 
+// 1 / feq in the KBC entropic products: correctly rounded in FP64; in FP32 the
+// fast hardware reciprocal (__fdividef, within 2 ulp for feq's range), since
+// the FP32 KBC collision is bound by these divisions.
+template <typename T>
+__device__ __forceinline__ T kbc_rcp(T x) { return T(1) / x; }
+template <>
+__device__ __forceinline__ float kbc_rcp<float>(float x) { return __fdividef(1.0f, x); }
+
 // Programmatic dependent launch: a kernel launched with programmatic stream
 // serialization may be scheduled while its predecessor in the stream is still
 // draining; it waits here, before touching any memory, until the predecessor

@@ -163,7 +163,7 @@ __device__ __forceinline__ void fluid3_collide(T (&f)[Q], const T om) {
         for (int i = 0; i < Q; ++i) {
             const T dS = kbc_shear3<T, Q>(i, nxz, nyz, pxy, pxz, pyz) * rho;
             const T dH = (f[i] - fe[i]) - dS;
-            const T ife = T(1) / fe[i];
+            const T ife = kbc_rcp<T>(fe[i]);
             sh += (dS * dH) * ife;
             hh += (dH * dH) * ife;
         }
