@@ -23,8 +23,9 @@ TOL = {"f64/f64": 1e-12, "f32/f32": 2e-5}
 # resting interior): the oracle's own 61-step cavity moves by 1.1e-12 (FP64) and
 # 1.5e-4 (FP32) of max |f| when its initial state is perturbed by one ulp.  The
 # kernel forms the entropic products with one reciprocal of feq per direction
-# where the reference divides (the same products up to one rounding); measured
-# against the oracle: 1.4e-12 (FP64) and 8.0e-5 (FP32).  The cavity comparison
+# where the reference divides (FP64: correctly rounded, the same products up to
+# one rounding; FP32: the hardware reciprocal, within 2 ulp); measured against
+# the oracle: 1.4e-12 (FP64) and 1.1e-4 (FP32).  The cavity comparison
 # of KBC is held to twice the one-ulp sensitivity; the periodic shear wave (no
 # resting region, sensitivity 6e-7 in FP32) keeps the tight tolerances.
 TOL_KBC_CAVITY = {"f64/f64": 1e-10, "f32/f32": 3e-4}
